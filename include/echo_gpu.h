@@ -1,0 +1,185 @@
+/*
+ * echo_gpu.h -- C-ABI of the B200 (sm_100a) implementation of ECHO-QGP's
+ * per-time-step right-hand side and update.
+ *
+ * The reference keeps all state in Fortran module globals and exposes the
+ * step through argument-less module procedures (evolve.f90, work.f90).  This
+ * library owns the same state on the device and exposes one entry point per
+ * reference procedure.  Every array crosses the boundary in the reference's
+ * own Fortran column-major order, v(ix,iy,iz,k) with x fastest and the
+ * variable index k slowest, so a Fortran caller passes its arrays unchanged.
+ *
+ * Conventions
+ *   - every function returns an int status: 0 = ok, ECHO_ERR_* < 0 for
+ *     API/CUDA errors.  Physics failures (superluminal states, EoS table
+ *     range, con2prim failure) are reported through the `errcode`
+ *     out-argument with the reference's own codes (333, 777, 107, 121-138).
+ *   - one host thread per context; contexts are independent.
+ *   - no entry point allocates device memory after echo_gpu_init, except
+ *     the batch and MLP set-up calls, which say so.
+ *
+ * Variable indices (0-based; reference common.f90:63 uses 1-based):
+ *   0 rho  1 v^x  2 v^y  3 v^eta  4 p
+ *   viscous: 5 Pi  6 pi^xy  7 pi^xeta  8 pi^yeta  9 pi^xx  10 pi^yy  11 pi^etaeta
+ *   ideal MHD: 5 B^x  6 B^y  7 B^eta  [8 psi_GLM when divergence cleaning]
+ */
+#ifndef ECHO_GPU_H
+#define ECHO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ECHO_MAX_NV 16
+
+/* reconstruction algorithms (REC_ALGO, common.f90:595, work.f90:429-523) */
+enum {
+  ECHO_REC_TVD2 = 0,
+  ECHO_REC_CENO3 = 1,
+  ECHO_REC_WENO3 = 2,
+  ECHO_REC_WENO5 = 3,
+  ECHO_REC_PPM4 = 4,
+  ECHO_REC_MPE3 = 5,
+  ECHO_REC_MPE5 = 6
+};
+
+/* time integrators (INT_ALGO, common.f90:186) */
+enum { ECHO_RK2 = 2, ECHO_RK3 = 3, ECHO_SSP = 4 };
+
+/* coordinates (COORD, common.f90:83) */
+enum { ECHO_MINKOWSKI = 1, ECHO_BJORKEN = 2 };
+
+/* equations of state (EOS, eos.f90:158-188) */
+enum { ECHO_EOS_CONFORMAL = 1, ECHO_EOS_IDEALGAS = 2, ECHO_EOS_TABLE = 3 };
+
+/* con2prim solvers for ideal MHD (ALG_SOLV, common.f90:289) */
+enum {
+  ECHO_C2P_BRENT = 1,   /* reference default: BRENTM on (v^2, w*gamma^2, p) */
+  ECHO_C2P_NEWTON = 100 /* this library: analytic-Jacobian Newton, same root */
+};
+
+/* status codes */
+enum {
+  ECHO_OK = 0,
+  ECHO_ERR_ARG = -1,
+  ECHO_ERR_CUDA = -2,
+  ECHO_ERR_UNSUPPORTED = -3,
+  ECHO_ERR_TIMEOUT = -4,
+  ECHO_ERR_NOCTX = -5
+};
+
+/* Run-time parameters of the path; the names follow param.dat keys. */
+typedef struct EchoParams {
+  int nx, ny, nz;                 /* NX NY NZ */
+  double x1, x2, y1, y2, z1, z2;  /* XMIN..ZMAX (common_grid, common.f90:441) */
+  int coordinates;                /* COORD */
+  int mhd;                        /* MHD (0/1; 2 resistive is rejected) */
+  int divclean;                   /* DIVCLEAN */
+  int viscosity;                  /* VISCOUS */
+  int bulkvis;                    /* BULK */
+  int recal;                      /* REC_ALGO, ECHO_REC_* */
+  int nrk;                        /* INT_ALGO, ECHO_RK2/RK3/SSP */
+  int eqstate;                    /* EOS, ECHO_EOS_* */
+  int algo_solver;                /* ALG_SOLV, ECHO_C2P_* */
+  int obtained_zz;                /* TRACE_IMP: 1 = 'zz', 0 = 'no' */
+  int init_type;                  /* INIT_TYPE (2 and 5 change eta, tau_pi) */
+  int enable_smooth_viscosity;    /* CUT_TEMP > 0 (common.f90:1849) */
+  int ibc[ECHO_MAX_NV][2][3];     /* boundary code per variable, side, dir */
+  double cfl;                     /* CFL */
+  double maxdt;                   /* MAXDT */
+  double maxspeed;                /* MAXSPEED */
+  double glm_alpha;               /* GLM_PARAM */
+  double eta_over_s;              /* ETA_S */
+  double tau_pi_coeff;            /* TAU_PI_C */
+  double smooth_pressure;         /* p(T=CUT_TEMP), computed by the host */
+  double enezero;                 /* ENEZERO */
+  double przero;                  /* p(ENEZERO) (eos.f90:131) */
+  double c2p_tol;                 /* Newton residual target (ECHO_C2P_NEWTON) */
+} EchoParams;
+
+typedef struct EchoCtx EchoCtx;
+
+/* Per-step diagnostics, counted on the device. */
+typedef struct EchoStats {
+  double dt;            /* last time step */
+  double t;             /* current time */
+  double glm_ch;        /* GLM wave speed of the last stage */
+  long long c2p_iters;  /* sum of con2prim iterations over cells, last stage */
+  long long c2p_cells;  /* cells inverted in the last stage */
+  long long repairs;    /* cells that went through the neighbour-average repair */
+  long long seed_fallbacks; /* MLP seeds that needed the bracketed fallback */
+  int errcode;          /* first reference error code, 0 if none */
+  int err_cell;         /* linear Fortran index of the first failing cell */
+} EchoStats;
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Replaces evolve_alloc (evolve.f90:49-79), work_alloc (work.f90:49-63) and
+ * the EoS table load (eos.f90:265-334).  eos_table is n_eos rows of
+ * (T, e, p, c_s^2) in GeV and GeV/fm^3, already converted as
+ * read_data_from_tabulated_file does; NULL for analytic EoS. */
+int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos,
+                  EchoCtx** out);
+int echo_gpu_free(EchoCtx* ctx);
+int echo_gpu_nv(const EchoCtx* ctx);
+
+/* State transfer.  v and u are nx*ny*nz*nv doubles, Fortran order.  u may be
+ * NULL: the device then runs system_prim2cons (system.f90:164-263).
+ * upload also resets the step bookkeeping (echo.f90:141-144: timeold=t,
+ * timeinterval=0, vold=0). */
+int echo_gpu_upload(EchoCtx* ctx, const double* v, const double* u, double t);
+int echo_gpu_download(EchoCtx* ctx, double* v, double* u);
+/* Same, with device pointers (no host round trip). */
+int echo_gpu_upload_device(EchoCtx* ctx, const double* d_v, const double* d_u,
+                           double t);
+int echo_gpu_download_device(EchoCtx* ctx, double* d_v, double* d_u);
+
+/* tout of the driver loop (echo.f90:172,243-250); evolve_main clips dt to it */
+int echo_gpu_set_tout(EchoCtx* ctx, double tout);
+
+/* ---- the step ------------------------------------------------------------ */
+
+/* evolve_main(irk, dt) (evolve.f90:114-298): one RK/IMEX stage.  dt is
+ * computed on irk == 1 and reused afterwards, as in the reference.  On
+ * return *errcode is the reference error code (0 = ok) and run_crashed is
+ * (*errcode != 0).  Synchronises the stream. */
+int echo_gpu_evolve_main(EchoCtx* ctx, int irk, double* dt, int* errcode);
+
+/* The driver's end of step (echo.f90:211-241): timeold=t; t=t+dt;
+ * system_metric(); timeinterval=dt; vold=vnewstep.  Asynchronous. */
+int echo_gpu_end_step(EchoCtx* ctx);
+
+/* One full time step = snapshot vnewstep + nrk stages + end_step. */
+int echo_gpu_step(EchoCtx* ctx, double* dt, int* errcode);
+
+/* nsteps full steps enqueued without host synchronisation (one CUDA graph
+ * per step after the first).  Check errors with echo_gpu_stats. */
+int echo_gpu_run(EchoCtx* ctx, int nsteps);
+
+int echo_gpu_stats(EchoCtx* ctx, EchoStats* st);
+int echo_gpu_sync(EchoCtx* ctx);
+
+/* ---- pieces of the step, for parity tests against the oracle ----------- */
+
+/* evolve_dfx/dfy/dfz + evolve_src of one stage (evolve.f90:302-718) into
+ * du (nx*ny*nz*nv, Fortran order, host memory), with ax/ay/az maxima. */
+int echo_gpu_rhs(EchoCtx* ctx, double* du, double* amax3);
+
+/* Reconstruction of m pencils of length n (+ghosts) with REC_ALGO.
+ * f is m rows of (n + 8) values, f[row*(n+8) + (i+4)] = f(i), i=-4..n+3;
+ * gl/gr are m rows of n+1 faces (holib.f90:47-348). */
+int echo_gpu_test_recon(int recal, int m, int n, const double* f, double* gl,
+                        double* gr);
+
+/* system_cons2prim on ncells independent cells (system.f90:423-1166).
+ * u and v are ncells*nv, cell-major (u[c*nv+k]); v holds the initial guess
+ * on input and the result on output; err gets the per-cell code and iters
+ * the per-cell iteration count (may be NULL).  g3 = g_cov(3), gp = sqrt(-g). */
+int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, int n_eos,
+                      int ncells, double g3, double gp, const double* u,
+                      double* v, int* err, int* iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ECHO_GPU_H */

@@ -1,0 +1,2216 @@
+/*
+ * echo_oracle.c -- CPU oracle (test infrastructure only) for ECHO-QGP's
+ * per-step right-hand side and update.
+ *
+ * A restatement, routine by routine, of the reference Fortran:
+ *   holib.f90    reconstructions and limiters
+ *   work.f90     work_rec, work_glm[xyz], work_fup[xyz] (HLL)
+ *   system.f90   system_metric, prim2cons, cons2prim (HD Newton, viscous
+ *                nested Newton, MHD algo 1 = BRENTM), system_flux,
+ *                system_source, E x B helpers, sist3
+ *   viscous.f90  dts, get_viscous_parameters, get_derived_pi(_zz), get_sigma
+ *   eos.f90      analytic (.def) and tabulated EoS lookups
+ *   libacm554.f90 BRENTM (ACM TOMS 554)
+ *   evolve.f90   evolve_main, evolve_df[xyz], evolve_src, evolve_dt,
+ *                evolve_u2v, evolve_bc[xyz], evolve_glm_source,
+ *                evolve_smooth_viscosity
+ *   echo.f90     one iteration of the time loop
+ *
+ * Floating point follows gfortran -fdefault-real-8 semantics: every literal
+ * is a double, expressions keep the reference's left-to-right grouping and
+ * parentheses, integer powers x**2 and the real power x**2. are x*x (gcc
+ * folds pow(x,2.0) exactly), other real powers call pow().  The file is
+ * compiled with -ffp-contract=off so no multiply-add is fused: that is the
+ * canonical arithmetic the CUDA parity build reproduces bit for bit.
+ *
+ * Where the reference reads memory it never wrote (uninitialised locals,
+ * out-of-bounds neighbours in the con2prim repair at the domain edge), the
+ * behaviour is undefined in Fortran; this restatement pins one definition
+ * and the CUDA code uses the same one:
+ *   - EoS table lookups out of range leave their outputs unchanged (locals
+ *     start at 0) and return the reference error code;
+ *   - the repair reads neighbours through the flat Fortran address
+ *     (column-major, no bounds check) and reads 0 outside the allocation.
+ */
+#include "echo_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NGC 3
+#define PADP 4 /* pencil index offset: f(i) stored at [i + PADP] */
+
+/* variable indices, 0-based (common.f90:63) */
+enum {
+  KRH = 0, KVX = 1, KVY = 2, KVZ = 3, KPR = 4,
+  KPIBU = 5, KPIXY = 6, KPIXZ = 7, KPIYZ = 8, KPIXX = 9, KPIYY = 10, KPIZZ = 11
+};
+/* derivative indices (common.f90:70-72), 0-based */
+enum {
+  DTX = 0, DTY, DTZ, DXX, DXY, DXZ, DYX, DYY, DYZ, DZX, DZY, DZZ,
+  DTT, DXT, DYT, DZT, NDERIV = 20
+};
+/* sigma indices (viscous.f90:47), 0-based */
+enum { SXX = 0, SYY = 1, SZZ = 2, SXY = 3, SXZ = 4, SYZ = 5 };
+
+/* ------------------------------------------------------------------------ */
+/* physics context shared by the pointwise routines                         */
+/* ------------------------------------------------------------------------ */
+typedef struct Phys {
+  const EchoParams* p;
+  int nv, nu;
+  int kbx, kby, kbz, kglm;
+  /* metric (system_metric_*, system.f90:132-160) */
+  double g1, g2, g3, gp, gm, g0;
+  double t;
+  /* EoS table (eos.f90:265-334) */
+  int nt;
+  const double *tT, *te, *tp, *tc;
+} Phys;
+
+static void phys_setup(Phys* ph, const EchoParams* p) {
+  memset(ph, 0, sizeof(*ph));
+  ph->p = p;
+  int nv = p->viscosity ? 12 : 5; /* system_setup, system.f90:80-88 */
+  ph->kbx = ph->kby = ph->kbz = ph->kglm = -1;
+  if (p->mhd) {
+    nv += 3;
+    ph->kbx = nv - 3;
+    ph->kby = nv - 2;
+    ph->kbz = nv - 1;
+    if (p->divclean) {
+      nv += 1;
+      ph->kglm = nv - 1;
+    }
+  }
+  ph->nv = nv;
+  ph->nu = nv;
+  ph->g0 = -1.;
+}
+
+static void phys_metric(Phys* ph, double t) {
+  ph->t = t;
+  if (ph->p->coordinates == ECHO_BJORKEN) {
+    ph->g1 = 1.;
+    ph->g2 = 1.;
+    ph->g3 = t * t;
+    ph->gp = t;
+    ph->gm = 1. / ph->gp;
+  } else {
+    ph->g1 = ph->g2 = ph->g3 = 1.;
+    ph->gp = 1.;
+    ph->gm = 1.;
+  }
+  ph->g0 = -1.;
+}
+
+/* ------------------------------------------------------------------------ */
+/* EoS                                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* binary search of eos.f90:430-442 (identical in every table routine):
+ * returns indxh (1-based); indxl = indxh - 1 */
+static int tab_search(const double* arr, int n, double val) {
+  int lo = 1, hi = n, mid = (lo + hi) / 2;
+  while (lo + 1 != hi) {
+    if (val > arr[mid - 1]) {
+      lo = mid;
+      mid = (lo + hi) / 2;
+    } else {
+      hi = mid;
+      mid = (lo + hi) / 2;
+    }
+  }
+  return hi;
+}
+
+/* eos_energy: tabulated get_energy (eos.f90:468-523) or analytic
+ * eos_energy_ana with NUM_DER=0 (eos.f90:1104-1185 + energy_den*.def) */
+static int eos_energy(const Phys* ph, double rh, double* en, double pr) {
+  const EchoParams* p = ph->p;
+  if (p->eqstate == ECHO_EOS_TABLE) {
+    if (pr < ph->tp[0]) return 125;
+    if (pr > ph->tp[ph->nt - 1]) return 126;
+    int h = tab_search(ph->tp, ph->nt, pr);
+    double p2 = ph->tp[h - 1], p1 = ph->tp[h - 2];
+    double e2 = ph->te[h - 1], e1 = ph->te[h - 2];
+    *en = e1 + (e2 - e1) * (pr - p1) / (p2 - p1);
+    return 0;
+  }
+  if (pr <= p->przero) { /* check_on_pressure branch, eos.f90:1118-1123 */
+    *en = p->enezero * pr / p->przero;
+    return 0;
+  }
+  if (p->eqstate == ECHO_EOS_CONFORMAL)
+    *en = 3. * pr;
+  else
+    *en = rh + pr / (4.0 / 3.0 - 1.);
+  return 0;
+}
+
+/* eos_pressure: get_pressure (eos.f90:399-464) or eos_pressure_ana
+ * (eos.f90:886-922, pressure_vs_rh_en*.def, part_der_pr_vs_rh_en*.def) */
+static int eos_pressure(const Phys* ph, double rh, double en, double* pr,
+                        double* dprdrh, double* dprden) {
+  const EchoParams* p = ph->p;
+  if (p->eqstate == ECHO_EOS_TABLE) {
+    if (en < ph->te[0]) return 123;
+    if (en > ph->te[ph->nt - 1]) return 124;
+    int h = tab_search(ph->te, ph->nt, en);
+    double p2 = ph->tp[h - 1], p1 = ph->tp[h - 2];
+    double e2 = ph->te[h - 1], e1 = ph->te[h - 2];
+    double t2 = ph->tT[h - 1], t1 = ph->tT[h - 2];
+    *pr = p1 + (p2 - p1) * (en - e1) / (e2 - e1);
+    double dpt = (p2 - p1) / (t2 - t1);
+    double det = (e2 - e1) / (t2 - t1);
+    *dprdrh = 0;
+    *dprden = dpt / det;
+    return 0;
+  }
+  if (p->eqstate == ECHO_EOS_CONFORMAL) {
+    double a = 3.0;
+    *pr = en / a;
+    *dprdrh = 0.;
+    *dprden = 1. / 3.;
+  } else {
+    double gam = 4.0 / 3.0;
+    *pr = (gam - 1.) * (en - rh);
+    *dprdrh = -gam + 1.;
+    *dprden = gam - 1.;
+  }
+  return 0;
+}
+
+/* eos_sound: get_sound (eos.f90:590-641) or eos_sound_ana (eos.f90:926-952) */
+static int eos_sound(const Phys* ph, double rh, double en, double pr,
+                     double* cs2) {
+  const EchoParams* p = ph->p;
+  if (p->eqstate == ECHO_EOS_TABLE) {
+    if (en < ph->te[0]) return 131;
+    if (en > ph->te[ph->nt - 1]) return 132;
+    int h = tab_search(ph->te, ph->nt, en);
+    double s2 = ph->tc[h - 1], s1 = ph->tc[h - 2];
+    double e2 = ph->te[h - 1], e1 = ph->te[h - 2];
+    *cs2 = s1 + (s2 - s1) * (en - e1) / (e2 - e1);
+    return 0;
+  }
+  double dprden, dprdrh;
+  if (p->eqstate == ECHO_EOS_CONFORMAL) {
+    dprden = 1. / 3.;
+    dprdrh = 0.;
+  } else {
+    double gam = 4.0 / 3.0;
+    dprden = gam - 1.;
+    dprdrh = -gam + 1.;
+  }
+  double c;
+  if (en + pr == 0)
+    c = dprden;
+  else
+    c = dprden + (rh / (en + pr)) * dprdrh;
+  *cs2 = c > 0.0 ? c : 0.0;
+  return 0;
+}
+
+/* get_derived_data: get_derived_data_tab (eos.f90:645-701) or
+ * get_derived_data_ana (eos.f90:956-968 with temperature.def) */
+static int get_derived_data(const Phys* ph, double rh, double pr, double* en,
+                            double* temp, double* s) {
+  const EchoParams* p = ph->p;
+  if (p->eqstate == ECHO_EOS_TABLE) {
+    if (pr < ph->tp[0]) return 135;
+    if (pr > ph->tp[ph->nt - 1]) return 136;
+    int h = tab_search(ph->tp, ph->nt, pr);
+    double p2 = ph->tp[h - 1], p1 = ph->tp[h - 2];
+    double e2 = ph->te[h - 1], e1 = ph->te[h - 2];
+    double t2 = ph->tT[h - 1], t1 = ph->tT[h - 2];
+    double fac = (pr - p1) / (p2 - p1);
+    *temp = t1 + (t2 - t1) * fac;
+    *en = e1 + (e2 - e1) * fac;
+    *s = (*en + pr) / *temp;
+    return 0;
+  }
+  int err = eos_energy(ph, rh, en, pr);
+  *temp = 0.148909 * pow(*en, 0.25);
+  if (*temp == 0)
+    *s = 0.;
+  else
+    *s = (*en + pr) / *temp;
+  return err;
+}
+
+/* ------------------------------------------------------------------------ */
+/* reconstruction (holib.f90)                                               */
+/* ------------------------------------------------------------------------ */
+
+static double fsign1(double d) { return copysign(1.0, d); }
+
+static double mm2(double d1, double d2) { /* holib.f90:440-452 */
+  double s1 = fsign1(d1), s2 = fsign1(d2);
+  double a1 = fabs(d1), a2 = fabs(d2);
+  return .5 * (s1 + s2) * (a1 < a2 ? a1 : a2);
+}
+
+static double fmin3(double a, double b, double c) {
+  double r = a;
+  if (b < r) r = b;
+  if (c < r) r = c;
+  return r;
+}
+static double fmax3(double a, double b, double c) {
+  double r = a;
+  if (b > r) r = b;
+  if (c > r) r = c;
+  return r;
+}
+
+static double mm4(double d1, double d2, double d3, double d4) { /* :472-486 */
+  double s1 = fsign1(d1), s2 = fsign1(d2), s3 = fsign1(d3), s4 = fsign1(d4);
+  double m = fabs(d1);
+  if (fabs(d2) < m) m = fabs(d2);
+  if (fabs(d3) < m) m = fabs(d3);
+  if (fabs(d4) < m) m = fabs(d4);
+  return .125 * (s1 + s2) * fabs((s1 + s3) * (s1 + s4)) * m;
+}
+
+static double ceno3(const double d[3]) { /* holib.f90:490-510 */
+  const double alpha = 0.7;
+  double r = 0.;
+  int is0 = (int)fsign1(d[0]), is1 = (int)fsign1(d[1]), is2 = (int)fsign1(d[2]);
+  int s = is0 + is1 + is2;
+  if (abs(s) == 3) {
+    double w0 = fabs(d[0]), w1 = alpha * fabs(d[1]), w2 = fabs(d[2]);
+    int m = 0;
+    double wm = w0;
+    if (w1 < wm) {
+      wm = w1;
+      m = 1;
+    }
+    if (w2 < wm) {
+      wm = w2;
+      m = 2;
+    }
+    r = d[m];
+  }
+  return r;
+}
+
+static double mp5(double f, double f1, double f2, double f3, double f4,
+                  double f5) { /* holib.f90:514-536 */
+  double r = f;
+  double ful = f3 + 2 * (f3 - f2);
+  double fmp = f3 + mm2(f4 - f3, ful - f3);
+  if ((f - f3) * (f - fmp) > 0.) {
+    double dm = f1 - 2 * f2 + f3;
+    double d0 = f2 - 2 * f3 + f4;
+    double dp = f3 - 2 * f4 + f5;
+    double fmd = .5 * (f3 + f4) - .5 * mm4(4 * d0 - dp, 4 * dp - d0, d0, dp);
+    double flc = f3 + .5 * (f3 - f2) + (4. / 3.) * mm4(4 * d0 - dm, 4 * dm - d0, d0, dm);
+    double lo1 = fmin3(f3, f4, fmd), lo2 = fmin3(f3, ful, flc);
+    double hi1 = fmax3(f3, f4, fmd), hi2 = fmax3(f3, ful, flc);
+    double fmin = lo1 > lo2 ? lo1 : lo2;
+    double fmax = hi1 < hi2 ? hi1 : hi2;
+    r = f + mm2(fmin - f, fmax - f);
+  }
+  return r;
+}
+
+/* f points at f(0); valid f(-3)..f(n+4).  gl/gr are faces 0..n. */
+static void rec_pencil(int recal, const double* f, double* gl, double* gr,
+                       int n) {
+  int i;
+  switch (recal) {
+    case ECHO_REC_TVD2: /* holib.f90:47-77 */
+      for (i = 1; i <= n; i++) {
+        double dp = .5 * mm2(f[i] - f[i - 1], f[i + 1] - f[i]);
+        gl[i] = f[i] + dp;
+        gr[i - 1] = f[i] - dp;
+      }
+      gl[0] = f[0] + .5 * mm2(f[0] - f[-1], f[1] - f[0]);
+      gr[n] = f[n + 1] - .5 * mm2(f[n + 1] - f[n], f[n + 2] - f[n + 1]);
+      break;
+    case ECHO_REC_CENO3: { /* holib.f90:81-126 */
+      const double c11 = 3 / 8., c21 = -10 / 8., c31 = 15 / 8.;
+      const double c12 = -1 / 8., c22 = 6 / 8., c32 = 3 / 8.;
+      const double c13 = 3 / 8., c23 = 6 / 8., c33 = -1 / 8.;
+      for (i = 0; i <= n; i++) {
+        double d[3], f1, f2, f3, f4, f5, p;
+        f1 = f[i - 2]; f2 = f[i - 1]; f3 = f[i]; f4 = f[i + 1]; f5 = f[i + 2];
+        p = f3 + .5 * mm2(f3 - f2, f4 - f3);
+        d[0] = c11 * f1 + c21 * f2 + c31 * f3 - p;
+        d[1] = c12 * f2 + c22 * f3 + c32 * f4 - p;
+        d[2] = c13 * f3 + c23 * f4 + c33 * f5 - p;
+        gl[i] = p + ceno3(d);
+        f1 = f[i + 3]; f2 = f[i + 2]; f3 = f[i + 1]; f4 = f[i]; f5 = f[i - 1];
+        p = f3 + .5 * mm2(f3 - f2, f4 - f3);
+        d[0] = c11 * f1 + c21 * f2 + c31 * f3 - p;
+        d[1] = c12 * f2 + c22 * f3 + c32 * f4 - p;
+        d[2] = c13 * f3 + c23 * f4 + c33 * f5 - p;
+        gr[i] = p + ceno3(d);
+      }
+      break;
+    }
+    case ECHO_REC_WENO3: { /* holib.f90:130-173 */
+      const double d1 = 1 / 3., d2 = 2 / 3., eps = 1.e-6;
+      const double c11 = -1 / 2., c21 = 3 / 2., c12 = 1 / 2., c22 = 1 / 2.;
+      for (i = 0; i <= n; i++) {
+        double f1, f2, f3, b1, b2, a1, a2, p1, p2;
+        f1 = f[i - 1]; f2 = f[i]; f3 = f[i + 1];
+        b1 = (f2 - f1) * (f2 - f1);
+        b2 = (f3 - f2) * (f3 - f2);
+        a1 = d1 / ((b1 + eps) * (b1 + eps));
+        a2 = d2 / ((b2 + eps) * (b2 + eps));
+        p1 = c11 * f1 + c21 * f2;
+        p2 = c12 * f2 + c22 * f3;
+        gl[i] = (a1 * p1 + a2 * p2) / (a1 + a2);
+        f1 = f[i + 2]; f2 = f[i + 1]; f3 = f[i];
+        b1 = (f2 - f1) * (f2 - f1);
+        b2 = (f3 - f2) * (f3 - f2);
+        a1 = d1 / ((b1 + eps) * (b1 + eps));
+        a2 = d2 / ((b2 + eps) * (b2 + eps));
+        p1 = c11 * f1 + c21 * f2;
+        p2 = c12 * f2 + c22 * f3;
+        gr[i] = (a1 * p1 + a2 * p2) / (a1 + a2);
+      }
+      break;
+    }
+    case ECHO_REC_WENO5: { /* holib.f90:177-232 */
+      const double d1 = 1 / 16., d2 = 10 / 16., d3 = 5 / 16., eps = 1.e-6;
+      const double c11 = 3 / 8., c21 = -10 / 8., c31 = 15 / 8.;
+      const double c12 = -1 / 8., c22 = 6 / 8., c32 = 3 / 8.;
+      const double c13 = 3 / 8., c23 = 6 / 8., c33 = -1 / 8.;
+      for (i = 0; i <= n; i++) {
+        double f1, f2, f3, f4, f5, t1, t2, b1, b2, b3, a1, a2, a3, p1, p2, p3, q;
+        f1 = f[i - 2]; f2 = f[i - 1]; f3 = f[i]; f4 = f[i + 1]; f5 = f[i + 2];
+        t1 = f3 - 2 * f2 + f1; t2 = 3. * f3 - 4. * f2 + f1;
+        b1 = 13. * (t1 * t1) + 3. * (t2 * t2);
+        t1 = f4 - 2 * f3 + f2; t2 = f4 - f2;
+        b2 = 13. * (t1 * t1) + 3. * (t2 * t2);
+        t1 = f5 - 2 * f4 + f3; t2 = f5 - 4. * f4 + 3. * f3;
+        b3 = 13. * (t1 * t1) + 3. * (t2 * t2);
+        q = b1 / 12. + eps; a1 = d1 / (q * q);
+        q = b2 / 12. + eps; a2 = d2 / (q * q);
+        q = b3 / 12. + eps; a3 = d3 / (q * q);
+        p1 = c11 * f1 + c21 * f2 + c31 * f3;
+        p2 = c12 * f2 + c22 * f3 + c32 * f4;
+        p3 = c13 * f3 + c23 * f4 + c33 * f5;
+        gl[i] = (a1 * p1 + a2 * p2 + a3 * p3) / (a1 + a2 + a3);
+        f1 = f[i + 3]; f2 = f[i + 2]; f3 = f[i + 1]; f4 = f[i]; f5 = f[i - 1];
+        t1 = f3 - 2 * f2 + f1; t2 = 3. * f3 - 4. * f2 + f1;
+        b1 = 13. * (t1 * t1) + 3. * (t2 * t2);
+        t1 = f4 - 2 * f3 + f2; t2 = f4 - f2;
+        b2 = 13. * (t1 * t1) + 3. * (t2 * t2);
+        t1 = f5 - 2 * f4 + f3; t2 = f5 - 4. * f4 + 3. * f3;
+        b3 = 13. * (t1 * t1) + 3. * (t2 * t2);
+        q = b1 / 12. + eps; a1 = d1 / (q * q);
+        q = b2 / 12. + eps; a2 = d2 / (q * q);
+        q = b3 / 12. + eps; a3 = d3 / (q * q);
+        p1 = c11 * f1 + c21 * f2 + c31 * f3;
+        p2 = c12 * f2 + c22 * f3 + c32 * f4;
+        p3 = c13 * f3 + c23 * f4 + c33 * f5;
+        gr[i] = (a1 * p1 + a2 * p2 + a3 * p3) / (a1 + a2 + a3);
+      }
+      break;
+    }
+    case ECHO_REC_PPM4: /* holib.f90:236-268 */
+      for (i = 0; i <= n; i++) {
+        double f1, f2, f3, f4;
+        f1 = f[i - 1]; f2 = f[i]; f3 = f[i + 1]; f4 = f[i + 2];
+        gl[i] = f2 + .5 * (f3 - f2) - .125 * (mm2(f4 - f3, f3 - f2) - mm2(f3 - f2, f2 - f1));
+        f1 = f[i + 2]; f2 = f[i + 1]; f3 = f[i]; f4 = f[i - 1];
+        gr[i] = f2 + .5 * (f3 - f2) - .125 * (mm2(f4 - f3, f3 - f2) - mm2(f3 - f2, f2 - f1));
+      }
+      break;
+    case ECHO_REC_MPE3: { /* holib.f90:272-294 */
+      const double d1 = -1 / 8., d2 = 6 / 8., d3 = 3 / 8.;
+      for (i = 0; i <= n; i++) {
+        gl[i] = d1 * f[i - 1] + d2 * f[i] + d3 * f[i + 1];
+        gr[i] = d1 * f[i + 2] + d2 * f[i + 1] + d3 * f[i];
+      }
+      for (i = 0; i <= n; i++) {
+        gl[i] = mp5(gl[i], f[i - 2], f[i - 1], f[i], f[i + 1], f[i + 2]);
+        gr[i] = mp5(gr[i], f[i + 3], f[i + 2], f[i + 1], f[i], f[i - 1]);
+      }
+      break;
+    }
+    case ECHO_REC_MPE5: { /* holib.f90:298-320 */
+      const double d1 = 3 / 128., d2 = -20 / 128., d3 = 90 / 128.,
+                   d4 = 60 / 128., d5 = -5 / 128.;
+      for (i = 0; i <= n; i++) {
+        gl[i] = d1 * f[i - 2] + d2 * f[i - 1] + d3 * f[i] + d4 * f[i + 1] + d5 * f[i + 2];
+        gr[i] = d1 * f[i + 3] + d2 * f[i + 2] + d3 * f[i + 1] + d4 * f[i] + d5 * f[i - 1];
+      }
+      for (i = 0; i <= n; i++) {
+        gl[i] = mp5(gl[i], f[i - 2], f[i - 1], f[i], f[i + 1], f[i + 2]);
+        gr[i] = mp5(gr[i], f[i + 3], f[i + 2], f[i + 1], f[i], f[i - 1]);
+      }
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+void orc_recon(int recal, int m, int n, const double* f, double* gl,
+               double* gr) {
+  for (int r = 0; r < m; r++)
+    rec_pencil(recal, f + (size_t)r * (n + 8) + 4, gl + (size_t)r * (n + 1),
+               gr + (size_t)r * (n + 1), n);
+}
+
+/* ------------------------------------------------------------------------ */
+/* viscous helpers (viscous.f90)                                            */
+/* ------------------------------------------------------------------------ */
+
+typedef struct Pit {
+  double tt, tx, ty, tz, zz;
+} Pit;
+
+/* get_derived_pi (viscous.f90:244-255) */
+static void derived_pi(const Phys* ph, const double* p, Pit* o) {
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3;
+  o->tx = p[KPIXX] * p[KVX] * g1 + p[KPIXY] * p[KVY] * g2 + p[KPIXZ] * p[KVZ] * g3;
+  o->ty = p[KPIXY] * p[KVX] * g1 + p[KPIYY] * p[KVY] * g2 + p[KPIYZ] * p[KVZ] * g3;
+  o->tz = p[KPIXZ] * p[KVX] * g1 + p[KPIYZ] * p[KVY] * g2 + p[KPIZZ] * p[KVZ] * g3;
+  o->tt = o->tx * p[KVX] * g1 + o->ty * p[KVY] * g2 + o->tz * p[KVZ] * g3;
+  o->zz = p[KPIZZ];
+}
+
+/* get_derived_pi_zz (viscous.f90:259-279) */
+static void derived_pi_zz(const Phys* ph, const double* p, Pit* o) {
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3;
+  double vx = p[KVX], vy = p[KVY], vz = p[KVZ];
+  double pixy = p[KPIXY], pixx = p[KPIXX], piyy = p[KPIYY], piyz = p[KPIYZ],
+         pixz = p[KPIXZ];
+  o->tt = 1. / (1. - vz * vz * g3) *
+          (vx * g1 * pixy * vy * g2 + vx * vx * g1 * g1 * pixx + vy * g1 * piyz * vz * g3 +
+           2. * vx * g1 * pixz * vz * g3 + vy * g1 * g1 * pixy * vx + vy * vy * g1 * piyy * g2 +
+           vz * g3 * piyz * vy * g2 - pixx * g1 * vz * vz * g3 - piyy * g2 * vz * vz * g3);
+  o->tx = pixx * vx * g1 + pixy * vy * g2 + pixz * vz * g3;
+  o->ty = pixy * vx * g1 + piyy * vy * g2 + piyz * vz * g3;
+  o->tz = 1. / (1. - vz * vz * g3) *
+          (pixz * vx * g1 + pixz * vx * g1 * vz * vz * g3 + piyz * vy * g2 +
+           vz * vx * g1 * pixy * vy * g2 - vz * pixx * g1 - vz * piyy * g2 +
+           vz * vx * vx * g1 * g1 * pixx + vy * g1 * piyz * vz * vz * g3 +
+           vz * vy * g1 * g1 * pixy * vx + vz * vy * vy * g1 * piyy * g2);
+  o->zz = 1. / (g3 * (1. - vz * vz * g3)) *
+          (vx * g1 * pixy * vy * g2 - pixx * g1 - piyy * g2 + vx * vx * g1 * g1 * pixx +
+           vy * g1 * piyz * vz * g3 + 2. * vx * g1 * pixz * vz * g3 + vy * g1 * g1 * pixy * vx +
+           vy * vy * g1 * piyy * g2 + vz * g3 * piyz * vy * g2);
+}
+
+/* the `obtained` switch used at every call site */
+static void derived_pi_any(const Phys* ph, double* p, Pit* o) {
+  if (ph->p->obtained_zz) {
+    derived_pi_zz(ph, p, o);
+    p[KPIZZ] = o->zz;
+  } else {
+    derived_pi(ph, p, o);
+  }
+}
+
+/* get_viscous_parameters (viscous.f90:172-199) */
+static int viscous_parameters(const Phys* ph, double dens, double press,
+                              double* eta, double* zeta, double* tau_pi,
+                              double* tau_pi_big) {
+  const EchoParams* p = ph->p;
+  double en = 0, temp = 0, s = 0, cs2 = 0;
+  /* errcode is overwritten by the eos_sound call (viscous.f90:180-181) */
+  (void)get_derived_data(ph, dens, press, &en, &temp, &s);
+  int err = eos_sound(ph, dens, en, press, &cs2);
+  const double hbar = 0.197326;
+  *eta = hbar * p->eta_over_s * s;
+  if (p->init_type == 2) *eta = p->eta_over_s;
+  if (p->bulkvis)
+    *zeta = 2. * *eta * (1. / 3. - cs2);
+  else
+    *zeta = 0.;
+  if (temp == 0 || s == 0)
+    *tau_pi = 0.;
+  else
+    *tau_pi = p->tau_pi_coeff * *eta / (temp * s);
+  if (p->init_type == 5) *tau_pi = 5. * *eta / (temp * s);
+  *tau_pi_big = *tau_pi;
+  return err;
+}
+
+/* get_sigma (viscous.f90:283-393); d = deriv of the cell, v = primitives */
+static void get_sigma(const Phys* ph, const double* v, const double* d,
+                      double sigma[6]) {
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, t = ph->t;
+  double ux = v[KVX], uy = v[KVY], uz = v[KVZ];
+  double ut = 1. / sqrt(1. - g1 * ux * ux - g2 * uy * uy - g3 * uz * uz);
+  ux = ux * ut;
+  uy = uy * ut;
+  uz = uz * ut;
+  double dutdt = d[DTT], dutdx = d[DTX], dutdy = d[DTY], dutdz = d[DTZ];
+  double duxdx = d[DXX], duydy = d[DYY], duzdz = d[DZZ], duzdt = d[DZT];
+  double duzdx = d[DZX], duzdy = d[DZY], duxdt = d[DXT], duxdy = d[DXY];
+  double duxdz = d[DXZ], duydt = d[DYT], duydx = d[DYX], duydz = d[DYZ];
+  (void)dutdx; (void)dutdy; (void)dutdz;
+  if (ph->p->coordinates == ECHO_MINKOWSKI) {
+    sigma[SZZ] = ut * uz * duzdt + uz * ux * duzdx + uz * uy * duzdy + (2. / 3.) * duzdz +
+                 (2. / 3.) * duzdz * (uz * uz) - dutdt / 3. - duxdx / 3. - duydy / 3. -
+                 (uz * uz) * dutdt / 3. - (uz * uz) * duxdx / 3. - (uz * uz) * duydy / 3.;
+    sigma[SXZ] = 0.5 * ut * ux * duzdt + 0.5 * duzdx + 0.5 * (ux * ux) * duzdx +
+                 0.5 * ux * uy * duzdy + ux * uz * duzdz / 6. + 0.5 * ut * uz * duxdt +
+                 ux * uz * duxdx / 6. + 0.5 * uy * uz * duxdy + 0.5 * duxdz +
+                 0.5 * duxdz * (uz * uz) - ux * uz * dutdt / 3. - ux * uz * duydy / 3.;
+    sigma[SXY] = 0.5 * ut * ux * duydt + 0.5 * duydx + 0.5 * (ux * ux) * duydx +
+                 ux * uy * duydy / 6. + ux * uz * duydz / 2. + 0.5 * ut * uy * duxdt +
+                 ux * uy * duxdx / 6. + 0.5 * duxdy + 0.5 * duxdy * (uy * uy) +
+                 uy * uz * duxdz / 2. - ux * uy * dutdt / 3. - ux * uy * duzdz / 3.;
+    sigma[SYZ] = 0.5 * ut * uy * duzdt + ux * uy * duzdx / 2. + duzdy / 2. +
+                 duzdy * (uy * uy) / 2. + uy * uz * duzdz / 6. + ut * uz * duydt / 2. +
+                 ux * uz * duydx / 2. + uy * uz * duydy / 6. + duydz / 2. +
+                 duydz / 2. * (uz * uz) - uy * uz * dutdt / 3. - uy * uz * duxdx / 3.;
+    sigma[SXX] = ut * ux * duxdt + (2. / 3.) * duxdx + (2. / 3.) * duxdx * (ux * ux) +
+                 ux * uy * duxdy + ux * uz * duxdz - dutdt / 3. - duydy / 3. - duzdz / 3. -
+                 (ux * ux) * dutdt / 3. - (ux * ux) * duydy / 3. - (ux * ux) * duzdz / 3.;
+    sigma[SYY] = ut * uy * duydt + ux * uy * duydx + (2. / 3.) * duydy +
+                 (2. / 3.) * duydy * (uy * uy) + uy * uz * duydz - dutdt / 3. - duxdx / 3. -
+                 duzdz / 3. - (uy * uy) * dutdt / 3. - (uy * uy) * duxdx / 3. -
+                 (uy * uy) * duzdz / 3.;
+  } else {
+    double t2 = t * t, t3 = pow(t, 3.);
+    sigma[SZZ] = ut * uz * duzdt + uz * ux * duzdx + uz * uy * duzdy + (2. * duzdz) / (3. * t2) +
+                 (2. / 3.) * duzdz * (uz * uz) - dutdt / (3. * t2) - duxdx / (3. * t2) -
+                 duydy / (3. * t2) - (uz * uz) * dutdt / 3. - (uz * uz) * duxdx / 3. -
+                 (uz * uz) * duydy / 3. + 2. / 3. * ut / t3 + 5. / 3. * (ut / t) * (uz * uz);
+    sigma[SXZ] = 0.5 * ut * ux * duzdt + 0.5 * duzdx + 0.5 * (ux * ux) * duzdx +
+                 0.5 * ux * uy * duzdy + ux * uz * duzdz / 6. + 0.5 * ut * uz * duxdt +
+                 ux * uz * duxdx / 6. + 0.5 * uy * uz * duxdy + duxdz / (2. * t2) +
+                 0.5 * duxdz * (uz * uz) - ux * uz * dutdt / 3. - ux * uz * duydy / 3. +
+                 (2. / 3.) * ut * uz * ux / t;
+    sigma[SXY] = 0.5 * ut * ux * duydt + 0.5 * duydx + 0.5 * (ux * ux) * duydx +
+                 ux * uy * duydy / 6. + ux * uz * duydz / 2. + 0.5 * ut * uy * duxdt +
+                 ux * uy * duxdx / 6. + 0.5 * duxdy + 0.5 * duxdy * (uy * uy) +
+                 uy * uz * duxdz / 2. - ux * uy * dutdt / 3. - ux * uy * duzdz / 3. -
+                 ut * ux * uy / (3. * t);
+    sigma[SYZ] = 0.5 * ut * uy * duzdt + ux * uy * duzdx / 2. + duzdy / 2. +
+                 duzdy * (uy * uy) / 2. + uy * uz * duzdz / 6. + ut * uz * duydt / 2. +
+                 ux * uz * duydx / 2. + uy * uz * duydy / 6. + duydz / (2. * t2) +
+                 duydz / 2. * (uz * uz) - uy * uz * dutdt / 3. - uy * uz * duxdx / 3. +
+                 (2. / 3.) * ut * uz * uy / t;
+    sigma[SXX] = ut * ux * duxdt + (2. / 3.) * duxdx + (2. / 3.) * duxdx * (ux * ux) +
+                 ux * uy * duxdy + ux * uz * duxdz - dutdt / 3. - duydy / 3. - duzdz / 3. -
+                 ut / (3. * t) - (ux * ux) * dutdt / 3. - (ux * ux) * duydy / 3. -
+                 (ux * ux) * duzdz / 3. - (ux * ux) * ut / (3. * t);
+    sigma[SYY] = ut * uy * duydt + ux * uy * duydx + (2. / 3.) * duydy +
+                 (2. / 3.) * duydy * (uy * uy) + uy * uz * duydz - dutdt / 3. - duxdx / 3. -
+                 duzdz / 3. - ut / (3. * t) - (uy * uy) * dutdt / 3. - (uy * uy) * duxdx / 3. -
+                 (uy * uy) * duzdz / 3. - (uy * uy) * ut / (3. * t);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* E x B helpers (system.f90:1846-1897)                                     */
+/* ------------------------------------------------------------------------ */
+static void e_ideal(const Phys* ph, const double* vv, const double* b,
+                    double* E) {
+  double gp = ph->gp;
+  E[0] = -gp * (vv[1] * b[2] - vv[2] * b[1]);
+  E[1] = -gp * (vv[2] * b[0] - vv[0] * b[2]);
+  E[2] = -gp * (vv[0] * b[1] - vv[1] * b[0]);
+}
+static void exb(const Phys* ph, const double* E, const double* b, double* o) {
+  double e0 = E[0], e1 = E[1], e2 = E[2] / ph->g3, gp = ph->gp;
+  o[0] = gp * (e1 * b[2] - e2 * b[1]);
+  o[1] = gp * (e2 * b[0] - e0 * b[2]);
+  o[2] = gp * (e0 * b[1] - e1 * b[0]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* prim2cons (system.f90:164-263)                                           */
+/* ------------------------------------------------------------------------ */
+static int prim2cons(const Phys* ph, double* v, double* u) {
+  const EchoParams* p = ph->p;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gp = ph->gp;
+  double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
+  double en = 0;
+  int err = eos_energy(ph, rh, &en, pr);
+  if (err) return err;
+  double v2 = g1 * vx * vx + g2 * vy * vy + g3 * vz * vz;
+  double glf = 1. / sqrt(1. - v2);
+  double w = en + pr;
+  double ww = w * (glf * glf);
+  u[KRH] = rh * glf;
+  double E[3], EXB[3], EEM = 0;
+  if (p->mhd) {
+    e_ideal(ph, v + KVX, v + ph->kbx, E);
+    double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
+    exb(ph, E, v + ph->kbx, EXB);
+    double bx = v[ph->kbx], by = v[ph->kby], bz = v[ph->kbz];
+    double B2 = bx * bx + by * by + (bz * bz) * g3;
+    EEM = 0.5 * (E2 + B2);
+  }
+  if (p->viscosity) {
+    w = w + v[KPIBU];
+    ww = w * (glf * glf);
+    Pit pi;
+    derived_pi_any(ph, v, &pi);
+    u[KVX] = (ww * vx + pi.tx);
+    u[KVY] = (ww * vy + pi.ty);
+    u[KVZ] = (ww * vz + pi.tz) * g3;
+    u[KPR] = ww - pr - v[KPIBU] - pi.tt * ph->g0;
+    u[KPIBU] = v[KPIBU] * u[KRH];
+    u[KPIZZ] = v[KPIZZ] * u[KRH];
+    u[KPIXZ] = v[KPIXZ] * u[KRH];
+    u[KPIXY] = v[KPIXY] * u[KRH];
+    u[KPIYZ] = v[KPIYZ] * u[KRH];
+    u[KPIXX] = v[KPIXX] * u[KRH];
+    u[KPIYY] = v[KPIYY] * u[KRH];
+  } else if (p->mhd) {
+    u[KVX] = ww * vx + EXB[0];
+    u[KVY] = ww * vy + EXB[1];
+    u[KVZ] = ww * vz * g3 + EXB[2];
+    u[KPR] = ww - pr + EEM;
+    u[ph->kbx] = v[ph->kbx];
+    u[ph->kby] = v[ph->kby];
+    u[ph->kbz] = v[ph->kbz];
+    if (p->divclean) u[ph->kglm] = v[ph->kglm] / gp;
+  } else {
+    u[KVX] = ww * vx;
+    u[KVY] = ww * vy;
+    u[KVZ] = ww * vz * g3;
+    u[KPR] = ww - pr;
+  }
+  for (int k = 0; k < ph->nu; k++) u[k] = u[k] * gp;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* BRENTM (libacm554.f90:8-362) applied to sist3 (system.f90:1199-1231)     */
+/* ------------------------------------------------------------------------ */
+typedef struct Sist3 {
+  const Phys* ph;
+  double B2, SB2, S2, U, D;
+} Sist3;
+
+static void sist3(const Sist3* s, const double* X, double* F, int K) {
+  double xx = X[0], yy = X[1], pp = X[2];
+  double B2 = s->B2, SB2 = s->SB2, S2 = s->S2, U = s->U, D = s->D;
+  if (K == 1) F[0] = (yy + B2) * (yy + B2) * xx - SB2 / (yy * yy) * (2 * yy + B2) - S2;
+  if (K == 2) F[1] = yy - pp + 0.5 * (1. + xx) * B2 - 0.5 * SB2 / (yy * yy) - U;
+  if (K == 3) {
+    double rh = D * sqrt(1 - xx), en = 0;
+    (void)eos_energy(s->ph, rh, &en, pp); /* errcode ignored, system.f90:1227 */
+    F[2] = yy - (pp + en) / (1 - xx);
+  }
+}
+
+static double dmax1(double a, double b) { return b > a ? b : a; }
+static double dsign(double a, double b) { return copysign(fabs(a), b); }
+
+/* returns INFO; *nfev_out = NFEV */
+static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL,
+                   double XTOL, int MAXFEV, int MOPT, int* nfev_out) {
+  enum { N = 3, LDQ = 3 };
+  double Q[LDQ * N], SIGMA[N], WA1[N], WA2[N];
+#define QQ(i, j) Q[((j)-1) * LDQ + ((i)-1)]
+  int I, J, K, M, NFCALL, NIER6, NIER7, NIER8, NSING, INFO, NFEV, IFLAG;
+  int CONV;
+  double DELTA, DIFIT, DIFIT1, EPS, EPSMCH, ETA, FKY, FKZ, FNORM, FNORM1, H,
+      SKNORM, TEMP, XNORM;
+  const double ZERO = 0.0, P05 = 5.0e-2, SCALE = 1.0e1;
+  EPSMCH = 2.220446049250313080847e-16; /* EPSILON(1.d0) */
+  INFO = 0;
+  IFLAG = 0;
+  NFEV = 0;
+  NFCALL = 0;
+  NIER6 = -1;
+  NIER7 = -1;
+  NIER8 = 0;
+  FNORM = ZERO;
+  DIFIT = ZERO;
+  XNORM = ZERO;
+  for (I = 1; I <= N; I++) XNORM = dmax1(XNORM, fabs(X[I - 1]));
+  EPS = sqrt(EPSMCH);
+  DELTA = SCALE * XNORM;
+  if (XNORM == ZERO) DELTA = SCALE;
+  for (;;) { /* label 20 */
+    NSING = N;
+    FNORM1 = FNORM;
+    DIFIT1 = DIFIT;
+    FNORM = ZERO;
+    H = EPS * XNORM;
+    if (H == ZERO) H = EPS;
+    for (J = 1; J <= N; J++) {
+      for (I = 1; I <= N; I++) QQ(I, J) = ZERO;
+      QQ(J, J) = H;
+      WA1[J - 1] = X[J - 1];
+    }
+    for (K = 1; K <= N; K++) {
+      IFLAG = K;
+      sist3(s, WA1, FVEC, IFLAG);
+      FKY = FVEC[K - 1];
+      NFCALL = NFCALL + 1;
+      NFEV = NFCALL / N;
+      FNORM = dmax1(FNORM, fabs(FKY));
+      for (J = K; J <= N; J++) {
+        for (I = 1; I <= N; I++) WA2[I - 1] = WA1[I - 1] + QQ(I, J);
+        sist3(s, WA2, FVEC, IFLAG);
+        FKZ = FVEC[K - 1];
+        NFCALL = NFCALL + 1;
+        NFEV = NFCALL / N;
+        SIGMA[J - 1] = FKZ - FKY;
+      }
+      FVEC[K - 1] = FKY;
+      ETA = ZERO;
+      for (I = K; I <= N; I++) ETA = dmax1(ETA, fabs(SIGMA[I - 1]));
+      if (ETA == ZERO) continue; /* GO TO 150 */
+      NSING = NSING - 1;
+      SKNORM = ZERO;
+      for (I = K; I <= N; I++) {
+        SIGMA[I - 1] = SIGMA[I - 1] / ETA;
+        SKNORM = SKNORM + SIGMA[I - 1] * SIGMA[I - 1];
+      }
+      SKNORM = sqrt(SKNORM);
+      if (SIGMA[K - 1] < ZERO) SKNORM = -SKNORM;
+      SIGMA[K - 1] = SIGMA[K - 1] + SKNORM;
+      for (I = 1; I <= N; I++) WA2[I - 1] = ZERO;
+      for (J = K; J <= N; J++) {
+        TEMP = SIGMA[J - 1];
+        for (I = 1; I <= N; I++) WA2[I - 1] = WA2[I - 1] + TEMP * QQ(I, J);
+      }
+      for (J = K; J <= N; J++) {
+        TEMP = SIGMA[J - 1] / (SKNORM * SIGMA[K - 1]);
+        for (I = 1; I <= N; I++) QQ(I, J) = QQ(I, J) - TEMP * WA2[I - 1];
+      }
+      SIGMA[K - 1] = SKNORM * ETA;
+      TEMP = FKY / SIGMA[K - 1];
+      if (H * fabs(TEMP) > DELTA) TEMP = dsign(DELTA / H, TEMP);
+      for (I = 1; I <= N; I++) WA1[I - 1] = WA1[I - 1] + TEMP * QQ(I, K);
+    }
+    XNORM = ZERO;
+    DIFIT = ZERO;
+    for (I = 1; I <= N; I++) {
+      XNORM = dmax1(XNORM, fabs(WA1[I - 1]));
+      DIFIT = dmax1(DIFIT, fabs(X[I - 1] - WA1[I - 1]));
+      X[I - 1] = WA1[I - 1];
+    }
+    DELTA = dmax1(DELTA, SCALE * XNORM);
+    CONV = (FNORM < FNORM1 && DIFIT < DIFIT1 && NSING == 0);
+    NIER6 = NIER6 + 1;
+    NIER7 = NIER7 + 1;
+    NIER8 = NIER8 + 1;
+    if (CONV) NIER6 = 0;
+    if (FNORM < FNORM1 || DIFIT < DIFIT1) NIER7 = 0;
+    if (DIFIT > EPS * XNORM) NIER8 = 0;
+    if (FNORM <= FTOL) INFO = 1;
+    if (DIFIT <= XTOL * XNORM && CONV) INFO = 2;
+    if (FNORM <= FTOL && INFO == 2) INFO = 3;
+    if (INFO != 0) break;
+    if (NFEV >= MAXFEV) INFO = 4;
+    if (NSING == N) INFO = 5;
+    if (NIER6 == 5) INFO = 6;
+    if (NIER7 == 3) INFO = 7;
+    if (NIER8 == 4) INFO = 8;
+    if (INFO != 0) break;
+    if (!CONV || DIFIT > P05 * XNORM || MOPT == 1) continue; /* GO TO 220 */
+    int done = 0;
+    for (M = 2; M <= MOPT; M++) {
+      int stop_refine = 0;
+      FNORM1 = FNORM;
+      FNORM = ZERO;
+      for (K = 1; K <= N; K++) {
+        IFLAG = K;
+        sist3(s, WA1, FVEC, IFLAG);
+        FKY = FVEC[K - 1];
+        NFCALL = NFCALL + 1;
+        NFEV = NFCALL / N;
+        FNORM = dmax1(FNORM, fabs(FKY));
+        if (!(FNORM < FNORM1)) {
+          FNORM = FNORM1;
+          stop_refine = 1; /* GO TO 220 */
+          break;
+        }
+        TEMP = FKY / SIGMA[K - 1];
+        for (I = 1; I <= N; I++) WA1[I - 1] = WA1[I - 1] + TEMP * QQ(I, K);
+      }
+      if (stop_refine) break;
+      XNORM = ZERO;
+      DIFIT = ZERO;
+      for (I = 1; I <= N; I++) {
+        XNORM = dmax1(XNORM, fabs(WA1[I - 1]));
+        DIFIT = dmax1(DIFIT, fabs(X[I - 1] - WA1[I - 1]));
+        X[I - 1] = WA1[I - 1];
+      }
+      if (FNORM <= FTOL) INFO = 1;
+      if (DIFIT <= XTOL * XNORM) INFO = 2;
+      if (FNORM <= FTOL && INFO == 2) INFO = 3;
+      if (NFEV >= MAXFEV && INFO == 0) INFO = 4;
+      if (INFO != 0) {
+        done = 1;
+        break;
+      }
+    }
+    if (done) break;
+  }
+#undef QQ
+  *nfev_out = NFEV;
+  return INFO;
+}
+
+/* ------------------------------------------------------------------------ */
+/* cons2prim (system.f90:423-1166)                                          */
+/* u, v have nv entries; v holds the guess.  Returns errcode, *iters the    */
+/* number of solver iterations (Newton steps, or BRENTM function evals).    */
+/* ------------------------------------------------------------------------ */
+static int cons2prim(const Phys* ph, double* u, double* v, int* iters) {
+  const EchoParams* p = ph->p;
+  const double tol = 1.e-12, eps = 1.e-12;
+  const int iter_max = 100, ivmax = 100, ipmax = 100;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gm = ph->gm;
+  int errcode = 0;
+  *iters = 0;
+  double d = gm * u[KRH];
+  double sx = gm * u[KVX];
+  double sy = gm * u[KVY];
+  double sz = gm * u[KVZ] / g3;
+  double et = gm * u[KPR];
+  double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
+
+  if (!p->viscosity && !p->mhd) {
+    /* ideal HD Newton-Raphson on p (system.f90:511-561) */
+    double pr = v[KPR], w = 0, v2, glf, rh = 0, en, drhdpr, dendpr;
+    double pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    int iter;
+    for (iter = 1; iter <= iter_max; iter++) {
+      w = et + pr;
+      v2 = s2 / (w * w);
+      if (v2 >= 1.) {
+        *iters = iter;
+        return 777;
+      }
+      glf = 1. / sqrt(1. - v2);
+      rh = d / glf;
+      en = w * (1. - v2) - pr;
+      drhdpr = rh * v2 * glf / (en + pr);
+      dendpr = v2;
+      errcode = eos_pressure(ph, rh, en, &pr_eos, &dprdrh, &dprden);
+      f = pr_eos - pr;
+      df = dprdrh * drhdpr + dprden * dendpr - 1.;
+      dpr = -f / df;
+      if (fabs(dpr) < tol * pr) break;
+      pr = pr + dpr;
+    }
+    *iters = iter;
+    v[KRH] = rh;
+    v[KVX] = sx / w;
+    v[KVY] = sy / w;
+    v[KVZ] = sz / w;
+    v[KPR] = pr;
+    if (pr <= 0) errcode = 777;
+    return errcode;
+  }
+
+  if (p->viscosity) {
+    /* nested iteration (system.f90:564-666) */
+    double uin[ECHO_MAX_NV], vprim[ECHO_MAX_NV];
+    for (int k = 0; k < ph->nu; k++) uin[k] = gm * u[k];
+    d = uin[KRH];
+    for (int k = KPIBU; k <= KPIZZ; k++) v[k] = uin[k] / uin[KRH];
+    double vx = v[KVX], vy = v[KVY], vz = v[KVZ];
+    double v2 = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+    for (int k = 0; k < ph->nv; k++) vprim[k] = v[k];
+    double rh = 0, pr = 0, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0,
+           dprden = 0, f, df, dpr;
+    int iv, ip, tot = 0;
+    for (iv = 1; iv <= ivmax; iv++) {
+      vprim[KVX] = vx;
+      vprim[KVY] = vy;
+      vprim[KVZ] = vz;
+      Pit pi;
+      derived_pi_any(ph, vprim, &pi);
+      double en1 = et + v[KPIBU] + pi.tt * ph->g0;
+      double sx_cov = uin[KVX] - pi.tx;
+      double sy_cov = uin[KVY] - pi.ty;
+      double sz_cov = uin[KVZ] - pi.tz * g3;
+      sx = sx_cov;
+      sy = sy_cov;
+      sz = sz_cov / g3;
+      s2 = sx * sx_cov + sy * sy_cov + sz * sz_cov;
+      pr = v[KPR];
+      for (ip = 1; ip <= ipmax; ip++) {
+        tot++;
+        v2 = s2 / ((en1 + pr) * (en1 + pr));
+        if (v2 >= 1.) {
+          *iters = tot;
+          return 107;
+        }
+        glf = 1. / sqrt(1. - v2);
+        rh = d / glf;
+        en = (en1 + pr) * (1. - v2) - pr - vprim[KPIBU];
+        drhdpr = rh * v2 * glf / (en + pr);
+        dendpr = v2;
+        errcode = eos_pressure(ph, rh, en, &pr_eos, &dprdrh, &dprden);
+        f = pr_eos - pr;
+        df = dprdrh * drhdpr + dprden * dendpr - 1.;
+        dpr = -f / df;
+        if (fabs(dpr) < tol * pr) break;
+        pr = pr + dpr;
+      }
+      vx = sx / (en1 + pr);
+      if (fabs(vx) < eps) vx = 0.;
+      vy = sy / (en1 + pr);
+      if (fabs(vy) < eps) vy = 0.;
+      vz = sz / (en1 + pr);
+      if (fabs(vz) < eps) vz = 0.;
+      vprim[KVX] = vx;
+      vprim[KVY] = vy;
+      vprim[KVZ] = vz;
+      if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) break;
+    }
+    *iters = tot;
+    v[KRH] = rh;
+    v[KVX] = vx;
+    v[KVY] = vy;
+    v[KVZ] = vz;
+    v[KPR] = pr;
+    if (p->obtained_zz) {
+      Pit pi;
+      derived_pi_zz(ph, v, &pi);
+      v[KPIZZ] = pi.zz;
+    }
+    return errcode;
+  }
+
+  /* ideal MHD, algo_solver 1: BRENTM on sist3 (system.f90:668-730) */
+  {
+    double uin[ECHO_MAX_NV];
+    for (int k = 0; k < ph->nu; k++) uin[k] = gm * u[k];
+    double DD = uin[KRH];
+    sx = uin[KVX];
+    sy = uin[KVY];
+    sz = uin[KVZ];
+    double UU = uin[KPR];
+    double bx = uin[ph->kbx], by = uin[ph->kby], bz = uin[ph->kbz];
+    v[ph->kbx] = uin[ph->kbx];
+    v[ph->kby] = uin[ph->kby];
+    v[ph->kbz] = uin[ph->kbz];
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = sx * bx + sy * by + sz * bz;
+    double SB2 = SB * SB;
+    double SS2 = sx * sx + sy * sy + sz * sz / g3;
+    double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
+    double en = 0;
+    errcode = eos_energy(ph, rh, &en, pr);
+    double v2 = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+    double X[3], F[3] = {0, 0, 0};
+    X[0] = v2;
+    X[1] = (en + pr) / (1 - v2);
+    X[2] = pr;
+    Sist3 s = {ph, B2, SB2, SS2, UU, DD};
+    int nfev = 0;
+    (void)brentm3(&s, X, F, 1.e-14, 1.e-14, 300, 3, &nfev);
+    *iters = nfev;
+    double xs = X[0], ys = X[1];
+    pr = X[2];
+    rh = DD * sqrt(1 - xs);
+    vx = (sx + SB * bx / ys) / (ys + B2);
+    vy = (sy + SB * by / ys) / (ys + B2);
+    vz = (sz / g3 + SB * bz / ys) / (ys + B2);
+    v[KRH] = rh;
+    v[KVX] = vx;
+    v[KVY] = vy;
+    v[KVZ] = vz;
+    v[KPR] = pr;
+    if (p->divclean) v[ph->kglm] = u[ph->kglm];
+    return errcode;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* system_flux (system.f90:1316-1583)                                       */
+/* ------------------------------------------------------------------------ */
+static int system_flux(const Phys* ph, double* v, double* u, double* f,
+                       double* vf, int dir) {
+  const EchoParams* p = ph->p;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gp = ph->gp, gm = ph->gm;
+  double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
+  double en = 0;
+  int err = eos_energy(ph, rh, &en, pr);
+  if (err) return err;
+  double v2 = g1 * vx * vx + g2 * vy * vy + g3 * vz * vz;
+  if (v2 > 1) return 333;
+  double glf = 1. / sqrt(1. - v2);
+  double w, E[3] = {0, 0, 0}, EXB[3] = {0, 0, 0}, E2 = 0, B2 = 0, EEM = 0;
+  int kbx = ph->kbx, kby = ph->kby, kbz = ph->kbz, kglm = ph->kglm;
+  Pit pi = {0, 0, 0, 0, 0};
+  if (!p->viscosity) {
+    w = en + pr;
+    if (p->mhd) {
+      e_ideal(ph, v + KVX, v + kbx, E);
+      E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
+      exb(ph, E, v + kbx, EXB);
+      B2 = v[kbx] * v[kbx] + v[kby] * v[kby] + (v[kbz] * v[kbz]) * g3;
+      EEM = 0.5 * (E2 + B2);
+    }
+  } else {
+    w = en + pr + v[KPIBU];
+  }
+  double ww = w * (glf * glf);
+  u[KRH] = rh * glf;
+  int nou = 5, nv = ph->nv, nu = ph->nu;
+  if (p->viscosity) {
+    derived_pi_any(ph, v, &pi);
+    for (int k = KPIBU; k < nv; k++) u[k] = v[k] * u[KRH];
+    u[KVX] = ww * vx + pi.tx;
+    u[KVY] = ww * vy + pi.ty;
+    u[KVZ] = (ww * vz + pi.tz) * g3;
+    u[KPR] = ww - pr - v[KPIBU] - pi.tt * ph->g0;
+  } else if (p->mhd) {
+    u[KVX] = ww * vx + EXB[0];
+    u[KVY] = ww * vy + EXB[1];
+    u[KVZ] = ww * vz * g3 + EXB[2];
+    u[KPR] = ww - pr + EEM;
+    u[kbx] = v[kbx];
+    u[kby] = v[kby];
+    u[kbz] = v[kbz];
+    if (p->divclean) u[kglm] = v[kglm] / gp;
+  } else {
+    u[KVX] = ww * vx;
+    u[KVY] = ww * vy;
+    u[KVZ] = ww * vz * g3;
+    u[KPR] = ww - pr;
+  }
+  double wwdir, vdir, gcov_dir;
+  if (dir == 1) {
+    wwdir = ww * vx;
+    vdir = vx;
+    gcov_dir = g1;
+    f[KRH] = rh * glf * vx;
+    if (p->viscosity) {
+      f[KVX] = wwdir * vx * g1 + pr + v[KPIBU] + v[KPIXX] * g1;
+      f[KVY] = wwdir * vy * g2 + v[KPIXY] * g2;
+      f[KVZ] = wwdir * vz * g3 + v[KPIXZ] * g3;
+      f[KPR] = wwdir + pi.tx;
+      for (int k = nou; k < nv; k++) f[k] = u[k] * vx;
+    } else if (p->mhd) {
+      f[KVX] = wwdir * vx - E[0] * E[0] - v[kbx] * v[kbx] + pr + EEM;
+      f[KVY] = wwdir * vy - E[0] * E[1] - v[kbx] * v[kby];
+      f[KVZ] = wwdir * vz * g3 - E[0] * E[2] - v[kbx] * v[kbz] * g3;
+      f[KPR] = wwdir + EXB[0];
+      f[kbx] = 0.;
+      f[kby] = -E[2] * gm;
+      f[kbz] = +E[1] * gm;
+      if (p->divclean) {
+        f[kbx] = v[kglm];
+        f[kglm] = v[kbx] / gp;
+      }
+    } else {
+      f[KVX] = wwdir * vx * g1 + pr;
+      f[KVY] = wwdir * vy * g2;
+      f[KVZ] = wwdir * vz * g3;
+      f[KPR] = wwdir;
+    }
+  } else if (dir == 2) {
+    wwdir = ww * vy;
+    vdir = vy;
+    gcov_dir = g2;
+    f[KRH] = rh * glf * vy;
+    if (p->viscosity) {
+      f[KVX] = wwdir * vx * g1 + v[KPIXY] * g1;
+      f[KVY] = wwdir * vy * g2 + pr + v[KPIBU] + v[KPIYY] * g2;
+      f[KVZ] = wwdir * vz * g3 + v[KPIYZ] * g3;
+      f[KPR] = wwdir + pi.ty;
+      for (int k = nou; k < nv; k++) f[k] = u[k] * vy;
+    } else if (p->mhd) {
+      f[KVX] = wwdir * vx - E[1] * E[0] - v[kby] * v[kbx];
+      f[KVY] = wwdir * vy - E[1] * E[1] - v[kby] * v[kby] + pr + EEM;
+      f[KVZ] = wwdir * vz * g3 - E[1] * E[2] - v[kby] * v[kbz] * g3;
+      f[KPR] = wwdir + EXB[1];
+      f[kbx] = E[2] * gm;
+      f[kby] = 0.;
+      f[kbz] = -E[0] * gm;
+      if (p->divclean) {
+        f[kby] = v[kglm];
+        f[kglm] = v[kby] / gp;
+      }
+    } else {
+      f[KVX] = wwdir * vx * g1;
+      f[KVY] = wwdir * vy * g2 + pr;
+      f[KVZ] = wwdir * vz * g3;
+      f[KPR] = wwdir;
+    }
+  } else {
+    wwdir = ww * vz;
+    vdir = vz;
+    gcov_dir = g3;
+    f[KRH] = rh * glf * vz;
+    if (p->viscosity) {
+      f[KVX] = wwdir * vx * g1 + v[KPIXZ] * g1;
+      f[KVY] = wwdir * vy * g2 + v[KPIYZ] * g2;
+      f[KVZ] = wwdir * vz * g3 + pr + v[KPIBU] + v[KPIZZ] * g3;
+      f[KPR] = wwdir + pi.tz;
+      for (int k = nou; k < nv; k++) f[k] = u[k] * vz;
+    } else if (p->mhd) {
+      f[KVX] = wwdir * vx - E[2] / g3 * E[0] - v[kbz] * v[kbx];
+      f[KVY] = wwdir * vy - E[2] / g3 * E[1] - v[kbz] * v[kby];
+      f[KVZ] = wwdir * vz * g3 - (E[2] * E[2]) / g3 - (v[kbz] * v[kbz]) * g3 + pr + EEM;
+      f[KPR] = wwdir + EXB[2] / g3;
+      f[kbx] = -E[1] * gm;
+      f[kby] = E[0] * gm;
+      f[kbz] = 0.;
+      if (p->divclean) {
+        f[kbz] = v[kglm] / g3;
+        f[kglm] = v[kbz] / gp;
+      }
+    } else {
+      f[KVX] = wwdir * vx * g1;
+      f[KVY] = wwdir * vy * g2;
+      f[KVZ] = wwdir * vz * g3 + pr;
+      f[KPR] = wwdir;
+    }
+  }
+  for (int k = 0; k < nu; k++) u[k] = u[k] * gp;
+  for (int k = 0; k < nu; k++) f[k] = f[k] * gp;
+  double ca2;
+  if (p->mhd) {
+    double bb2 = B2 - E2;
+    ca2 = bb2 / (bb2 + (en + pr));
+  } else {
+    ca2 = 0.;
+  }
+  double cs2 = 0;
+  err = eos_sound(ph, rh, en, pr, &cs2);
+  if (err) return err;
+  double a2 = cs2 + ca2 - cs2 * ca2;
+  double den = 1. / (1. - v2 * a2);
+  double vf1 = den * (1. - a2) * vdir;
+  double vf2 = den * sqrt(a2 * (1. - v2) * ((1. - v2 * a2) / gcov_dir - (1. - a2) * (vdir * vdir)));
+  vf[0] = vf1 + vf2;
+  vf[1] = vf1 - vf2;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* system_source (system.f90:1587-1842), non-resistive                      */
+/* v: cell primitives (copy), d: deriv of the cell                          */
+/* ------------------------------------------------------------------------ */
+static int system_source(const Phys* ph, double* v, const double* dv,
+                         double* src) {
+  const EchoParams* p = ph->p;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gp = ph->gp, g0 = ph->g0;
+  double t = ph->t;
+  for (int k = 0; k < ph->nv; k++) src[k] = 0.;
+  double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
+  double en = 0;
+  int err = eos_energy(ph, rh, &en, pr);
+  if (err) return err;
+  double v2 = g1 * vx * vx + g2 * vy * vy + g3 * vz * vz;
+  double glf = 1. / sqrt(1. - v2);
+  double ut = glf;
+  const double lambda0 = 1., lambda1 = 1., lambda2 = 0.;
+  if (p->coordinates == ECHO_BJORKEN) {
+    if (!p->viscosity) {
+      double w = en + pr;
+      double ww = w * (glf * glf);
+      if (p->mhd) {
+        double E[3];
+        e_ideal(ph, v + KVX, v + ph->kbx, E);
+        double bx = v[ph->kbx], by = v[ph->kby], bz = v[ph->kbz];
+        double B2 = bx * bx + by * by + (bz * bz) * g3;
+        double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
+        double EEM = 0.5 * (E2 + B2);
+        double e3g = E[2] / g3;
+        src[KPR] = -t * (ww * vz * vz - e3g * e3g - bz * bz + (EEM + pr) / g3);
+      } else {
+        src[KPR] = -t * (ww * vz * vz + pr / g3);
+      }
+    } else {
+      double sigma[6], eta, zeta, tau_pi, tau_pi_big;
+      get_sigma(ph, v, dv, sigma);
+      err = viscous_parameters(ph, v[KRH], v[KPR], &eta, &zeta, &tau_pi, &tau_pi_big);
+      if (err) return err;
+      Pit pi;
+      derived_pi_any(ph, v, &pi);
+      double pitt = pi.tt, pitx = pi.tx, pity = pi.ty, pitz = pi.tz;
+      double dutdt = dv[DTT], dutdx = dv[DTX], dutdy = dv[DTY], dutdz = dv[DTZ];
+      double duxdx = dv[DXX], duydy = dv[DYY], duzdz = dv[DZZ], duzdt = dv[DZT];
+      double duzdx = dv[DZX], duzdy = dv[DZY], duxdt = dv[DXT], duxdy = dv[DXY];
+      double duxdz = dv[DXZ], duydt = dv[DYT], duydx = dv[DYX], duydz = dv[DYZ];
+      double sum_der = dutdt + duxdx + duydy + duzdz;
+      double sum_der_t = sum_der + ut / t;
+      double sum_der_0 = g0 * (glf * dutdt + glf * v[KVX] * dutdx + glf * v[KVY] * dutdy + glf * v[KVZ] * dutdz);
+      double sum_der_x = g1 * (glf * duxdt + glf * v[KVX] * duxdx + glf * v[KVY] * duxdy + glf * v[KVZ] * duxdz);
+      double sum_der_y = g2 * (glf * duydt + glf * v[KVX] * duydx + glf * v[KVY] * duydy + glf * v[KVZ] * duydz);
+      double sum_der_z = glf * ((t * t) * duzdt + 2. * t * v[KVZ]) +
+                         (t * t) * (glf * v[KVX] * duzdx + glf * v[KVY] * duzdy + glf * v[KVZ] * duzdz);
+      double w = en + pr + v[KPIBU];
+      double ww = w * (glf * glf);
+      src[KPR] = -t * (ww * vz * vz + (pr + v[KPIBU]) / g3 + v[KPIZZ]);
+      src[KPIBU] = -1. / tau_pi_big * (v[KPIBU] + zeta * sum_der_t) - lambda0 * 4. / 3. * v[KPIBU] * sum_der_t;
+      double w0x = -0.5 * (dutdx + duxdt) + 0.5 * glf * (sum_der_x - v[KVX] * g1 * sum_der_0);
+      double w0y = -0.5 * (dutdy + duydt) + 0.5 * glf * (sum_der_y - v[KVY] * g2 * sum_der_0);
+      double w0z = -0.5 * (dutdz + duzdt) + 0.5 * glf * (sum_der_z - v[KVZ] * g3 * sum_der_0);
+      double wxy = 0.5 * (g2 * duydx - duxdy) + 0.5 * glf * (g1 * v[KVX] * sum_der_y - g2 * v[KVY] * sum_der_x);
+      double wxz = 0.5 * (g3 * duzdx - duxdz) + 0.5 * glf * (g1 * v[KVX] * sum_der_z - g3 * v[KVZ] * sum_der_x);
+      double wyz = 0.5 * (g3 * duzdy - duydz) + 0.5 * glf * (g2 * v[KVY] * sum_der_z - g3 * v[KVZ] * sum_der_y);
+      double wx0 = w0x, wy0 = w0y, wz0 = w0z, wyx = -wxy, wzx = -wxz, wzy = -wyz;
+      double IVzz = 2. * (pitz * wz0 + v[KPIXZ] * wzx + v[KPIYZ] * wzy);
+      double IVxx = 2. * (pitx * wx0 + v[KPIXY] * wxy + v[KPIXZ] * wxz);
+      double IVyy = 2. * (pity * wy0 + v[KPIXY] * wyx + v[KPIYZ] * wyz);
+      double IVxy = v[KPIXX] * wyx + v[KPIYY] * wxy + v[KPIXZ] * wyz + v[KPIYZ] * wxz + pitx * wy0 + pity * wx0;
+      double IVxz = v[KPIXX] * wzx + v[KPIZZ] * wxz + v[KPIXY] * wzy + v[KPIYZ] * wxy + pitx * wz0 + pitz * wx0;
+      double IVyz = v[KPIYY] * wzy + v[KPIZZ] * wyz + v[KPIXY] * wzx + v[KPIXZ] * wyx + pity * wz0 + pitz * wy0;
+      (void)pitt;
+      src[KPIZZ] = -1. / tau_pi * (v[KPIZZ] + 2. * eta * sigma[SZZ]) - 2. * glf * v[KPIZZ] / t -
+                   2. * (glf * vz) * pitz / t - lambda0 * 4. / 3. * v[KPIZZ] * sum_der_t +
+                   lambda1 * glf * (2. * v[KVZ] * (pitz * sum_der_0 + v[KPIXZ] * sum_der_x + v[KPIYZ] * sum_der_y + v[KPIZZ] * sum_der_z)) -
+                   lambda2 * IVzz;
+      src[KPIXZ] = -1. / tau_pi * (v[KPIXZ] + 2. * eta * sigma[SXZ]) + lambda0 * (-4. / 3. * v[KPIXZ] * sum_der_t) -
+                   glf / t * v[KPIXZ] - glf * vz * pitx / t +
+                   lambda1 * glf * ((pitx * v[KVZ] + pitz * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVZ] + v[KPIXZ] * v[KVX]) * sum_der_x +
+                                    (v[KPIXY] * v[KVZ] + v[KPIYZ] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVZ] + v[KPIZZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxz;
+      src[KPIYZ] = -1. / tau_pi * (v[KPIYZ] + 2. * eta * sigma[SYZ]) + lambda0 * (-4. / 3. * v[KPIYZ] * sum_der_t) -
+                   glf / t * v[KPIYZ] - glf * vz * pity / t +
+                   lambda1 * glf * ((pity * v[KVZ] + pitz * v[KVY]) * sum_der_0 + (v[KPIXY] * v[KVZ] + v[KPIXZ] * v[KVY]) * sum_der_x +
+                                    (v[KPIYY] * v[KVZ] + v[KPIYZ] * v[KVY]) * sum_der_y + (v[KPIYZ] * v[KVZ] + v[KPIZZ] * v[KVY]) * sum_der_z) -
+                   lambda2 * IVyz;
+      src[KPIXY] = -1. / tau_pi * (v[KPIXY] + 2. * eta * sigma[SXY]) + lambda0 * (-4. / 3. * v[KPIXY] * sum_der_t) +
+                   lambda1 * glf * ((pitx * v[KVY] + pity * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVY] + v[KPIXY] * v[KVX]) * sum_der_x +
+                                    (v[KPIXY] * v[KVY] + v[KPIYY] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVY] + v[KPIYZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxy;
+      src[KPIXX] = -1. / tau_pi * (v[KPIXX] + 2. * eta * sigma[SXX]) + lambda0 * (-4. / 3. * v[KPIXX] * sum_der_t) +
+                   lambda1 * glf * (2. * v[KVX] * (pitx * sum_der_0 + v[KPIXX] * sum_der_x + v[KPIXY] * sum_der_y + v[KPIXZ] * sum_der_z)) -
+                   lambda2 * IVxx;
+      src[KPIYY] = -1. / tau_pi * (v[KPIYY] + 2. * eta * sigma[SYY]) + lambda0 * (-4. / 3. * v[KPIYY] * sum_der_t) +
+                   lambda1 * glf * (2. * v[KVY] * (pity * sum_der_0 + v[KPIXY] * sum_der_x + v[KPIYY] * sum_der_y + v[KPIYZ] * sum_der_z)) -
+                   lambda2 * IVyy;
+    }
+  } else {
+    if (p->viscosity) {
+      double sigma[6], eta, zeta, tau_pi, tau_pi_big;
+      get_sigma(ph, v, dv, sigma);
+      err = viscous_parameters(ph, v[KRH], v[KPR], &eta, &zeta, &tau_pi, &tau_pi_big);
+      if (err) return err;
+      Pit pi;
+      derived_pi_any(ph, v, &pi);
+      double pitx = pi.tx, pity = pi.ty, pitz = pi.tz;
+      double dutdt = dv[DTT], dutdx = dv[DTX], dutdy = dv[DTY], dutdz = dv[DTZ];
+      double duxdx = dv[DXX], duydy = dv[DYY], duzdz = dv[DZZ], duzdt = dv[DZT];
+      double duzdx = dv[DZX], duzdy = dv[DZY], duxdt = dv[DXT], duxdy = dv[DXY];
+      double duxdz = dv[DXZ], duydt = dv[DYT], duydx = dv[DYX], duydz = dv[DYZ];
+      double sum_der = dutdt + duxdx + duydy + duzdz;
+      double sum_der_0 = g0 * (glf * dutdt + v[KVX] * dutdx + v[KVY] * dutdy + v[KVZ] * dutdz);
+      double sum_der_x = g1 * (glf * duxdt + v[KVX] * duxdx + v[KVY] * duxdy + v[KVZ] * duxdz);
+      double sum_der_y = g2 * (glf * duydt + v[KVX] * duydx + v[KVY] * duydy + v[KVZ] * duydz);
+      double sum_der_z = g3 * (glf * duzdt + v[KVX] * duzdx + v[KVY] * duzdy + v[KVZ] * duzdz);
+      src[KPIBU] = -1. / tau_pi_big * (v[KPIBU] + zeta * sum_der) + lambda0 * (-1. / 3. * v[KPIBU] * sum_der);
+      double w0x = -0.5 * (dutdx + duxdt) + 0.5 * glf * (sum_der_x - v[KVX] * g1 * sum_der_0);
+      double w0y = -0.5 * (dutdy + duydt) + 0.5 * glf * (sum_der_y - v[KVY] * g2 * sum_der_0);
+      double w0z = -0.5 * (dutdz + duzdt) + 0.5 * glf * (sum_der_z - v[KVZ] * g3 * sum_der_0);
+      double wxy = 0.5 * (g2 * duydx - duxdy) + 0.5 * glf * (g1 * v[KVX] * sum_der_y - g2 * v[KVY] * sum_der_x);
+      double wxz = 0.5 * (g3 * duzdx - duxdz) + 0.5 * glf * (g1 * v[KVX] * sum_der_z - g3 * v[KVZ] * sum_der_x);
+      double wyz = 0.5 * (g3 * duzdy - duydz) + 0.5 * glf * (g2 * v[KVY] * sum_der_z - g3 * v[KVZ] * sum_der_y);
+      double wx0 = w0x, wy0 = w0y, wz0 = w0z, wyx = -wxy, wzx = -wxz, wzy = -wyz;
+      double IVzz = 2. * (pitz * wz0 + v[KPIXZ] * wzx + v[KPIYZ] * wzy);
+      double IVxx = 2. * (pitx * wx0 + v[KPIXY] * wxy + v[KPIXZ] * wxz);
+      double IVyy = 2. * (pity * wy0 + v[KPIXY] * wyx + v[KPIYZ] * wyz);
+      double IVxy = v[KPIXX] * wyx + v[KPIYY] * wxy + v[KPIXZ] * wyz + v[KPIYZ] * wxz + pitx * wy0 + pity * wx0;
+      double IVxz = v[KPIXX] * wzx + v[KPIZZ] * wxz + v[KPIXY] * wzy + v[KPIYZ] * wxy + pitx * wz0 + pitz * wx0;
+      double IVyz = v[KPIYY] * wzy + v[KPIZZ] * wyz + v[KPIXY] * wzx + v[KPIXZ] * wyx + pity * wz0 + pitz * wy0;
+      src[KPIZZ] = -1. / tau_pi * (v[KPIZZ] + 2. * eta * sigma[SZZ]) + lambda0 * (-4. / 3. * v[KPIZZ] * sum_der) +
+                   lambda1 * (2. * v[KVZ] * (pitz * sum_der_0 + v[KPIXZ] * sum_der_x + v[KPIYZ] * sum_der_y + v[KPIZZ] * sum_der_z)) -
+                   lambda2 * IVzz;
+      src[KPIXZ] = -1. / tau_pi * (v[KPIXZ] + 2. * eta * sigma[SXZ]) + lambda0 * (-4. / 3. * v[KPIXZ] * sum_der) +
+                   lambda1 * ((pitx * v[KVZ] + pitz * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVZ] + v[KPIXZ] * v[KVX]) * sum_der_x +
+                              (v[KPIXY] * v[KVZ] + v[KPIYZ] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVZ] + v[KPIZZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxz;
+      src[KPIXY] = -1. / tau_pi * (v[KPIXY] + 2. * eta * sigma[SXY]) + lambda0 * (-4. / 3. * v[KPIXY] * sum_der) +
+                   lambda1 * ((pitx * v[KVY] + pity * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVY] + v[KPIXY] * v[KVX]) * sum_der_x +
+                              (v[KPIXY] * v[KVY] + v[KPIYY] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVY] + v[KPIYZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxy;
+      src[KPIYZ] = -1. / tau_pi * (v[KPIYZ] + 2. * eta * sigma[SYZ]) + lambda0 * (-4. / 3. * v[KPIYZ] * sum_der) +
+                   lambda1 * ((pity * v[KVZ] + pitz * v[KVY]) * sum_der_0 + (v[KPIXY] * v[KVZ] + v[KPIXZ] * v[KVY]) * sum_der_x +
+                              (v[KPIYY] * v[KVZ] + v[KPIYZ] * v[KVY]) * sum_der_y + (v[KPIYZ] * v[KVZ] + v[KPIZZ] * v[KVY]) * sum_der_z) -
+                   lambda2 * IVyz;
+      src[KPIXX] = -1. / tau_pi * (v[KPIXX] + 2. * eta * sigma[SXX]) + lambda0 * (-4. / 3. * v[KPIXX] * sum_der) +
+                   lambda1 * (2. * v[KVX] * (pitx * sum_der_0 + v[KPIXX] * sum_der_x + v[KPIXY] * sum_der_y + v[KPIXZ] * sum_der_z)) -
+                   lambda2 * IVxx;
+      src[KPIYY] = -1. / tau_pi * (v[KPIYY] + 2. * eta * sigma[SYY]) + lambda0 * (-4. / 3. * v[KPIYY] * sum_der) +
+                   lambda1 * (2. * v[KVY] * (pity * sum_der_0 + v[KPIXY] * sum_der_x + v[KPIYY] * sum_der_y + v[KPIYZ] * sum_der_z)) -
+                   lambda2 * IVyy;
+    }
+  }
+  if (p->viscosity)
+    for (int k = KPIBU; k < ph->nv; k++) src[k] = src[k] * v[KRH];
+  for (int k = 0; k < ph->nv; k++) src[k] = src[k] * gp;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* the grid context                                                         */
+/* ------------------------------------------------------------------------ */
+struct Orc {
+  EchoParams p;
+  Phys ph;
+  int nx, ny, nz, nv, nu, nvold;
+  size_t ncell;
+  double dx, dy, dz, ddx, ddy, ddz;
+  int nt;
+  double *tT, *te, *tp, *tc;
+  double *v, *u, *u0, *du[4], *dus[4], *w, *ax, *ay, *az, *deriv;
+  double *vold, *vnewstep, *vtmp;
+  unsigned char* fail;
+  double t, tout, dtout, tmax, timeold, timeinterval, dt, g3old;
+  double glm_ch, glm_ch_old, aflux[3];
+  int run_crashed, errcode, nthreads;
+  long long repairs, c2p_iters;
+};
+
+#define IDX(e, k, ix, iy, iz) \
+  ((((size_t)(k) * (e)->nz + ((iz)-1)) * (e)->ny + ((iy)-1)) * (e)->nx + ((ix)-1))
+#define WIDX(e, k, ix, iy, iz)                                            \
+  ((((size_t)(k) * ((e)->nz + 2 * NGC) + ((iz) + NGC - 1)) * ((e)->ny + 2 * NGC) + \
+    ((iy) + NGC - 1)) * ((e)->nx + 2 * NGC) + ((ix) + NGC - 1))
+
+int orc_nv(const Orc* e) { return e->nv; }
+void orc_set_threads(Orc* e, int n) { e->nthreads = n > 0 ? n : 1; }
+double orc_time(const Orc* e) { return e->t; }
+double orc_dt(const Orc* e) { return e->dt; }
+double orc_glm_ch(const Orc* e) { return e->glm_ch; }
+long long orc_repairs(const Orc* e) { return e->repairs; }
+long long orc_c2p_iters(const Orc* e) { return e->c2p_iters; }
+
+static void table_attach(Phys* ph, double** tT, double** te, double** tp,
+                         double** tc, int* nt, const double* tab, int n) {
+  *nt = n;
+  if (n > 0 && tab) {
+    *tT = (double*)malloc(sizeof(double) * n);
+    *te = (double*)malloc(sizeof(double) * n);
+    *tp = (double*)malloc(sizeof(double) * n);
+    *tc = (double*)malloc(sizeof(double) * n);
+    for (int i = 0; i < n; i++) {
+      (*tT)[i] = tab[4 * i + 0];
+      (*te)[i] = tab[4 * i + 1];
+      (*tp)[i] = tab[4 * i + 2];
+      (*tc)[i] = tab[4 * i + 3];
+    }
+  }
+  ph->nt = n;
+  ph->tT = *tT;
+  ph->te = *te;
+  ph->tp = *tp;
+  ph->tc = *tc;
+}
+
+Orc* orc_create(const EchoParams* p, const double* eos_table, int n_eos) {
+  if (p->mhd && p->viscosity) return NULL;
+  if (p->mhd > 1) return NULL;
+  Orc* e = (Orc*)calloc(1, sizeof(Orc));
+  e->p = *p;
+  phys_setup(&e->ph, &e->p);
+  e->nx = p->nx;
+  e->ny = p->ny;
+  e->nz = p->nz;
+  e->nv = e->ph.nv;
+  e->nu = e->ph.nu;
+  e->nvold = p->mhd ? e->ph.kbz + 1 : KPR + 1;
+  e->ncell = (size_t)e->nx * e->ny * e->nz;
+  e->nthreads = 1;
+  /* common_grid (common.f90:441-481) */
+  e->dx = (p->x2 - p->x1) / e->nx;
+  e->dy = (p->y2 - p->y1) / e->ny;
+  e->dz = (p->z2 - p->z1) / e->nz;
+  e->ddx = e->nx > 1 ? 1. / e->dx : 0.;
+  e->ddy = e->ny > 1 ? 1. / e->dy : 0.;
+  e->ddz = e->nz > 1 ? 1. / e->dz : 0.;
+  table_attach(&e->ph, &e->tT, &e->te, &e->tp, &e->tc, &e->nt, eos_table, n_eos);
+  size_t nc = e->ncell, nv = e->nv;
+  e->v = (double*)calloc(nc * nv, sizeof(double));
+  e->u = (double*)calloc(nc * nv, sizeof(double));
+  e->u0 = (double*)calloc(nc * nv, sizeof(double));
+  int nstage = p->nrk == ECHO_SSP ? 4 : 1;
+  for (int s = 0; s < nstage; s++) {
+    e->du[s] = (double*)calloc(nc * nv, sizeof(double));
+    e->dus[s] = (double*)calloc(nc * nv, sizeof(double));
+  }
+  e->w = (double*)calloc((size_t)(e->nx + 2 * NGC) * (e->ny + 2 * NGC) * (e->nz + 2 * NGC) * nv,
+                         sizeof(double));
+  e->ax = (double*)calloc((size_t)2 * (e->nx + 1) * e->ny * e->nz, sizeof(double));
+  e->ay = (double*)calloc((size_t)2 * e->nx * (e->ny + 1) * e->nz, sizeof(double));
+  e->az = (double*)calloc((size_t)2 * e->nx * e->ny * (e->nz + 1), sizeof(double));
+  e->deriv = (double*)calloc(nc * NDERIV, sizeof(double));
+  e->vold = (double*)calloc(nc * e->nvold, sizeof(double));
+  e->vnewstep = (double*)calloc(nc * e->nvold, sizeof(double));
+  e->vtmp = (double*)calloc(nc * nv, sizeof(double));
+  e->fail = (unsigned char*)calloc(nc, 1);
+  e->glm_ch_old = 0.5; /* common.f90:283 */
+  e->tout = 1e300;
+  e->dtout = 1e300;
+  e->tmax = 1e300;
+  return e;
+}
+
+void orc_free(Orc* e) {
+  if (!e) return;
+  free(e->v); free(e->u); free(e->u0);
+  for (int s = 0; s < 4; s++) { free(e->du[s]); free(e->dus[s]); }
+  free(e->w); free(e->ax); free(e->ay); free(e->az); free(e->deriv);
+  free(e->vold); free(e->vnewstep); free(e->vtmp); free(e->fail);
+  free(e->tT); free(e->te); free(e->tp); free(e->tc);
+  free(e);
+}
+
+int orc_set_state(Orc* e, const double* v, const double* u, double t) {
+  size_t nc = e->ncell;
+  int nv = e->nv;
+  memcpy(e->v, v, sizeof(double) * nc * nv);
+  e->t = t;
+  e->timeold = t;
+  e->timeinterval = 0;
+  e->dt = 0;
+  phys_metric(&e->ph, t);
+  e->g3old = e->ph.g3;
+  memset(e->vold, 0, sizeof(double) * nc * e->nvold);
+  memset(e->vnewstep, 0, sizeof(double) * nc * e->nvold);
+  memset(e->deriv, 0, sizeof(double) * nc * NDERIV);
+  e->run_crashed = 0;
+  e->errcode = 0;
+  if (u) {
+    memcpy(e->u, u, sizeof(double) * nc * nv);
+    return 0;
+  }
+  double vv[ECHO_MAX_NV], uu[ECHO_MAX_NV];
+  for (size_t c = 0; c < nc; c++) {
+    for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
+    int err = prim2cons(&e->ph, vv, uu);
+    if (err) return err;
+    for (int k = 0; k < nv; k++) {
+      e->u[(size_t)k * nc + c] = uu[k];
+      e->v[(size_t)k * nc + c] = vv[k];
+    }
+  }
+  return 0;
+}
+
+void orc_get_state(const Orc* e, double* v, double* u) {
+  size_t n = e->ncell * e->nv;
+  if (v) memcpy(v, e->v, sizeof(double) * n);
+  if (u) memcpy(u, e->u, sizeof(double) * n);
+}
+
+void orc_set_tout(Orc* e, double tout, double dtout, double tmax) {
+  e->tout = tout;
+  e->dtout = dtout;
+  e->tmax = tmax;
+}
+
+/* ------------------------------------------------------------------------ */
+/* boundary conditions (evolve.f90:872-1127) for one direction, on w        */
+/* ------------------------------------------------------------------------ */
+static void evolve_bc(Orc* e, int dir) {
+  int n = dir == 0 ? e->nx : dir == 1 ? e->ny : e->nz;
+  const int i0 = 1, l0 = NGC;
+  int na = dir == 0 ? e->ny : e->nx; /* the two transverse ranges */
+  int nb = dir == 2 ? e->ny : e->nz;
+  for (int k = 0; k < e->nv; k++) {
+    for (int b = 1; b <= nb; b++)
+      for (int a = 1; a <= na; a++) {
+#define WP(i)                                                          \
+  e->w[dir == 0 ? WIDX(e, k, (i), a, b)                                \
+                : dir == 1 ? WIDX(e, k, a, (i), b) : WIDX(e, k, a, b, (i))]
+        int l;
+        switch (e->p.ibc[k][0][dir]) {
+          case 0:
+            for (l = 1; l <= l0; l++) WP(-NGC + l) = WP(n - NGC + l);
+            break;
+          case 1:
+            for (l = 1; l <= l0; l++) WP(-NGC + l) = WP(NGC + i0 - l);
+            break;
+          case -1:
+            for (l = 1; l <= l0; l++) WP(-NGC + l) = -WP(NGC + i0 - l);
+            break;
+          case 2:
+            for (l = 1; l <= l0; l++) WP(-NGC + l) = WP(i0);
+            break;
+          case 3:
+            for (l = 1; l <= l0; l++)
+              WP(i0 - l) = WP(i0 - l + 3) - 3. * (WP(i0 - l + 2) - WP(i0 - l + 1));
+            break;
+          default:
+            break;
+        }
+        switch (e->p.ibc[k][1][dir]) {
+          case 0:
+            for (l = 1; l <= l0; l++) WP(n + l) = WP(l);
+            break;
+          case 1:
+            for (l = 1; l <= l0; l++) WP(n + l) = WP(n + i0 - l);
+            break;
+          case -1:
+            for (l = 1; l <= l0; l++) WP(n + l) = -WP(n + i0 - l);
+            break;
+          case 2:
+            for (l = 1; l <= l0; l++) WP(n + l) = WP(n);
+            break;
+          case 3:
+            for (l = 1; l <= l0; l++)
+              WP(n + l) = WP(n + l - 3) - 3. * (WP(n + l - 2) - WP(n + l - 1));
+            break;
+          default:
+            break;
+        }
+#undef WP
+      }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* evolve_dfx/dfy/dfz (evolve.f90:302-685) with work_rec, work_glm,         */
+/* work_fup (work.f90)                                                      */
+/* ------------------------------------------------------------------------ */
+typedef struct Pencil {
+  double *w0, *wl, *wr, *w1, *wd, *wdl, *wdr;
+  int len;
+} Pencil;
+
+static void pencil_alloc(Pencil* pc, int nmax, int nv) {
+  pc->len = nmax + 2 * PADP + 2;
+  size_t L = (size_t)pc->len;
+  pc->w0 = (double*)calloc(L * nv, sizeof(double));
+  pc->wl = (double*)calloc(L * nv, sizeof(double));
+  pc->wr = (double*)calloc(L * nv, sizeof(double));
+  pc->w1 = (double*)calloc(L * (nv + 2), sizeof(double));
+  pc->wd = (double*)calloc(L * 4, sizeof(double));
+  pc->wdl = (double*)calloc(L * 4, sizeof(double));
+  pc->wdr = (double*)calloc(L * 4, sizeof(double));
+}
+static void pencil_free(Pencil* pc) {
+  free(pc->w0); free(pc->wl); free(pc->wr); free(pc->w1);
+  free(pc->wd); free(pc->wdl); free(pc->wdr);
+}
+#define PIX(pc, k, i) ((size_t)(k) * (pc)->len + (size_t)((i) + PADP))
+
+/* one pencil: returns the work_fup error code, writes aflux_last */
+static int do_pencil(Orc* e, Pencil* pc, int dir, int a, int b, int iteration,
+                     double* aflux_last) {
+  const Phys* ph = &e->ph;
+  const EchoParams* p = &e->p;
+  int n = dir == 0 ? e->nx : dir == 1 ? e->ny : e->nz;
+  int nv = e->nv;
+  double dd = dir == 0 ? e->ddx : dir == 1 ? e->ddy : e->ddz;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3;
+  int i, k;
+#define WG(k, i)                                                        \
+  e->w[dir == 0 ? WIDX(e, k, (i), a, b)                                 \
+                : dir == 1 ? WIDX(e, k, a, (i), b) : WIDX(e, k, a, b, (i))]
+#define CELL(i) (dir == 0 ? IDX(e, 0, (i), a, b) : dir == 1 ? IDX(e, 0, a, (i), b) : IDX(e, 0, a, b, (i)))
+  for (k = 0; k < nv; k++)
+    for (i = 1 - NGC; i <= n + NGC; i++) pc->w0[PIX(pc, k, i)] = WG(k, i);
+  if (p->viscosity) {
+    for (i = 1 - NGC; i <= n + NGC; i++) {
+      double vx = WG(KVX, i), vy = WG(KVY, i), vz = WG(KVZ, i);
+      double g = 1. / sqrt(1. - vx * vx - vy * vy - g3 * (vz * vz));
+      pc->wd[PIX(pc, 0, i)] = g;
+      pc->wd[PIX(pc, 1, i)] = g * vx;
+      pc->wd[PIX(pc, 2, i)] = g * vy;
+      pc->wd[PIX(pc, 3, i)] = g * vz;
+    }
+  }
+  /* work_rec(n,1,nv,0) and work_rec(n,1,4,1) */
+  for (k = 0; k < nv; k++)
+    rec_pencil(p->recal, pc->w0 + PIX(pc, k, 0), pc->wl + PIX(pc, k, 0),
+               pc->wr + PIX(pc, k, 0), n);
+  if (p->viscosity)
+    for (k = 0; k < 4; k++)
+      rec_pencil(p->recal, pc->wd + PIX(pc, k, 0), pc->wdl + PIX(pc, k, 0),
+                 pc->wdr + PIX(pc, k, 0), n);
+  /* fix-ups of evolve.f90:334-369 */
+  for (i = 0; i <= n; i++) {
+    double v2;
+    if (pc->wr[PIX(pc, KPR, i)] <= 0) pc->wr[PIX(pc, KPR, i)] = pc->w0[PIX(pc, KPR, i)];
+    v2 = 0;
+    v2 = v2 + pc->wr[PIX(pc, KVX, i)] * pc->wr[PIX(pc, KVX, i)] * g1;
+    v2 = v2 + pc->wr[PIX(pc, KVY, i)] * pc->wr[PIX(pc, KVY, i)] * g2;
+    v2 = v2 + pc->wr[PIX(pc, KVZ, i)] * pc->wr[PIX(pc, KVZ, i)] * g3;
+    if (v2 >= 1.) {
+      for (k = KVX; k <= KVZ; k++) pc->wr[PIX(pc, k, i)] = pc->w0[PIX(pc, k, i)];
+      v2 = 0;
+      v2 = v2 + pc->wr[PIX(pc, KVX, i)] * pc->wr[PIX(pc, KVX, i)] * g1;
+      v2 = v2 + pc->wr[PIX(pc, KVY, i)] * pc->wr[PIX(pc, KVY, i)] * g2;
+      v2 = v2 + pc->wr[PIX(pc, KVZ, i)] * pc->wr[PIX(pc, KVZ, i)] * g3;
+      if (v2 >= 1) {
+        for (k = KVX; k <= KVZ; k++) {
+          pc->w0[PIX(pc, k, i)] = pc->w0[PIX(pc, k, i)] * p->maxspeed / (sqrt(v2));
+          pc->wr[PIX(pc, k, i)] = pc->w0[PIX(pc, k, i)];
+        }
+      }
+    }
+    if (pc->wl[PIX(pc, KPR, i)] <= 0) pc->wl[PIX(pc, KPR, i)] = pc->w0[PIX(pc, KPR, i)];
+    v2 = 0;
+    v2 = v2 + pc->wl[PIX(pc, KVX, i)] * pc->wl[PIX(pc, KVX, i)] * g1;
+    v2 = v2 + pc->wl[PIX(pc, KVY, i)] * pc->wl[PIX(pc, KVY, i)] * g2;
+    v2 = v2 + pc->wl[PIX(pc, KVZ, i)] * pc->wl[PIX(pc, KVZ, i)] * g3;
+    if (v2 >= 1.) {
+      for (k = KVX; k <= KVZ; k++) pc->wl[PIX(pc, k, i)] = pc->w0[PIX(pc, k, i)];
+      v2 = 0;
+      v2 = v2 + pc->wl[PIX(pc, KVX, i)] * pc->wl[PIX(pc, KVX, i)] * g1;
+      v2 = v2 + pc->wl[PIX(pc, KVY, i)] * pc->wl[PIX(pc, KVY, i)] * g2;
+      v2 = v2 + pc->wl[PIX(pc, KVZ, i)] * pc->wl[PIX(pc, KVZ, i)] * g3;
+      if (v2 >= 1) {
+        for (k = KVX; k <= KVZ; k++) {
+          pc->w0[PIX(pc, k, i)] = pc->w0[PIX(pc, k, i)] * p->maxspeed / (sqrt(v2));
+          pc->wl[PIX(pc, k, i)] = pc->w0[PIX(pc, k, i)];
+        }
+      }
+    }
+  }
+  /* derivatives of u^mu (evolve.f90:371-374) */
+  if (p->viscosity) {
+    int dt_ = dir == 0 ? DTX : dir == 1 ? DTY : DTZ;
+    int dxk = dir == 0 ? DXX : dir == 1 ? DXY : DXZ;
+    int dyk = dir == 0 ? DYX : dir == 1 ? DYY : DYZ;
+    int dzk = dir == 0 ? DZX : dir == 1 ? DZY : DZZ;
+    int dk[4] = {dt_, dxk, dyk, dzk};
+    for (int c = 0; c < 4; c++)
+      for (i = 1; i <= n; i++)
+        e->deriv[(size_t)dk[c] * e->ncell + CELL(i)] =
+            dd * 0.5 * (pc->wdl[PIX(pc, c, i)] + pc->wdr[PIX(pc, c, i)] - pc->wdl[PIX(pc, c, i - 1)] - pc->wdr[PIX(pc, c, i - 1)]);
+  }
+  /* work_glm[xyz] (work.f90:67-139) */
+  if (p->divclean) {
+    int kb = dir == 0 ? ph->kbx : dir == 1 ? ph->kby : ph->kbz, kg = ph->kglm;
+    double ch = e->glm_ch;
+    for (i = 0; i <= n; i++) {
+      pc->wl[PIX(pc, kg, i)] = 0.5 * (pc->wl[PIX(pc, kg, i)] + pc->wr[PIX(pc, kg, i)]) -
+                               (pc->wr[PIX(pc, kb, i)] - pc->wl[PIX(pc, kb, i)]) * ch / 2;
+      pc->wr[PIX(pc, kg, i)] = pc->wl[PIX(pc, kg, i)];
+      pc->wl[PIX(pc, kb, i)] = 0.5 * (pc->wl[PIX(pc, kb, i)] + pc->wr[PIX(pc, kb, i)]) -
+                               (pc->wr[PIX(pc, kg, i)] - pc->wl[PIX(pc, kg, i)]) / (2 * ch);
+      pc->wr[PIX(pc, kb, i)] = pc->wl[PIX(pc, kb, i)];
+    }
+  }
+  /* work_fup[xyz], HLL (work.f90:195-229) */
+  int errc = 0;
+  for (i = 0; i <= n; i++) {
+    double vl[ECHO_MAX_NV], vr[ECHO_MAX_NV], ul[ECHO_MAX_NV], ur[ECHO_MAX_NV],
+        fl[ECHO_MAX_NV], fr[ECHO_MAX_NV], vfl[2], vfr[2];
+    for (k = 0; k < nv; k++) {
+      vl[k] = pc->wl[PIX(pc, k, i)];
+      vr[k] = pc->wr[PIX(pc, k, i)];
+    }
+    errc = system_flux(ph, vl, ul, fl, vfl, dir + 1);
+    if (errc) break;
+    errc = system_flux(ph, vr, ur, fr, vfr, dir + 1);
+    if (errc) break;
+    double ap = 0., am = 0.;
+    if (vfl[0] > ap) ap = vfl[0];
+    if (vfr[0] > ap) ap = vfr[0];
+    if (-vfl[1] > am) am = -vfl[1];
+    if (-vfr[1] > am) am = -vfr[1];
+    *aflux_last = ap > am ? ap : am;
+    double a1 = (ap == 0.0 && am == 0.0) ? 1. : 1. / (ap + am);
+    for (k = 0; k < nv; k++)
+      pc->w1[PIX(pc, k, i)] = a1 * (ap * fl[k] + am * fr[k] - ap * am * (ur[k] - ul[k]));
+    pc->w1[PIX(pc, nv, i)] = ap;
+    pc->w1[PIX(pc, nv + 1, i)] = am;
+  }
+  /* du += dd*(w1(i)-w1(i-1)) (evolve.f90:382-384) and ax/ay/az */
+  double* du = e->du[iteration - 1];
+  for (k = 0; k < e->nu; k++)
+    for (i = 1; i <= n; i++) {
+      size_t c = CELL(i) + (size_t)k * e->ncell;
+      du[c] = du[c] + dd * (pc->w1[PIX(pc, k, i)] - pc->w1[PIX(pc, k, i - 1)]);
+    }
+  for (i = 0; i <= n; i++)
+    for (int s = 0; s < 2; s++) {
+      double a_ = pc->w1[PIX(pc, nv + s, i)];
+      if (dir == 0)
+        e->ax[(((size_t)s * e->nz + (b - 1)) * e->ny + (a - 1)) * (e->nx + 1) + i] = a_;
+      else if (dir == 1)
+        e->ay[(((size_t)s * e->nz + (b - 1)) * (e->ny + 1) + i) * e->nx + (a - 1)] = a_;
+      else
+        e->az[(((size_t)s * (e->nz + 1) + i) * e->ny + (b - 1)) * e->nx + (a - 1)] = a_;
+    }
+#undef WG
+#undef CELL
+  return errc;
+}
+
+static int evolve_df(Orc* e, int dir, int iteration) {
+  int n = dir == 0 ? e->nx : dir == 1 ? e->ny : e->nz;
+  if (n <= 1) return 0;
+  int nv = e->nv;
+  /* w(interior) = v */
+  for (int k = 0; k < nv; k++)
+    for (int iz = 1; iz <= e->nz; iz++)
+      for (int iy = 1; iy <= e->ny; iy++)
+        for (int ix = 1; ix <= e->nx; ix++)
+          e->w[WIDX(e, k, ix, iy, iz)] = e->v[IDX(e, k, ix, iy, iz)];
+  evolve_bc(e, dir);
+  int na = dir == 0 ? e->ny : e->nx;
+  int nb = dir == 2 ? e->ny : e->nz;
+  int nmax = e->nx > e->ny ? e->nx : e->ny;
+  if (e->nz > nmax) nmax = e->nz;
+  int err = 0;
+  double af_last = e->aflux[dir];
+  int nth = e->nthreads;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nth)
+#endif
+  {
+    Pencil pc;
+    pencil_alloc(&pc, nmax, nv);
+#ifdef _OPENMP
+#pragma omp for schedule(static) collapse(2)
+#endif
+    for (int b = 1; b <= nb; b++)
+      for (int a = 1; a <= na; a++) {
+        double af = 0;
+        int ec = do_pencil(e, &pc, dir, a, b, iteration, &af);
+        if (a == na && b == nb) {
+          af_last = af;
+          err = ec;
+        } else if (ec) {
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+          { if (!e->run_crashed) e->run_crashed = ec; }
+        }
+      }
+    pencil_free(&pc);
+  }
+  (void)nth;
+  e->aflux[dir] = af_last;
+  if (err) {
+    e->errcode = err;
+    e->run_crashed = 1;
+  } else if (e->run_crashed) {
+    /* system_flux sets run_crashed itself on any face (system.f90:1346,1355) */
+    e->errcode = e->run_crashed;
+    e->run_crashed = 1;
+  }
+  return e->run_crashed ? e->errcode : 0;
+}
+
+/* dts (viscous.f90:56-97) */
+static void evolve_dts(Orc* e) {
+  size_t nc = e->ncell;
+  if (e->timeinterval == 0) {
+    for (int d = DTT; d <= DZT; d++)
+      for (size_t c = 0; c < nc; c++) e->deriv[(size_t)d * nc + c] = 0.;
+    return;
+  }
+  double g1 = e->ph.g1, g2 = e->ph.g2, g3 = e->ph.g3, ti = e->timeinterval;
+  for (size_t c = 0; c < nc; c++) {
+    double vxo = e->vold[1 * nc + c], vyo = e->vold[2 * nc + c], vzo = e->vold[3 * nc + c];
+    double vx = e->vnewstep[1 * nc + c], vy = e->vnewstep[2 * nc + c], vz = e->vnewstep[3 * nc + c];
+    double gamma1 = 1. / sqrt(1. - g1 * (vxo * vxo) - g2 * (vyo * vyo) - e->g3old * (vzo * vzo));
+    double gamma2 = 1. / sqrt(1. - g1 * (vx * vx) - g2 * (vy * vy) - g3 * (vz * vz));
+    e->deriv[(size_t)DTT * nc + c] = (gamma2 - gamma1) / (ti);
+    e->deriv[(size_t)DXT * nc + c] = (gamma2 * vx - gamma1 * vxo) / ti;
+    e->deriv[(size_t)DYT * nc + c] = (gamma2 * vy - gamma1 * vyo) / ti;
+    e->deriv[(size_t)DZT * nc + c] = (gamma2 * vz - gamma1 * vzo) / ti;
+  }
+}
+
+/* evolve_src (evolve.f90:689-718) */
+static int evolve_src(Orc* e, int iteration) {
+  size_t nc = e->ncell;
+  int nv = e->nv;
+  if (e->p.viscosity) evolve_dts(e);
+  int err = 0;
+  double* du = e->du[iteration - 1];
+  for (size_t c = 0; c < nc && !err; c++) {
+    double vv[ECHO_MAX_NV], src[ECHO_MAX_NV], dv[NDERIV];
+    for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
+    if (e->p.viscosity)
+      for (int d = 0; d < NDERIV; d++) dv[d] = e->deriv[(size_t)d * nc + c];
+    int ec = system_source(&e->ph, vv, dv, src);
+    if (ec) {
+      err = ec;
+      break;
+    }
+    for (int k = 0; k < e->nu; k++) du[(size_t)k * nc + c] = du[(size_t)k * nc + c] - src[k];
+  }
+  if (err) {
+    e->errcode = err;
+    e->run_crashed = 1;
+  }
+  return err;
+}
+
+/* evolve_dt (evolve.f90:723-764) */
+static double evolve_dt(Orc* e) {
+  double amax;
+  if (e->p.divclean) {
+    amax = 1;
+  } else {
+    amax = 0.;
+    int nx = e->nx, ny = e->ny, nz = e->nz;
+    for (int iz = 1; iz <= nz; iz++)
+      for (int iy = 1; iy <= ny; iy++)
+        for (int ix = 1; ix <= nx; ix++) {
+          double m, c;
+          if (nx > 1) {
+            m = -INFINITY;
+            for (int s = 0; s < 2; s++)
+              for (int i = ix - 1; i <= ix; i++) {
+                c = e->ax[(((size_t)s * nz + (iz - 1)) * ny + (iy - 1)) * (nx + 1) + i];
+                if (c > m) m = c;
+              }
+            c = e->ddx * m;
+            if (c > amax) amax = c;
+          }
+          if (ny > 1) {
+            m = -INFINITY;
+            for (int s = 0; s < 2; s++)
+              for (int i = iy - 1; i <= iy; i++) {
+                c = e->ay[(((size_t)s * nz + (iz - 1)) * (ny + 1) + i) * nx + (ix - 1)];
+                if (c > m) m = c;
+              }
+            c = e->ddy * m;
+            if (c > amax) amax = c;
+          }
+          if (nz > 1) {
+            m = -INFINITY;
+            for (int s = 0; s < 2; s++)
+              for (int i = iz - 1; i <= iz; i++) {
+                c = e->az[(((size_t)s * (nz + 1) + i) * ny + (iy - 1)) * nx + (ix - 1)];
+                if (c > m) m = c;
+              }
+            c = e->ddz * m;
+            if (c > amax) amax = c;
+          }
+        }
+    if (amax == 0) {
+      if (nx > 1 && e->ddx > amax) amax = e->ddx;
+      if (ny > 1 && e->ddy > amax) amax = e->ddy;
+      if (nz > 1 && e->ddz > amax) amax = e->ddz;
+    }
+  }
+  return e->p.cfl / amax;
+}
+
+/* evolve_u2v (evolve.f90:769-868) with the repair path of :795-842 */
+static double flat_get(const double* a, size_t total, long long off) {
+  if (off < 0 || (size_t)off >= total) return 0.;
+  return a[off];
+}
+
+static int evolve_u2v(Orc* e) {
+  const Phys* ph = &e->ph;
+  size_t nc = e->ncell;
+  int nv = e->nv, nu = e->nu;
+  int nx = e->nx, ny = e->ny, nz = e->nz;
+  long long c2p = 0;
+  /* pass 1: every cell independently (vtmp = new v, fail = flag); the
+   * Fortran loop gives the same result because a cell's inversion reads
+   * only its own u and its own old v */
+  memset(e->fail, 0, nc);
+  int nth = e->nthreads;
+  (void)nth;
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nth) schedule(static) reduction(+ : c2p)
+#endif
+  for (long long c = 0; c < (long long)nc; c++) {
+    double uu[ECHO_MAX_NV], vv[ECHO_MAX_NV];
+    for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
+    for (int k = 0; k < nu; k++) uu[k] = e->u[(size_t)k * nc + c];
+    int it = 0;
+    int err = cons2prim(ph, uu, vv, &it);
+    c2p += it;
+    if (err) {
+      e->fail[c] = 1;
+    } else {
+      for (int k = 0; k < nv; k++) e->vtmp[(size_t)k * nc + c] = vv[k];
+    }
+  }
+  e->c2p_iters = c2p;
+  /* pass 2: the failing cells in Fortran loop order; neighbours earlier in
+   * the loop already hold their new v, later ones still the old v */
+  for (int iz = 1; iz <= nz; iz++)
+    for (int iy = 1; iy <= ny; iy++)
+      for (int ix = 1; ix <= nx; ix++) {
+        size_t c = IDX(e, 0, ix, iy, iz);
+        if (!e->fail[c]) {
+          for (int k = 0; k < nv; k++) e->v[(size_t)k * nc + c] = e->vtmp[(size_t)k * nc + c];
+          continue;
+        }
+        double uu[ECHO_MAX_NV], vv[ECHO_MAX_NV], g3 = ph->g3;
+        int it;
+        e->repairs++;
+        for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
+        for (int k = 0; k < nu; k++) uu[k] = e->u[(size_t)k * nc + c];
+        (void)cons2prim(ph, uu, vv, &it); /* the failed call, for its side effects on vv */
+        size_t totu = nc * nu, totv = nc * nv;
+        for (int k = 0; k < nu; k++) {
+          long long base = (long long)k * nc;
+          long long o = (long long)(ix - 1) + (long long)nx * ((iy - 1) + (long long)ny * (iz - 1));
+          double s = flat_get(e->u, totu, base + o - 1) + flat_get(e->u, totu, base + o + 1) +
+                     flat_get(e->u, totu, base + o - nx) + flat_get(e->u, totu, base + o + nx) +
+                     flat_get(e->u, totu, base + o - (long long)nx * ny) +
+                     flat_get(e->u, totu, base + o + (long long)nx * ny);
+          e->u[(size_t)k * nc + c] = s / 6.;
+          uu[k] = e->u[(size_t)k * nc + c];
+        }
+        (void)cons2prim(ph, uu, vv, &it);
+        double v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * g3;
+        if (v2 > 1) {
+          double fac = e->p.maxspeed / sqrt(v2);
+          vv[KVX] = fac * vv[KVX];
+          vv[KVY] = fac * vv[KVY];
+          vv[KVZ] = fac * vv[KVZ];
+        }
+        if (vv[KPR] < 0) {
+          long long base = (long long)KPR * nc;
+          long long o = (long long)(ix - 1) + (long long)nx * ((iy - 1) + (long long)ny * (iz - 1));
+          double pxl = flat_get(e->v, totv, base + o - 1), pxr = flat_get(e->v, totv, base + o + 1);
+          double pyl = flat_get(e->v, totv, base + o - nx), pyr = flat_get(e->v, totv, base + o + nx);
+          double pzl = flat_get(e->v, totv, base + o - (long long)nx * ny);
+          double pzr = flat_get(e->v, totv, base + o + (long long)nx * ny);
+          vv[KPR] = (pxl + pxr + pyl + pyr + pzl + pzr) / 6.;
+        }
+        (void)prim2cons(ph, vv, uu);
+        int err = cons2prim(ph, uu, vv, &it);
+        (void)err;
+        v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * g3;
+        int ok = (vv[KPR] > 0) && (v2 < 1);
+        if (e->p.viscosity && e->p.obtained_zz) e->v[(size_t)KPIZZ * nc + c] = vv[KPIZZ];
+        for (int k = 0; k < nu; k++) e->u[(size_t)k * nc + c] = uu[k];
+        if (!ok) {
+          e->errcode = 1;
+          e->run_crashed = 1;
+          return 1;
+        }
+        for (int k = 0; k < nv; k++) e->v[(size_t)k * nc + c] = vv[k];
+      }
+  return 0;
+}
+
+/* evolve_smooth_viscosity (evolve.f90:1159-1207) */
+static int evolve_smooth_viscosity(Orc* e) {
+  const Phys* ph = &e->ph;
+  size_t nc = e->ncell;
+  int nv = e->nv;
+  double ps = e->p.smooth_pressure;
+  for (size_t c = 0; c < nc; c++) {
+    double pr = e->v[(size_t)KPR * nc + c];
+    if (pr < ps) {
+      double vv[ECHO_MAX_NV], uu[ECHO_MAX_NV];
+      for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
+      double r = vv[KPR] / ps;
+      double fac = r * r;
+      for (int k = KPIBU; k <= KPIZZ; k++) vv[k] = vv[k] * fac;
+      if (e->p.obtained_zz) {
+        Pit pi;
+        derived_pi_zz(ph, vv, &pi);
+        vv[KPIZZ] = pi.zz;
+      }
+      int err = prim2cons(ph, vv, uu);
+      for (int k = 0; k < nv; k++) {
+        e->v[(size_t)k * nc + c] = vv[k];
+        e->u[(size_t)k * nc + c] = uu[k];
+      }
+      if (err) {
+        e->errcode = err;
+        e->run_crashed = 1;
+        return err;
+      }
+    }
+  }
+  return 0;
+}
+
+static void glm_source(Orc* e, double dt_glm) { /* evolve.f90:83-110 */
+  double expfact = exp(-e->glm_ch * e->glm_ch * e->p.glm_alpha * dt_glm);
+  size_t nc = e->ncell;
+  double* ug = e->u + (size_t)e->ph.kglm * nc;
+  for (size_t c = 0; c < nc; c++) ug[c] = ug[c] * expfact;
+}
+
+static int rhs_all(Orc* e, int iteration) {
+  double* du = e->du[iteration - 1];
+  memset(du, 0, sizeof(double) * e->ncell * e->nv);
+  if (e->dus[iteration - 1]) memset(e->dus[iteration - 1], 0, sizeof(double) * e->ncell * e->nv);
+  e->glm_ch = e->glm_ch_old;
+  if (evolve_df(e, 0, iteration)) return e->errcode;
+  if (evolve_df(e, 1, iteration)) return e->errcode;
+  if (evolve_df(e, 2, iteration)) return e->errcode;
+  if (evolve_src(e, iteration)) return e->errcode;
+  double m = e->aflux[0];
+  if (e->aflux[1] > m) m = e->aflux[1];
+  if (e->aflux[2] > m) m = e->aflux[2];
+  e->glm_ch_old = m;
+  return 0;
+}
+
+static double dt_clip(Orc* e, double dt_local) { /* evolve.f90:181-188 */
+  if (e->p.maxdt < dt_local) dt_local = e->p.maxdt;
+  if (e->tout - e->t < dt_local) dt_local = e->tout - e->t;
+  if (fabs(e->t + e->dt - e->tout) < 1.e-9) {
+    dt_local = e->tout - e->t;
+  } else {
+    if ((e->t + 2. * dt_local - e->tout) > 1.e-9) dt_local = (e->tout - e->t) / 2.;
+  }
+  return dt_local;
+}
+
+/* evolve_main (evolve.f90:114-298) */
+int orc_evolve_main(Orc* e, int irk, double* dt_out) {
+  size_t n = e->ncell * e->nv;
+  int nu = e->nu;
+  (void)nu;
+  if (e->p.nrk != ECHO_SSP) {
+    static const double crk[3][3][2] = {
+        {{0., 1.}, {0., 0.}, {0., 0.}},
+        {{0., 1.}, {1. / 2., 1. / 2.}, {0., 0.}},
+        {{0., 1.}, {3. / 4., 1. / 4.}, {1. / 3., 2. / 3.}}};
+    double c1 = crk[e->p.nrk - 1][irk - 1][0], c2 = crk[e->p.nrk - 1][irk - 1][1];
+    if (rhs_all(e, 1)) return e->errcode;
+    if (irk == 1) {
+      double dtl = dt_clip(e, evolve_dt(e));
+      e->dt = dtl;
+      if (e->p.divclean) glm_source(e, e->dt / 2.);
+      memcpy(e->u0, e->u, sizeof(double) * n);
+    }
+    double dt = e->dt, *du = e->du[0];
+    for (size_t i = 0; i < n; i++) e->u[i] = c1 * e->u0[i] + c2 * (e->u[i] - dt * du[i]);
+    if (e->p.divclean && irk == e->p.nrk) glm_source(e, dt / 2.);
+    if (evolve_u2v(e)) return e->errcode;
+  } else {
+    const double alpha_imex = 0.24169426078821, beta_imex = 0.06042356519705,
+                 eta_imex = 0.12915286960590;
+    const double delta_imex = 0.5 - beta_imex - eta_imex - alpha_imex;
+    double dt;
+    if (irk == 1) {
+      double dtl = dt_clip(e, evolve_dt(e));
+      e->dt = dtl;
+      memcpy(e->u0, e->u, sizeof(double) * n);
+      if (rhs_all(e, 1)) return e->errcode;
+      if (e->p.divclean) glm_source(e, e->dt / 2.);
+    } else if (irk == 2) {
+      dt = e->dt;
+      for (size_t i = 0; i < n; i++) e->u[i] = e->u0[i] + dt * alpha_imex * e->dus[0][i];
+      if (evolve_u2v(e)) return e->errcode;
+      if (rhs_all(e, 2)) return e->errcode;
+    } else if (irk == 3) {
+      dt = e->dt;
+      for (size_t i = 0; i < n; i++)
+        e->u[i] = e->u0[i] - dt * (e->du[1][i] + (1. - alpha_imex) * e->dus[1][i]);
+      if (evolve_u2v(e)) return e->errcode;
+      if (rhs_all(e, 3)) return e->errcode;
+    } else {
+      dt = e->dt;
+      for (size_t i = 0; i < n; i++)
+        e->u[i] = e->u0[i] - dt * (e->du[1][i] / 4. + e->du[2][i] / 4. + beta_imex * e->dus[0][i] +
+                                   eta_imex * e->dus[1][i] + delta_imex * e->dus[2][i]);
+      if (evolve_u2v(e)) return e->errcode;
+      if (rhs_all(e, 4)) return e->errcode;
+      for (size_t i = 0; i < n; i++)
+        e->u[i] = e->u0[i] - dt * (e->du[1][i] / 6. + e->du[2][i] / 6. + e->du[3][i] * 2. / 3. +
+                                   e->dus[1][i] / 6. + e->dus[2][i] / 6. + e->dus[3][i] * 2. / 3.);
+      if (e->p.divclean) glm_source(e, dt / 2.);
+      if (evolve_u2v(e)) return e->errcode;
+    }
+  }
+  if (e->p.viscosity && e->p.enable_smooth_viscosity)
+    if (evolve_smooth_viscosity(e)) return e->errcode;
+  if (dt_out) *dt_out = e->dt;
+  return 0;
+}
+
+/* echo.f90:185-262 without output */
+int orc_step(Orc* e, double* dt_out) {
+  size_t nc = e->ncell;
+  memcpy(e->vnewstep, e->v, sizeof(double) * nc * e->nvold);
+  int nstage = e->p.nrk == ECHO_SSP ? 4 : e->p.nrk;
+  for (int irk = 1; irk <= nstage; irk++) {
+    int err = orc_evolve_main(e, irk, NULL);
+    if (err) return err;
+  }
+  e->timeold = e->t;
+  e->t = e->t + e->dt;
+  e->g3old = e->ph.g3;
+  phys_metric(&e->ph, e->t);
+  e->timeinterval = e->dt;
+  memcpy(e->vold, e->vnewstep, sizeof(double) * nc * e->nvold);
+  if ((e->t > e->tout) || ((e->tout - e->t) < 1.e-10)) {
+    e->tout = e->tout + e->dtout;
+    if ((fabs(e->tout - e->tmax) < 1.e-10) || (e->tout > e->tmax)) e->tout = e->tmax;
+  }
+  if (dt_out) *dt_out = e->dt;
+  return 0;
+}
+
+int orc_rhs(Orc* e, double* du, double* amax3) {
+  int err = rhs_all(e, 1);
+  if (du) memcpy(du, e->du[0], sizeof(double) * e->ncell * e->nv);
+  if (amax3) {
+    int nx = e->nx, ny = e->ny, nz = e->nz;
+    double m[3] = {0, 0, 0};
+    size_t na = (size_t)2 * (nx + 1) * ny * nz, nb = (size_t)2 * nx * (ny + 1) * nz,
+           nn = (size_t)2 * nx * ny * (nz + 1);
+    for (size_t i = 0; i < na; i++) if (e->ax[i] > m[0]) m[0] = e->ax[i];
+    for (size_t i = 0; i < nb; i++) if (e->ay[i] > m[1]) m[1] = e->ay[i];
+    for (size_t i = 0; i < nn; i++) if (e->az[i] > m[2]) m[2] = e->az[i];
+    amax3[0] = m[0]; amax3[1] = m[1]; amax3[2] = m[2];
+  }
+  return err;
+}
+
+/* ------------------------------------------------------------------------ */
+/* pointwise entry points for unit tests                                    */
+/* ------------------------------------------------------------------------ */
+static void unit_phys(Phys* ph, const EchoParams* p, double g3, double gp,
+                      const double* tab, int n, double** bufs) {
+  phys_setup(ph, p);
+  ph->g1 = 1.;
+  ph->g2 = 1.;
+  ph->g3 = g3;
+  ph->gp = gp;
+  ph->gm = 1. / gp;
+  ph->t = gp;
+  int nt;
+  table_attach(ph, &bufs[0], &bufs[1], &bufs[2], &bufs[3], &nt, tab, n);
+}
+
+int orc_c2p(const EchoParams* p, const double* tab, int n_eos, int ncells,
+            double g3, double gp, const double* u, double* v, int* err,
+            int* iters) {
+  Phys ph;
+  double* bufs[4] = {0, 0, 0, 0};
+  unit_phys(&ph, p, g3, gp, tab, n_eos, bufs);
+  int nv = ph.nv;
+  for (int c = 0; c < ncells; c++) {
+    double uu[ECHO_MAX_NV];
+    for (int k = 0; k < nv; k++) uu[k] = u[(size_t)c * nv + k];
+    int it = 0;
+    int e = cons2prim(&ph, uu, v + (size_t)c * nv, &it);
+    if (err) err[c] = e;
+    if (iters) iters[c] = it;
+  }
+  for (int i = 0; i < 4; i++) free(bufs[i]);
+  return nv;
+}
+
+int orc_prim2cons(const EchoParams* p, const double* tab, int n_eos,
+                  int ncells, double g3, double gp, double* v, double* u) {
+  Phys ph;
+  double* bufs[4] = {0, 0, 0, 0};
+  unit_phys(&ph, p, g3, gp, tab, n_eos, bufs);
+  int nv = ph.nv, bad = 0;
+  for (int c = 0; c < ncells; c++)
+    if (prim2cons(&ph, v + (size_t)c * nv, u + (size_t)c * nv)) bad++;
+  for (int i = 0; i < 4; i++) free(bufs[i]);
+  return bad;
+}
+
+int orc_flux(const EchoParams* p, const double* tab, int n_eos, double g3,
+             double gp, int dir, double* v, double* u, double* f, double* vf) {
+  Phys ph;
+  double* bufs[4] = {0, 0, 0, 0};
+  unit_phys(&ph, p, g3, gp, tab, n_eos, bufs);
+  int r = system_flux(&ph, v, u, f, vf, dir);
+  for (int i = 0; i < 4; i++) free(bufs[i]);
+  return r;
+}
