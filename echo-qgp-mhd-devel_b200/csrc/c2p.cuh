@@ -1,0 +1,643 @@
+// c2p.cuh -- conserved -> primitive inversion on the device
+// (system_cons2prim, system.f90:423-1166) and the per-cell source terms
+// (system_source, system.f90:1587-1842; get_sigma, viscous.f90:283-393).
+#pragma once
+
+#include "physics.cuh"
+
+namespace echo {
+
+// ---------------------------------------------------------------------------
+// BRENTM (libacm554.f90:8-362) on the 3x3 system sist3 (system.f90:1199-1231)
+// ---------------------------------------------------------------------------
+struct Sist3 {
+  double B2, SB2, S2, U, D;
+};
+
+__device__ __forceinline__ double sist3_f(const DevPhys& P, const Sist3& s, const double* X, int K) {
+  double xx = X[0], yy = X[1], pp = X[2];
+  if (K == 1) return (yy + s.B2) * (yy + s.B2) * xx - s.SB2 / (yy * yy) * (2 * yy + s.B2) - s.S2;
+  if (K == 2) return yy - pp + 0.5 * (1. + xx) * s.B2 - 0.5 * s.SB2 / (yy * yy) - s.U;
+  double rh = s.D * sqrt(1 - xx), en = 0;
+  (void)eos_energy(P, rh, &en, pp);  // errcode ignored (system.f90:1227)
+  return yy - (pp + en) / (1 - xx);
+}
+
+__device__ __forceinline__ double dmax1(double a, double b) { return b > a ? b : a; }
+
+// Returns INFO; X in/out; *nfev = NFEV.  MAXFEV bounds the iteration count.
+static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, double FTOL, double XTOL, int MAXFEV,
+                       int MOPT, int* nfev_out) {
+  const int N = 3;
+  double Q[9], SIGMA[3], WA1[3], WA2[3];
+#define QQ(i, j) Q[((j)-1) * 3 + ((i)-1)]
+  int NFCALL = 0, NIER6 = -1, NIER7 = -1, NIER8 = 0, NSING, INFO = 0, NFEV = 0;
+  bool CONV;
+  double DELTA, DIFIT = 0., DIFIT1, EPS, FKY, FKZ, FNORM = 0., FNORM1, H, SKNORM, TEMP, XNORM = 0., ETA;
+  const double ZERO = 0.0, P05 = 5.0e-2, SCALE = 1.0e1;
+  const double EPSMCH = 2.220446049250313080847e-16;
+  for (int I = 1; I <= N; I++) XNORM = dmax1(XNORM, fabs(X[I - 1]));
+  EPS = sqrt(EPSMCH);
+  DELTA = SCALE * XNORM;
+  if (XNORM == ZERO) DELTA = SCALE;
+  for (;;) {
+    NSING = N;
+    FNORM1 = FNORM;
+    DIFIT1 = DIFIT;
+    FNORM = ZERO;
+    H = EPS * XNORM;
+    if (H == ZERO) H = EPS;
+#pragma unroll
+    for (int J = 1; J <= N; J++) {
+#pragma unroll
+      for (int I = 1; I <= N; I++) QQ(I, J) = ZERO;
+      QQ(J, J) = H;
+      WA1[J - 1] = X[J - 1];
+    }
+#pragma unroll
+    for (int K = 1; K <= N; K++) {
+      FKY = sist3_f(P, s, WA1, K);
+      NFCALL = NFCALL + 1;
+      NFEV = NFCALL / N;
+      FNORM = dmax1(FNORM, fabs(FKY));
+#pragma unroll
+      for (int J = K; J <= N; J++) {
+#pragma unroll
+        for (int I = 1; I <= N; I++) WA2[I - 1] = WA1[I - 1] + QQ(I, J);
+        FKZ = sist3_f(P, s, WA2, K);
+        NFCALL = NFCALL + 1;
+        NFEV = NFCALL / N;
+        SIGMA[J - 1] = FKZ - FKY;
+      }
+      ETA = ZERO;
+#pragma unroll
+      for (int I = K; I <= N; I++) ETA = dmax1(ETA, fabs(SIGMA[I - 1]));
+      if (ETA == ZERO) continue;
+      NSING = NSING - 1;
+      SKNORM = ZERO;
+#pragma unroll
+      for (int I = K; I <= N; I++) {
+        SIGMA[I - 1] = SIGMA[I - 1] / ETA;
+        SKNORM = SKNORM + SIGMA[I - 1] * SIGMA[I - 1];
+      }
+      SKNORM = sqrt(SKNORM);
+      if (SIGMA[K - 1] < ZERO) SKNORM = -SKNORM;
+      SIGMA[K - 1] = SIGMA[K - 1] + SKNORM;
+#pragma unroll
+      for (int I = 1; I <= N; I++) WA2[I - 1] = ZERO;
+#pragma unroll
+      for (int J = K; J <= N; J++) {
+        TEMP = SIGMA[J - 1];
+#pragma unroll
+        for (int I = 1; I <= N; I++) WA2[I - 1] = WA2[I - 1] + TEMP * QQ(I, J);
+      }
+#pragma unroll
+      for (int J = K; J <= N; J++) {
+        TEMP = SIGMA[J - 1] / (SKNORM * SIGMA[K - 1]);
+#pragma unroll
+        for (int I = 1; I <= N; I++) QQ(I, J) = QQ(I, J) - TEMP * WA2[I - 1];
+      }
+      SIGMA[K - 1] = SKNORM * ETA;
+      TEMP = FKY / SIGMA[K - 1];
+      if (H * fabs(TEMP) > DELTA) TEMP = copysign(fabs(DELTA / H), TEMP);
+#pragma unroll
+      for (int I = 1; I <= N; I++) WA1[I - 1] = WA1[I - 1] + TEMP * QQ(I, K);
+    }
+    XNORM = ZERO;
+    DIFIT = ZERO;
+#pragma unroll
+    for (int I = 1; I <= N; I++) {
+      XNORM = dmax1(XNORM, fabs(WA1[I - 1]));
+      DIFIT = dmax1(DIFIT, fabs(X[I - 1] - WA1[I - 1]));
+      X[I - 1] = WA1[I - 1];
+    }
+    DELTA = dmax1(DELTA, SCALE * XNORM);
+    CONV = (FNORM < FNORM1 && DIFIT < DIFIT1 && NSING == 0);
+    NIER6 = NIER6 + 1;
+    NIER7 = NIER7 + 1;
+    NIER8 = NIER8 + 1;
+    if (CONV) NIER6 = 0;
+    if (FNORM < FNORM1 || DIFIT < DIFIT1) NIER7 = 0;
+    if (DIFIT > EPS * XNORM) NIER8 = 0;
+    if (FNORM <= FTOL) INFO = 1;
+    if (DIFIT <= XTOL * XNORM && CONV) INFO = 2;
+    if (FNORM <= FTOL && INFO == 2) INFO = 3;
+    if (INFO != 0) break;
+    if (NFEV >= MAXFEV) INFO = 4;
+    if (NSING == N) INFO = 5;
+    if (NIER6 == 5) INFO = 6;
+    if (NIER7 == 3) INFO = 7;
+    if (NIER8 == 4) INFO = 8;
+    if (INFO != 0) break;
+    if (!CONV || DIFIT > P05 * XNORM || MOPT == 1) continue;
+    bool done = false;
+    for (int M = 2; M <= MOPT; M++) {
+      bool stop_refine = false;
+      FNORM1 = FNORM;
+      FNORM = ZERO;
+#pragma unroll
+      for (int K = 1; K <= N; K++) {
+        if (!stop_refine) {
+          FKY = sist3_f(P, s, WA1, K);
+          NFCALL = NFCALL + 1;
+          NFEV = NFCALL / N;
+          FNORM = dmax1(FNORM, fabs(FKY));
+          if (!(FNORM < FNORM1)) {
+            FNORM = FNORM1;
+            stop_refine = true;
+          } else {
+            TEMP = FKY / SIGMA[K - 1];
+#pragma unroll
+            for (int I = 1; I <= N; I++) WA1[I - 1] = WA1[I - 1] + TEMP * QQ(I, K);
+          }
+        }
+      }
+      if (stop_refine) break;
+      XNORM = ZERO;
+      DIFIT = ZERO;
+#pragma unroll
+      for (int I = 1; I <= N; I++) {
+        XNORM = dmax1(XNORM, fabs(WA1[I - 1]));
+        DIFIT = dmax1(DIFIT, fabs(X[I - 1] - WA1[I - 1]));
+        X[I - 1] = WA1[I - 1];
+      }
+      if (FNORM <= FTOL) INFO = 1;
+      if (DIFIT <= XTOL * XNORM) INFO = 2;
+      if (FNORM <= FTOL && INFO == 2) INFO = 3;
+      if (NFEV >= MAXFEV && INFO == 0) INFO = 4;
+      if (INFO != 0) {
+        done = true;
+        break;
+      }
+    }
+    if (done) break;
+  }
+#undef QQ
+  *nfev_out = NFEV;
+  return INFO;
+}
+
+// ---------------------------------------------------------------------------
+// Newton on the same 3x3 system with the analytic Jacobian (the root BRENTM
+// converges to); used by ECHO_C2P_NEWTON.  Residual target `tol` is on the
+// relative size of the three equations.  Returns iterations, or -1 when it
+// did not converge within `maxit` (the caller then falls back to BRENTM).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int eos_energy_slope(const DevPhys& P, double rh, double pr, double* en,
+                                                double* dedp) {
+  if (P.eqstate == ECHO_EOS_TABLE) {
+    if (pr < __ldg(P.tp)) return 125;
+    if (pr > __ldg(P.tp + P.nt - 1)) return 126;
+    int h = SEARCH_P(P, pr);
+    double p2 = __ldg(P.tp + h - 1), p1 = __ldg(P.tp + h - 2);
+    double e2 = __ldg(P.te + h - 1), e1 = __ldg(P.te + h - 2);
+    *dedp = (e2 - e1) / (p2 - p1);
+    *en = e1 + (e2 - e1) * (pr - p1) / (p2 - p1);
+    return 0;
+  }
+  if (pr <= P.przero) {
+    *en = P.enezero * pr / P.przero;
+    *dedp = P.enezero / P.przero;
+    return 0;
+  }
+  if (P.eqstate == ECHO_EOS_CONFORMAL) {
+    *en = 3. * pr;
+    *dedp = 3.;
+  } else {
+    *en = rh + pr / (4.0 / 3.0 - 1.);
+    *dedp = 3.;
+  }
+  return 0;
+}
+
+static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, double tol, int maxit) {
+  double xx = X[0], yy = X[1], pp = X[2];
+  for (int it = 1; it <= maxit; it++) {
+    if (!(xx < 1.0) || !(yy > 0.0)) return -1;
+    double sq = sqrt(1. - xx);
+    double rh = s.D * sq, en = 0, dedp = 0;
+    if (eos_energy_slope(P, rh, pp, &en, &dedp)) return -1;
+    double ib = yy + s.B2, iy2 = 1.0 / (yy * yy), iy3 = iy2 / yy, i1x = 1.0 / (1. - xx);
+    double F1 = ib * ib * xx - s.SB2 * iy2 * (2 * yy + s.B2) - s.S2;
+    double F2 = yy - pp + 0.5 * (1. + xx) * s.B2 - 0.5 * s.SB2 * iy2 - s.U;
+    double F3 = yy - (pp + en) * i1x;
+    // d(en)/dx through rh is zero: the tabulated and conformal e(p) do not depend on rh
+    double J11 = ib * ib, J12 = 2 * ib * xx + 2 * s.SB2 * (2 * yy + s.B2) * iy3 - 2 * s.SB2 * iy2, J13 = 0.;
+    double J21 = 0.5 * s.B2, J22 = 1. + s.SB2 * iy3, J23 = -1.;
+    double J31 = -(pp + en) * i1x * i1x, J32 = 1., J33 = -(1. + dedp) * i1x;
+    // Cramer solve of J d = -F
+    double c11 = J22 * J33 - J23 * J32, c12 = J23 * J31 - J21 * J33, c13 = J21 * J32 - J22 * J31;
+    double det = J11 * c11 + J12 * c12 + J13 * c13;
+    if (det == 0.0 || !isfinite(det)) return -1;
+    double idet = 1.0 / det;
+    double b1 = -F1, b2 = -F2, b3 = -F3;
+    double dx = (b1 * c11 + b2 * (J13 * J32 - J12 * J33) + b3 * (J12 * J23 - J13 * J22)) * idet;
+    double dy = (b1 * c12 + b2 * (J11 * J33 - J13 * J31) + b3 * (J13 * J21 - J11 * J23)) * idet;
+    double dp = (b1 * c13 + b2 * (J12 * J31 - J11 * J32) + b3 * (J11 * J22 - J12 * J21)) * idet;
+    // damp steps that would leave the physical domain
+    double lam = 1.0;
+    for (int k = 0; k < 30 && (xx + lam * dx >= 1.0 || yy + lam * dy <= 0.0 || pp + lam * dp <= 0.0); k++)
+      lam *= 0.5;
+    xx += lam * dx;
+    yy += lam * dy;
+    pp += lam * dp;
+    double scale = fabs(yy) + fabs(s.U) + fabs(pp);
+    if (fabs(dx) <= tol * fmax(fabs(xx), 1e-300) + tol * 1e-3 && fabs(dy) <= tol * fabs(yy) &&
+        fabs(dp) <= tol * fabs(pp) && fabs(F2) <= 1e3 * tol * scale) {
+      X[0] = xx;
+      X[1] = yy;
+      X[2] = pp;
+      return it;
+    }
+  }
+  return -1;
+}
+
+// ---------------------------------------------------------------------------
+// system_cons2prim (system.f90:423-1166).  u, v of length NV; v holds the
+// initial guess.  Returns the reference errcode; *iters gets the iteration
+// count (Newton steps, or BRENTM function evaluations).
+// ---------------------------------------------------------------------------
+template <int KIND>
+__device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol, const double* u,
+                         double* v, int* iters) {
+  typedef Traits<KIND> T;
+  const double eps = 1.e-12;
+  const double ntol = 1.e-12;
+  double g1 = M.g1, g2 = M.g2, g3 = M.g3, gm = M.gm;
+  int errcode = 0;
+  *iters = 0;
+  if (!T::VISC && !T::MHD) {
+    // ideal hydro Newton-Raphson (system.f90:511-561)
+    double d = gm * u[KRH];
+    double sx = gm * u[KVX];
+    double sy = gm * u[KVY];
+    double sz = gm * u[KVZ] / g3;
+    double et = gm * u[KPR];
+    double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
+    double pr = v[KPR], w = 0, v2, glf, rh = 0, en, drhdpr, dendpr;
+    double pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    int iter;
+    for (iter = 1; iter <= 100; iter++) {
+      w = et + pr;
+      v2 = s2 / (w * w);
+      if (v2 >= 1.) {
+        *iters = iter;
+        return 777;
+      }
+      glf = 1. / sqrt(1. - v2);
+      rh = d / glf;
+      en = w * (1. - v2) - pr;
+      drhdpr = rh * v2 * glf / (en + pr);
+      dendpr = v2;
+      errcode = eos_pressure(P, rh, en, &pr_eos, &dprdrh, &dprden);
+      f = pr_eos - pr;
+      df = dprdrh * drhdpr + dprden * dendpr - 1.;
+      dpr = -f / df;
+      if (fabs(dpr) < ntol * pr) break;
+      pr = pr + dpr;
+    }
+    *iters = iter;
+    v[KRH] = rh;
+    v[KVX] = sx / w;
+    v[KVY] = sy / w;
+    v[KVZ] = sz / w;
+    v[KPR] = pr;
+    if (pr <= 0) errcode = 777;
+    return errcode;
+  } else if (T::VISC) {
+    // nested iteration (system.f90:564-666)
+    double uin[T::NV], vprim[T::NV];
+#pragma unroll
+    for (int k = 0; k < T::NV; k++) uin[k] = gm * u[k];
+    double d = uin[KRH];
+#pragma unroll
+    for (int k = KPIBU; k <= KPIZZ; k++) v[k] = uin[k] / uin[KRH];
+    double vx = v[KVX], vy = v[KVY], vz = v[KVZ];
+    double v2 = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+#pragma unroll
+    for (int k = 0; k < T::NV; k++) vprim[k] = v[k];
+    double rh = 0, pr = 0, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    double et = gm * u[KPR];
+    int tot = 0;
+    for (int iv = 1; iv <= 100; iv++) {
+      vprim[KVX] = vx;
+      vprim[KVY] = vy;
+      vprim[KVZ] = vz;
+      Pit pi;
+      derived_pi_any(P, M, vprim, pi);
+      double en1 = et + v[KPIBU] + pi.tt * M.g0;
+      double sx_cov = uin[KVX] - pi.tx;
+      double sy_cov = uin[KVY] - pi.ty;
+      double sz_cov = uin[KVZ] - pi.tz * g3;
+      double sx = sx_cov, sy = sy_cov, sz = sz_cov / g3;
+      double s2 = sx * sx_cov + sy * sy_cov + sz * sz_cov;
+      pr = v[KPR];
+      for (int ip = 1; ip <= 100; ip++) {
+        tot++;
+        v2 = s2 / ((en1 + pr) * (en1 + pr));
+        if (v2 >= 1.) {
+          *iters = tot;
+          return 107;
+        }
+        glf = 1. / sqrt(1. - v2);
+        rh = d / glf;
+        en = (en1 + pr) * (1. - v2) - pr - vprim[KPIBU];
+        drhdpr = rh * v2 * glf / (en + pr);
+        dendpr = v2;
+        errcode = eos_pressure(P, rh, en, &pr_eos, &dprdrh, &dprden);
+        f = pr_eos - pr;
+        df = dprdrh * drhdpr + dprden * dendpr - 1.;
+        dpr = -f / df;
+        if (fabs(dpr) < ntol * pr) break;
+        pr = pr + dpr;
+      }
+      vx = sx / (en1 + pr);
+      if (fabs(vx) < eps) vx = 0.;
+      vy = sy / (en1 + pr);
+      if (fabs(vy) < eps) vy = 0.;
+      vz = sz / (en1 + pr);
+      if (fabs(vz) < eps) vz = 0.;
+      vprim[KVX] = vx;
+      vprim[KVY] = vy;
+      vprim[KVZ] = vz;
+      if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) break;
+    }
+    *iters = tot;
+    v[KRH] = rh;
+    v[KVX] = vx;
+    v[KVY] = vy;
+    v[KVZ] = vz;
+    v[KPR] = pr;
+    if (P.obtained_zz) {
+      Pit pi;
+      derived_pi_zz(M, v, pi);
+      v[KPIZZ] = pi.zz;
+    }
+    return errcode;
+  } else {
+    // ideal MHD (system.f90:668-730): BRENTM on sist3, or Newton on the same system
+    double uin[T::NV];
+#pragma unroll
+    for (int k = 0; k < T::NV; k++) uin[k] = gm * u[k];
+    double DD = uin[KRH];
+    double sx = uin[KVX], sy = uin[KVY], sz = uin[KVZ];
+    double UU = uin[KPR];
+    double bx = uin[KBX], by = uin[KBY], bz = uin[KBZ];
+    v[KBX] = uin[KBX];
+    v[KBY] = uin[KBY];
+    v[KBZ] = uin[KBZ];
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = sx * bx + sy * by + sz * bz;
+    double SB2 = SB * SB;
+    double SS2 = sx * sx + sy * sy + sz * sz / g3;
+    double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
+    double en = 0;
+    errcode = eos_energy(P, rh, &en, pr);
+    double v2 = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+    double X[3];
+    X[0] = v2;
+    X[1] = (en + pr) / (1 - v2);
+    X[2] = pr;
+    Sist3 s = {B2, SB2, SS2, UU, DD};
+    int nfev = 0;
+    if (algo == ECHO_C2P_NEWTON) {
+      double Xn[3] = {X[0], X[1], X[2]};
+      int it = newton3(P, s, Xn, tol, 30);
+      if (it > 0) {
+        X[0] = Xn[0];
+        X[1] = Xn[1];
+        X[2] = Xn[2];
+        nfev = it;
+      } else {
+        (void)brentm3(P, s, X, 1.e-14, 1.e-14, 300, 3, &nfev);
+        nfev += 1000;  // marks a fallback in the iteration statistics
+      }
+    } else {
+      (void)brentm3(P, s, X, 1.e-14, 1.e-14, 300, 3, &nfev);
+    }
+    *iters = nfev;
+    double xs = X[0], ys = X[1];
+    pr = X[2];
+    rh = DD * sqrt(1 - xs);
+    vx = (sx + SB * bx / ys) / (ys + B2);
+    vy = (sy + SB * by / ys) / (ys + B2);
+    vz = (sz / g3 + SB * bz / ys) / (ys + B2);
+    v[KRH] = rh;
+    v[KVX] = vx;
+    v[KVY] = vy;
+    v[KVZ] = vz;
+    v[KPR] = pr;
+    if (T::GLM) v[KGLM] = u[KGLM];
+    return errcode;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// get_sigma (viscous.f90:283-393)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void get_sigma(const DevPhys& P, const Metric& M, const double* v, const double* d,
+                                          double sigma[6]) {
+  enum { SXX = 0, SYY = 1, SZZ = 2, SXY = 3, SXZ = 4, SYZ = 5 };
+  double g1 = M.g1, g2 = M.g2, g3 = M.g3, t = M.t;
+  double ux = v[KVX], uy = v[KVY], uz = v[KVZ];
+  double ut = 1. / sqrt(1. - g1 * ux * ux - g2 * uy * uy - g3 * uz * uz);
+  ux = ux * ut;
+  uy = uy * ut;
+  uz = uz * ut;
+  double dutdt = d[DTT], duxdx = d[DXX], duydy = d[DYY], duzdz = d[DZZ], duzdt = d[DZT];
+  double duzdx = d[DZX], duzdy = d[DZY], duxdt = d[DXT], duxdy = d[DXY];
+  double duxdz = d[DXZ], duydt = d[DYT], duydx = d[DYX], duydz = d[DYZ];
+  if (P.coordinates == ECHO_MINKOWSKI) {
+    sigma[SZZ] = ut * uz * duzdt + uz * ux * duzdx + uz * uy * duzdy + (2. / 3.) * duzdz +
+                 (2. / 3.) * duzdz * (uz * uz) - dutdt / 3. - duxdx / 3. - duydy / 3. -
+                 (uz * uz) * dutdt / 3. - (uz * uz) * duxdx / 3. - (uz * uz) * duydy / 3.;
+    sigma[SXZ] = 0.5 * ut * ux * duzdt + 0.5 * duzdx + 0.5 * (ux * ux) * duzdx + 0.5 * ux * uy * duzdy +
+                 ux * uz * duzdz / 6. + 0.5 * ut * uz * duxdt + ux * uz * duxdx / 6. + 0.5 * uy * uz * duxdy +
+                 0.5 * duxdz + 0.5 * duxdz * (uz * uz) - ux * uz * dutdt / 3. - ux * uz * duydy / 3.;
+    sigma[SXY] = 0.5 * ut * ux * duydt + 0.5 * duydx + 0.5 * (ux * ux) * duydx + ux * uy * duydy / 6. +
+                 ux * uz * duydz / 2. + 0.5 * ut * uy * duxdt + ux * uy * duxdx / 6. + 0.5 * duxdy +
+                 0.5 * duxdy * (uy * uy) + uy * uz * duxdz / 2. - ux * uy * dutdt / 3. - ux * uy * duzdz / 3.;
+    sigma[SYZ] = 0.5 * ut * uy * duzdt + ux * uy * duzdx / 2. + duzdy / 2. + duzdy * (uy * uy) / 2. +
+                 uy * uz * duzdz / 6. + ut * uz * duydt / 2. + ux * uz * duydx / 2. + uy * uz * duydy / 6. +
+                 duydz / 2. + duydz / 2. * (uz * uz) - uy * uz * dutdt / 3. - uy * uz * duxdx / 3.;
+    sigma[SXX] = ut * ux * duxdt + (2. / 3.) * duxdx + (2. / 3.) * duxdx * (ux * ux) + ux * uy * duxdy +
+                 ux * uz * duxdz - dutdt / 3. - duydy / 3. - duzdz / 3. - (ux * ux) * dutdt / 3. -
+                 (ux * ux) * duydy / 3. - (ux * ux) * duzdz / 3.;
+    sigma[SYY] = ut * uy * duydt + ux * uy * duydx + (2. / 3.) * duydy + (2. / 3.) * duydy * (uy * uy) +
+                 uy * uz * duydz - dutdt / 3. - duxdx / 3. - duzdz / 3. - (uy * uy) * dutdt / 3. -
+                 (uy * uy) * duxdx / 3. - (uy * uy) * duzdz / 3.;
+  } else {
+    double t2 = t * t, t3 = M.t3;
+    sigma[SZZ] = ut * uz * duzdt + uz * ux * duzdx + uz * uy * duzdy + (2. * duzdz) / (3. * t2) +
+                 (2. / 3.) * duzdz * (uz * uz) - dutdt / (3. * t2) - duxdx / (3. * t2) - duydy / (3. * t2) -
+                 (uz * uz) * dutdt / 3. - (uz * uz) * duxdx / 3. - (uz * uz) * duydy / 3. + 2. / 3. * ut / t3 +
+                 5. / 3. * (ut / t) * (uz * uz);
+    sigma[SXZ] = 0.5 * ut * ux * duzdt + 0.5 * duzdx + 0.5 * (ux * ux) * duzdx + 0.5 * ux * uy * duzdy +
+                 ux * uz * duzdz / 6. + 0.5 * ut * uz * duxdt + ux * uz * duxdx / 6. + 0.5 * uy * uz * duxdy +
+                 duxdz / (2. * t2) + 0.5 * duxdz * (uz * uz) - ux * uz * dutdt / 3. - ux * uz * duydy / 3. +
+                 (2. / 3.) * ut * uz * ux / t;
+    sigma[SXY] = 0.5 * ut * ux * duydt + 0.5 * duydx + 0.5 * (ux * ux) * duydx + ux * uy * duydy / 6. +
+                 ux * uz * duydz / 2. + 0.5 * ut * uy * duxdt + ux * uy * duxdx / 6. + 0.5 * duxdy +
+                 0.5 * duxdy * (uy * uy) + uy * uz * duxdz / 2. - ux * uy * dutdt / 3. - ux * uy * duzdz / 3. -
+                 ut * ux * uy / (3. * t);
+    sigma[SYZ] = 0.5 * ut * uy * duzdt + ux * uy * duzdx / 2. + duzdy / 2. + duzdy * (uy * uy) / 2. +
+                 uy * uz * duzdz / 6. + ut * uz * duydt / 2. + ux * uz * duydx / 2. + uy * uz * duydy / 6. +
+                 duydz / (2. * t2) + duydz / 2. * (uz * uz) - uy * uz * dutdt / 3. - uy * uz * duxdx / 3. +
+                 (2. / 3.) * ut * uz * uy / t;
+    sigma[SXX] = ut * ux * duxdt + (2. / 3.) * duxdx + (2. / 3.) * duxdx * (ux * ux) + ux * uy * duxdy +
+                 ux * uz * duxdz - dutdt / 3. - duydy / 3. - duzdz / 3. - ut / (3. * t) - (ux * ux) * dutdt / 3. -
+                 (ux * ux) * duydy / 3. - (ux * ux) * duzdz / 3. - (ux * ux) * ut / (3. * t);
+    sigma[SYY] = ut * uy * duydt + ux * uy * duydx + (2. / 3.) * duydy + (2. / 3.) * duydy * (uy * uy) +
+                 uy * uz * duydz - dutdt / 3. - duxdx / 3. - duzdz / 3. - ut / (3. * t) - (uy * uy) * dutdt / 3. -
+                 (uy * uy) * duxdx / 3. - (uy * uy) * duzdz / 3. - (uy * uy) * ut / (3. * t);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// system_source (system.f90:1587-1842) without the resistive terms.
+// v: primitives of the cell (modified copy), dv: its 16 derivatives.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__device__ int system_source(const DevPhys& P, const Metric& M, double* v, const double* dv, double* src) {
+  typedef Traits<KIND> T;
+  double g1 = M.g1, g2 = M.g2, g3 = M.g3, gp = M.gp, g0 = M.g0, t = M.t;
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) src[k] = 0.;
+  double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
+  double en = 0;
+  int err = eos_energy(P, rh, &en, pr);
+  if (err) return err;
+  double v2 = g1 * vx * vx + g2 * vy * vy + g3 * vz * vz;
+  double glf = 1. / sqrt(1. - v2);
+  double ut = glf;
+  const double lambda0 = 1., lambda1 = 1., lambda2 = 0.;
+  if (!T::VISC) {
+    if (P.coordinates == ECHO_BJORKEN) {
+      double w = en + pr;
+      double ww = w * (glf * glf);
+      if (T::MHD) {
+        double E[3];
+        e_ideal(M, vx, vy, vz, v[KBX], v[KBY], v[KBZ], E);
+        double bx = v[KBX], by = v[KBY], bz = v[KBZ];
+        double B2 = bx * bx + by * by + (bz * bz) * g3;
+        double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
+        double EEM = 0.5 * (E2 + B2);
+        double e3g = E[2] / g3;
+        src[KPR] = -t * (ww * vz * vz - e3g * e3g - bz * bz + (EEM + pr) / g3);
+      } else {
+        src[KPR] = -t * (ww * vz * vz + pr / g3);
+      }
+    }
+  } else {
+    double sigma[6], eta, zeta, tau_pi, tau_pi_big;
+    enum { SXX = 0, SYY = 1, SZZ = 2, SXY = 3, SXZ = 4, SYZ = 5 };
+    get_sigma(P, M, v, dv, sigma);
+    err = viscous_parameters(P, v[KRH], v[KPR], &eta, &zeta, &tau_pi, &tau_pi_big);
+    if (err) return err;
+    Pit pi;
+    derived_pi_any(P, M, v, pi);
+    double pitx = pi.tx, pity = pi.ty, pitz = pi.tz;
+    double dutdt = dv[DTT], dutdx = dv[DTX], dutdy = dv[DTY], dutdz = dv[DTZ];
+    double duxdx = dv[DXX], duydy = dv[DYY], duzdz = dv[DZZ], duzdt = dv[DZT];
+    double duzdx = dv[DZX], duzdy = dv[DZY], duxdt = dv[DXT], duxdy = dv[DXY];
+    double duxdz = dv[DXZ], duydt = dv[DYT], duydx = dv[DYX], duydz = dv[DYZ];
+    double sum_der = dutdt + duxdx + duydy + duzdz;
+    if (P.coordinates == ECHO_BJORKEN) {
+      double sum_der_t = sum_der + ut / t;
+      double sum_der_0 = g0 * (glf * dutdt + glf * v[KVX] * dutdx + glf * v[KVY] * dutdy + glf * v[KVZ] * dutdz);
+      double sum_der_x = g1 * (glf * duxdt + glf * v[KVX] * duxdx + glf * v[KVY] * duxdy + glf * v[KVZ] * duxdz);
+      double sum_der_y = g2 * (glf * duydt + glf * v[KVX] * duydx + glf * v[KVY] * duydy + glf * v[KVZ] * duydz);
+      double sum_der_z = glf * ((t * t) * duzdt + 2. * t * v[KVZ]) +
+                         (t * t) * (glf * v[KVX] * duzdx + glf * v[KVY] * duzdy + glf * v[KVZ] * duzdz);
+      double w = en + pr + v[KPIBU];
+      double ww = w * (glf * glf);
+      src[KPR] = -t * (ww * vz * vz + (pr + v[KPIBU]) / g3 + v[KPIZZ]);
+      src[KPIBU] = -1. / tau_pi_big * (v[KPIBU] + zeta * sum_der_t) - lambda0 * 4. / 3. * v[KPIBU] * sum_der_t;
+      double w0x = -0.5 * (dutdx + duxdt) + 0.5 * glf * (sum_der_x - v[KVX] * g1 * sum_der_0);
+      double w0y = -0.5 * (dutdy + duydt) + 0.5 * glf * (sum_der_y - v[KVY] * g2 * sum_der_0);
+      double w0z = -0.5 * (dutdz + duzdt) + 0.5 * glf * (sum_der_z - v[KVZ] * g3 * sum_der_0);
+      double wxy = 0.5 * (g2 * duydx - duxdy) + 0.5 * glf * (g1 * v[KVX] * sum_der_y - g2 * v[KVY] * sum_der_x);
+      double wxz = 0.5 * (g3 * duzdx - duxdz) + 0.5 * glf * (g1 * v[KVX] * sum_der_z - g3 * v[KVZ] * sum_der_x);
+      double wyz = 0.5 * (g3 * duzdy - duydz) + 0.5 * glf * (g2 * v[KVY] * sum_der_z - g3 * v[KVZ] * sum_der_y);
+      double wx0 = w0x, wy0 = w0y, wz0 = w0z, wyx = -wxy, wzx = -wxz, wzy = -wyz;
+      double IVzz = 2. * (pitz * wz0 + v[KPIXZ] * wzx + v[KPIYZ] * wzy);
+      double IVxx = 2. * (pitx * wx0 + v[KPIXY] * wxy + v[KPIXZ] * wxz);
+      double IVyy = 2. * (pity * wy0 + v[KPIXY] * wyx + v[KPIYZ] * wyz);
+      double IVxy = v[KPIXX] * wyx + v[KPIYY] * wxy + v[KPIXZ] * wyz + v[KPIYZ] * wxz + pitx * wy0 + pity * wx0;
+      double IVxz = v[KPIXX] * wzx + v[KPIZZ] * wxz + v[KPIXY] * wzy + v[KPIYZ] * wxy + pitx * wz0 + pitz * wx0;
+      double IVyz = v[KPIYY] * wzy + v[KPIZZ] * wyz + v[KPIXY] * wzx + v[KPIXZ] * wyx + pity * wz0 + pitz * wy0;
+      src[KPIZZ] = -1. / tau_pi * (v[KPIZZ] + 2. * eta * sigma[SZZ]) - 2. * glf * v[KPIZZ] / t -
+                   2. * (glf * vz) * pitz / t - lambda0 * 4. / 3. * v[KPIZZ] * sum_der_t +
+                   lambda1 * glf * (2. * v[KVZ] * (pitz * sum_der_0 + v[KPIXZ] * sum_der_x + v[KPIYZ] * sum_der_y + v[KPIZZ] * sum_der_z)) -
+                   lambda2 * IVzz;
+      src[KPIXZ] = -1. / tau_pi * (v[KPIXZ] + 2. * eta * sigma[SXZ]) + lambda0 * (-4. / 3. * v[KPIXZ] * sum_der_t) -
+                   glf / t * v[KPIXZ] - glf * vz * pitx / t +
+                   lambda1 * glf * ((pitx * v[KVZ] + pitz * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVZ] + v[KPIXZ] * v[KVX]) * sum_der_x +
+                                    (v[KPIXY] * v[KVZ] + v[KPIYZ] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVZ] + v[KPIZZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxz;
+      src[KPIYZ] = -1. / tau_pi * (v[KPIYZ] + 2. * eta * sigma[SYZ]) + lambda0 * (-4. / 3. * v[KPIYZ] * sum_der_t) -
+                   glf / t * v[KPIYZ] - glf * vz * pity / t +
+                   lambda1 * glf * ((pity * v[KVZ] + pitz * v[KVY]) * sum_der_0 + (v[KPIXY] * v[KVZ] + v[KPIXZ] * v[KVY]) * sum_der_x +
+                                    (v[KPIYY] * v[KVZ] + v[KPIYZ] * v[KVY]) * sum_der_y + (v[KPIYZ] * v[KVZ] + v[KPIZZ] * v[KVY]) * sum_der_z) -
+                   lambda2 * IVyz;
+      src[KPIXY] = -1. / tau_pi * (v[KPIXY] + 2. * eta * sigma[SXY]) + lambda0 * (-4. / 3. * v[KPIXY] * sum_der_t) +
+                   lambda1 * glf * ((pitx * v[KVY] + pity * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVY] + v[KPIXY] * v[KVX]) * sum_der_x +
+                                    (v[KPIXY] * v[KVY] + v[KPIYY] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVY] + v[KPIYZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxy;
+      src[KPIXX] = -1. / tau_pi * (v[KPIXX] + 2. * eta * sigma[SXX]) + lambda0 * (-4. / 3. * v[KPIXX] * sum_der_t) +
+                   lambda1 * glf * (2. * v[KVX] * (pitx * sum_der_0 + v[KPIXX] * sum_der_x + v[KPIXY] * sum_der_y + v[KPIXZ] * sum_der_z)) -
+                   lambda2 * IVxx;
+      src[KPIYY] = -1. / tau_pi * (v[KPIYY] + 2. * eta * sigma[SYY]) + lambda0 * (-4. / 3. * v[KPIYY] * sum_der_t) +
+                   lambda1 * glf * (2. * v[KVY] * (pity * sum_der_0 + v[KPIXY] * sum_der_x + v[KPIYY] * sum_der_y + v[KPIYZ] * sum_der_z)) -
+                   lambda2 * IVyy;
+    } else {
+      double sum_der_0 = g0 * (glf * dutdt + v[KVX] * dutdx + v[KVY] * dutdy + v[KVZ] * dutdz);
+      double sum_der_x = g1 * (glf * duxdt + v[KVX] * duxdx + v[KVY] * duxdy + v[KVZ] * duxdz);
+      double sum_der_y = g2 * (glf * duydt + v[KVX] * duydx + v[KVY] * duydy + v[KVZ] * duydz);
+      double sum_der_z = g3 * (glf * duzdt + v[KVX] * duzdx + v[KVY] * duzdy + v[KVZ] * duzdz);
+      src[KPIBU] = -1. / tau_pi_big * (v[KPIBU] + zeta * sum_der) + lambda0 * (-1. / 3. * v[KPIBU] * sum_der);
+      double w0x = -0.5 * (dutdx + duxdt) + 0.5 * glf * (sum_der_x - v[KVX] * g1 * sum_der_0);
+      double w0y = -0.5 * (dutdy + duydt) + 0.5 * glf * (sum_der_y - v[KVY] * g2 * sum_der_0);
+      double w0z = -0.5 * (dutdz + duzdt) + 0.5 * glf * (sum_der_z - v[KVZ] * g3 * sum_der_0);
+      double wxy = 0.5 * (g2 * duydx - duxdy) + 0.5 * glf * (g1 * v[KVX] * sum_der_y - g2 * v[KVY] * sum_der_x);
+      double wxz = 0.5 * (g3 * duzdx - duxdz) + 0.5 * glf * (g1 * v[KVX] * sum_der_z - g3 * v[KVZ] * sum_der_x);
+      double wyz = 0.5 * (g3 * duzdy - duydz) + 0.5 * glf * (g2 * v[KVY] * sum_der_z - g3 * v[KVZ] * sum_der_y);
+      double wx0 = w0x, wy0 = w0y, wz0 = w0z, wyx = -wxy, wzx = -wxz, wzy = -wyz;
+      double IVzz = 2. * (pitz * wz0 + v[KPIXZ] * wzx + v[KPIYZ] * wzy);
+      double IVxx = 2. * (pitx * wx0 + v[KPIXY] * wxy + v[KPIXZ] * wxz);
+      double IVyy = 2. * (pity * wy0 + v[KPIXY] * wyx + v[KPIYZ] * wyz);
+      double IVxy = v[KPIXX] * wyx + v[KPIYY] * wxy + v[KPIXZ] * wyz + v[KPIYZ] * wxz + pitx * wy0 + pity * wx0;
+      double IVxz = v[KPIXX] * wzx + v[KPIZZ] * wxz + v[KPIXY] * wzy + v[KPIYZ] * wxy + pitx * wz0 + pitz * wx0;
+      double IVyz = v[KPIYY] * wzy + v[KPIZZ] * wyz + v[KPIXY] * wzx + v[KPIXZ] * wyx + pity * wz0 + pitz * wy0;
+      src[KPIZZ] = -1. / tau_pi * (v[KPIZZ] + 2. * eta * sigma[SZZ]) + lambda0 * (-4. / 3. * v[KPIZZ] * sum_der) +
+                   lambda1 * (2. * v[KVZ] * (pitz * sum_der_0 + v[KPIXZ] * sum_der_x + v[KPIYZ] * sum_der_y + v[KPIZZ] * sum_der_z)) -
+                   lambda2 * IVzz;
+      src[KPIXZ] = -1. / tau_pi * (v[KPIXZ] + 2. * eta * sigma[SXZ]) + lambda0 * (-4. / 3. * v[KPIXZ] * sum_der) +
+                   lambda1 * ((pitx * v[KVZ] + pitz * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVZ] + v[KPIXZ] * v[KVX]) * sum_der_x +
+                              (v[KPIXY] * v[KVZ] + v[KPIYZ] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVZ] + v[KPIZZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxz;
+      src[KPIXY] = -1. / tau_pi * (v[KPIXY] + 2. * eta * sigma[SXY]) + lambda0 * (-4. / 3. * v[KPIXY] * sum_der) +
+                   lambda1 * ((pitx * v[KVY] + pity * v[KVX]) * sum_der_0 + (v[KPIXX] * v[KVY] + v[KPIXY] * v[KVX]) * sum_der_x +
+                              (v[KPIXY] * v[KVY] + v[KPIYY] * v[KVX]) * sum_der_y + (v[KPIXZ] * v[KVY] + v[KPIYZ] * v[KVX]) * sum_der_z) -
+                   lambda2 * IVxy;
+      src[KPIYZ] = -1. / tau_pi * (v[KPIYZ] + 2. * eta * sigma[SYZ]) + lambda0 * (-4. / 3. * v[KPIYZ] * sum_der) +
+                   lambda1 * ((pity * v[KVZ] + pitz * v[KVY]) * sum_der_0 + (v[KPIXY] * v[KVZ] + v[KPIXZ] * v[KVY]) * sum_der_x +
+                              (v[KPIYY] * v[KVZ] + v[KPIYZ] * v[KVY]) * sum_der_y + (v[KPIYZ] * v[KVZ] + v[KPIZZ] * v[KVY]) * sum_der_z) -
+                   lambda2 * IVyz;
+      src[KPIXX] = -1. / tau_pi * (v[KPIXX] + 2. * eta * sigma[SXX]) + lambda0 * (-4. / 3. * v[KPIXX] * sum_der) +
+                   lambda1 * (2. * v[KVX] * (pitx * sum_der_0 + v[KPIXX] * sum_der_x + v[KPIXY] * sum_der_y + v[KPIXZ] * sum_der_z)) -
+                   lambda2 * IVxx;
+      src[KPIYY] = -1. / tau_pi * (v[KPIYY] + 2. * eta * sigma[SYY]) + lambda0 * (-4. / 3. * v[KPIYY] * sum_der) +
+                   lambda1 * (2. * v[KVY] * (pity * sum_der_0 + v[KPIXY] * sum_der_x + v[KPIYY] * sum_der_y + v[KPIYZ] * sum_der_z)) -
+                   lambda2 * IVyy;
+    }
+#pragma unroll
+    for (int k = KPIBU; k < T::NV; k++) src[k] = src[k] * v[KRH];
+  }
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) src[k] = src[k] * gp;
+  return 0;
+}
+
+}  // namespace echo

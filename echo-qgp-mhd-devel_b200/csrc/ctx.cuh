@@ -1,0 +1,71 @@
+// ctx.cuh -- the device context of one run and the per-equation-set launch
+// functions.  The launchers are explicitly instantiated once per equation
+// set in kind_*.cu so the four instantiations compile in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <utility>
+#include <vector>
+
+#include "../../include/echo_gpu.h"
+#include "kernels.cuh"
+
+using namespace echo;
+
+struct EchoCtx {
+  EchoParams p;
+  int kind, nv, nvold;
+  Grid g;
+  DevPhys P;
+  BcDir bc[3];
+  int bc_uniform[3], bc_signed[3];
+  cudaStream_t stream;
+  double* d_v[2];
+  int vcur;
+  double* d_u[2];
+  int ucur;
+  double *d_F[3], *d_WD[3];
+  size_t nfaces[3];
+  double* d_vh[2];          // vnewstep / vold history (first 4 components used)
+  int vn;                   // d_vh[vn] = vnewstep, d_vh[1-vn] = vold
+  double* d_tab;
+  int* d_bk;                // EoS bracket accelerators
+  double* d_du;             // scratch for echo_gpu_rhs
+  unsigned char* d_fail;
+  DevScalars* d_sc;
+  DevScalars* h_sc;         // pinned mirror
+  cudaGraphExec_t graph[8];  // one per buffer-role key at step start
+  bool graph_ok[8];
+  // per-kernel timing (echo_gpu_profile_step): events recorded after each launch group
+  std::vector<std::pair<int, cudaEvent_t>>* marks;
+};
+
+// kernel classes reported by echo_gpu_profile_step
+enum { PK_FACES_X = 0, PK_FACES_Y = 1, PK_FACES_Z = 2, PK_SCALARS = 3, PK_UPDATE = 4, PK_REPAIR = 5, PK_END = 6,
+       PK_N = 7 };
+
+inline void mark(EchoCtx* c, int cls) {
+  if (!c->marks) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, c->stream);
+  c->marks->push_back({cls, e});
+}
+
+// Bracket accelerator of tab_bracket: for every bucket of the bit pattern
+// (>> BK_SHIFT) between the first and last table value, the smallest
+// bracket index max(2, first i with arr(i) >= lowest value of the bucket).
+
+namespace echo {
+
+template <int KIND>
+void launch_faces(EchoCtx* c, int dir);
+template <int KIND>
+void launch_update(EchoCtx* c, int irk, int mode, double* du_out);
+template <int KIND>
+void launch_repair_smooth(EchoCtx* c);
+template <int KIND>
+void launch_p2c(EchoCtx* c);
+
+}  // namespace echo

@@ -1,0 +1,526 @@
+// echo_gpu.cu -- context management and the C-ABI entry points of
+// include/echo_gpu.h.  One CUDA stream per context; every stage is a fixed
+// sequence of launches with no host synchronisation, so whole steps are
+// captured into a CUDA graph (echo_gpu_run).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/echo_gpu.h"
+#include "ctx.cuh"
+
+using namespace echo;
+
+#define CK(x)                                                                               \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) {                                                                \
+      fprintf(stderr, "echo_gpu: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+              __LINE__);                                                                    \
+      return ECHO_ERR_CUDA;                                                                 \
+    }                                                                                       \
+  } while (0)
+
+bool echo_make_buckets(const double* arr, int n, std::vector<int>& bk, long long& k0) {
+  if (n < 2 || !(arr[0] > 0.0)) return false;
+  for (int i = 1; i < n; i++)
+    if (!(arr[i] > arr[i - 1])) return false;
+  long long b0, b1;
+  memcpy(&b0, &arr[0], 8);
+  memcpy(&b1, &arr[n - 1], 8);
+  k0 = b0 >> BK_SHIFT;
+  long long nb = (b1 >> BK_SHIFT) - k0 + 1;
+  if (nb > (1 << 22)) return false;
+  bk.resize((size_t)nb);
+  int i = 1;  // 1-based
+  for (long long b = 0; b < nb; b++) {
+    long long bits = (k0 + b) << BK_SHIFT;
+    double lo;
+    memcpy(&lo, &bits, 8);
+    while (i < n && arr[i - 1] < lo) i++;
+    bk[(size_t)b] = i < 2 ? 2 : i;
+  }
+  return true;
+}
+
+int echo_kind_of(const EchoParams* p) {
+  if (p->viscosity) return KIND_VISC;
+  if (p->mhd) return p->divclean ? KIND_MHDGLM : KIND_MHD;
+  return KIND_HD;
+}
+int echo_nv_of(int kind) {
+  switch (kind) {
+    case KIND_VISC: return 12;
+    case KIND_MHD: return 8;
+    case KIND_MHDGLM: return 9;
+    default: return 5;
+  }
+}
+
+#define DISPATCH(c, fn, ...)                                      \
+  do {                                                            \
+    switch ((c)->kind) {                                          \
+      case KIND_HD: fn<KIND_HD>(__VA_ARGS__); break;              \
+      case KIND_VISC: fn<KIND_VISC>(__VA_ARGS__); break;          \
+      case KIND_MHD: fn<KIND_MHD>(__VA_ARGS__); break;            \
+      default: fn<KIND_MHDGLM>(__VA_ARGS__); break;               \
+    }                                                             \
+  } while (0)
+
+static void launch_scalars(EchoCtx* c, int irk) {
+  ScalarArgs S;
+  S.sc = c->d_sc;
+  S.g = c->g;
+  S.cfl = c->p.cfl;
+  S.maxdt = c->p.maxdt;
+  S.glm_alpha = c->p.glm_alpha;
+  S.irk = irk;
+  S.nrk = c->p.nrk;
+  S.divclean = c->p.divclean;
+  stage_scalars_kernel<<<1, 1, 0, c->stream>>>(S);
+}
+
+// one explicit RK stage, all asynchronous
+static void enqueue_stage(EchoCtx* c, int irk) {
+  for (int d = 0; d < 3; d++) {
+    int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
+    if (n > 1) {
+      DISPATCH(c, launch_faces, c, d);
+      mark(c, PK_FACES_X + d);
+    }
+  }
+  launch_scalars(c, irk);
+  cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
+  mark(c, PK_SCALARS);
+  DISPATCH(c, launch_update, c, irk, MODE_RK, (double*)nullptr);
+  mark(c, PK_UPDATE);
+  DISPATCH(c, launch_repair_smooth, c);
+  mark(c, PK_REPAIR);
+  if (irk == 1) c->ucur = 1 - c->ucur;
+  c->vcur = 1 - c->vcur;
+}
+
+static void snapshot_vnewstep(EchoCtx* c) {
+  // vnewstep = v (echo.f90:193-201); only the viscous time derivatives read it
+  if (c->p.viscosity)
+    cudaMemcpyAsync(c->d_vh[c->vn], c->d_v[c->vcur], sizeof(double) * c->g.ncell * 4, cudaMemcpyDeviceToDevice,
+                    c->stream);
+}
+
+// end of step: vold = vnewstep (echo.f90:240) is a role swap
+static void end_step(EchoCtx* c) {
+  end_step_kernel<<<1, 1, 0, c->stream>>>(c->d_sc, c->p.coordinates);
+  mark(c, PK_END);
+  if (c->p.viscosity) c->vn = 1 - c->vn;
+}
+
+static void enqueue_step(EchoCtx* c) {
+  snapshot_vnewstep(c);
+  for (int irk = 1; irk <= c->p.nrk; irk++) enqueue_stage(c, irk);
+  end_step(c);
+}
+
+// the role changes of enqueue_step without launching anything
+static void advance_roles(EchoCtx* c) {
+  c->ucur = 1 - c->ucur;
+  c->vcur = c->vcur ^ (c->p.nrk & 1);
+  if (c->p.viscosity) c->vn = 1 - c->vn;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int echo_gpu_nv(const EchoCtx* c) { return c ? c->nv : 0; }
+
+int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoCtx** out) {
+  if (!p || !out) return ECHO_ERR_ARG;
+  *out = nullptr;
+  if (p->mhd > 1 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
+  if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3) return ECHO_ERR_UNSUPPORTED;
+  if (p->nx < 1 || p->ny < 1 || p->nz < 1) return ECHO_ERR_ARG;
+  if ((p->nx > 1 && p->nx < 3) || (p->ny > 1 && p->ny < 3) || (p->nz > 1 && p->nz < 3)) return ECHO_ERR_ARG;
+  if (p->eqstate == ECHO_EOS_TABLE && (!eos_table || n_eos < 2)) return ECHO_ERR_ARG;
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return ECHO_ERR_CUDA;
+  EchoCtx* c = (EchoCtx*)calloc(1, sizeof(EchoCtx));
+  c->p = *p;
+  c->kind = echo_kind_of(p);
+  c->nv = echo_nv_of(c->kind);
+  c->g.nx = p->nx;
+  c->g.ny = p->ny;
+  c->g.nz = p->nz;
+  c->g.ncell = (size_t)p->nx * p->ny * p->nz;
+  double dx = (p->x2 - p->x1) / p->nx, dy = (p->y2 - p->y1) / p->ny, dz = (p->z2 - p->z1) / p->nz;
+  c->g.ddx = p->nx > 1 ? 1. / dx : 0.;
+  c->g.ddy = p->ny > 1 ? 1. / dy : 0.;
+  c->g.ddz = p->nz > 1 ? 1. / dz : 0.;
+  for (int d = 0; d < 3; d++)
+    for (int k = 0; k < ECHO_MAX_NV; k++)
+      for (int s = 0; s < 2; s++) c->bc[d].c[k][s] = (signed char)p->ibc[k][s][d];
+  for (int d = 0; d < 3; d++) {
+    int uni = 1, sgn = 0;
+    for (int k = 0; k < c->nv; k++)
+      for (int q = 0; q < 2; q++) {
+        int code = p->ibc[k][q][d];
+        if (code != p->ibc[0][q][d] || code == 3 || code < -1 || code > 3) uni = 0;
+        if (code == -1) sgn = 1;
+      }
+    c->bc_uniform[d] = uni;
+    c->bc_signed[d] = sgn;
+  }
+  c->nfaces[0] = (size_t)(p->nx + 1) * p->ny * p->nz;
+  c->nfaces[1] = (size_t)p->nx * (p->ny + 1) * p->nz;
+  c->nfaces[2] = (size_t)p->nx * p->ny * (p->nz + 1);
+  size_t nvc = (size_t)c->nv * c->g.ncell;
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; i++) {
+    CK(cudaMalloc(&c->d_v[i], sizeof(double) * nvc));
+    CK(cudaMalloc(&c->d_u[i], sizeof(double) * nvc));
+    CK(cudaMemset(c->d_v[i], 0, sizeof(double) * nvc));
+    CK(cudaMemset(c->d_u[i], 0, sizeof(double) * nvc));
+  }
+  for (int d = 0; d < 3; d++) {
+    int n = d == 0 ? p->nx : d == 1 ? p->ny : p->nz;
+    c->d_F[d] = nullptr;
+    c->d_WD[d] = nullptr;
+    if (n > 1) {
+      CK(cudaMalloc(&c->d_F[d], sizeof(double) * c->nv * c->nfaces[d]));
+      if (p->viscosity) CK(cudaMalloc(&c->d_WD[d], sizeof(double) * 8 * c->nfaces[d]));
+    }
+  }
+  for (int i = 0; i < 2; i++) {
+    CK(cudaMalloc(&c->d_vh[i], sizeof(double) * 4 * c->g.ncell));
+    CK(cudaMemset(c->d_vh[i], 0, sizeof(double) * 4 * c->g.ncell));
+  }
+  CK(cudaMalloc(&c->d_fail, c->g.ncell));
+  CK(cudaMemset(c->d_fail, 0, c->g.ncell));
+  CK(cudaMalloc(&c->d_sc, sizeof(DevScalars)));
+  CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars)));
+  memset(c->h_sc, 0, sizeof(DevScalars));
+  c->d_tab = nullptr;
+  int nt = 0;
+  if (eos_table && n_eos > 0) {
+    nt = n_eos;
+    std::vector<double> cols((size_t)4 * n_eos);
+    for (int i = 0; i < n_eos; i++)
+      for (int q = 0; q < 4; q++) cols[(size_t)q * n_eos + i] = eos_table[4 * i + q];
+    CK(cudaMalloc(&c->d_tab, sizeof(double) * 4 * n_eos));
+    CK(cudaMemcpy(c->d_tab, cols.data(), sizeof(double) * 4 * n_eos, cudaMemcpyHostToDevice));
+  }
+  c->P.eqstate = p->eqstate;
+  c->P.coordinates = p->coordinates;
+  c->P.recal = p->recal;
+  c->P.obtained_zz = p->obtained_zz;
+  c->P.init_type = p->init_type;
+  c->P.bulkvis = p->bulkvis;
+  c->P.nt = nt;
+  c->P.tT = c->d_tab;
+  c->P.te = c->d_tab ? c->d_tab + nt : nullptr;
+  c->P.tp = c->d_tab ? c->d_tab + 2 * nt : nullptr;
+  c->P.tc = c->d_tab ? c->d_tab + 3 * nt : nullptr;
+  c->P.maxspeed = p->maxspeed;
+  c->P.eta_over_s = p->eta_over_s;
+  c->P.tau_pi_coeff = p->tau_pi_coeff;
+  c->P.enezero = p->enezero;
+  c->P.przero = p->przero;
+  c->P.glm_alpha = p->glm_alpha;
+  c->P.bke = c->P.bkp = nullptr;
+  c->d_bk = nullptr;
+  if (nt > 0) {
+    std::vector<double> te(nt), tp(nt);
+    for (int i = 0; i < nt; i++) {
+      te[i] = eos_table[4 * i + 1];
+      tp[i] = eos_table[4 * i + 2];
+    }
+    std::vector<int> be, bp;
+    long long ke0 = 0, kp0 = 0;
+    if (echo_make_buckets(te.data(), nt, be, ke0) && echo_make_buckets(tp.data(), nt, bp, kp0)) {
+      CK(cudaMalloc(&c->d_bk, sizeof(int) * (be.size() + bp.size())));
+      CK(cudaMemcpy(c->d_bk, be.data(), sizeof(int) * be.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(c->d_bk + be.size(), bp.data(), sizeof(int) * bp.size(), cudaMemcpyHostToDevice));
+      c->P.bke = c->d_bk;
+      c->P.bkp = c->d_bk + be.size();
+      c->P.bke0 = ke0;
+      c->P.bkp0 = kp0;
+      c->P.nbke = (int)be.size();
+      c->P.nbkp = (int)bp.size();
+    }
+  }
+  c->d_du = nullptr;
+  c->marks = nullptr;
+  *out = c;
+  return ECHO_OK;
+}
+
+int echo_gpu_free(EchoCtx* c) {
+  if (!c) return ECHO_OK;
+  cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < 8; i++)
+    if (c->graph_ok[i]) cudaGraphExecDestroy(c->graph[i]);
+  for (int i = 0; i < 2; i++) {
+    cudaFree(c->d_v[i]);
+    cudaFree(c->d_u[i]);
+    cudaFree(c->d_vh[i]);
+  }
+  for (int d = 0; d < 3; d++) {
+    cudaFree(c->d_F[d]);
+    cudaFree(c->d_WD[d]);
+  }
+  cudaFree(c->d_fail);
+  cudaFree(c->d_sc);
+  cudaFree(c->d_tab);
+  cudaFree(c->d_bk);
+  cudaFree(c->d_du);
+  cudaFreeHost(c->h_sc);
+  cudaStreamDestroy(c->stream);
+  free(c);
+  return ECHO_OK;
+}
+
+static int reset_scalars(EchoCtx* c, double t) {
+  DevScalars s;
+  memset(&s, 0, sizeof(s));
+  s.t = t;
+  s.t3 = pow(t, 3.);
+  s.dt = 0.;
+  s.tout = 1e300;
+  s.dtout = 1e300;
+  s.tmax = 1e300;
+  s.timeold = t;
+  s.timeinterval = 0.;
+  s.g3old = c->p.coordinates == ECHO_BJORKEN ? t * t : 1.;
+  s.glm_ch_old = 0.5;  // common.f90:283
+  s.err_key = ~0ull;
+  CK(cudaMemcpyAsync(c->d_sc, &s, sizeof(s), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->d_vh[0], 0, sizeof(double) * 4 * c->g.ncell, c->stream));
+  CK(cudaMemsetAsync(c->d_vh[1], 0, sizeof(double) * 4 * c->g.ncell, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ECHO_OK;
+}
+
+static int upload_impl(EchoCtx* c, const double* v, const double* u, double t, cudaMemcpyKind kind) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c || !v) return ECHO_ERR_ARG;
+  size_t bytes = sizeof(double) * c->nv * c->g.ncell;
+  c->vcur = 0;
+  c->ucur = 0;
+  c->vn = 0;
+  int r = reset_scalars(c, t);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->d_v[0], v, bytes, kind, c->stream));
+  if (u) {
+    CK(cudaMemcpyAsync(c->d_u[0], u, bytes, kind, c->stream));
+  } else {
+    DISPATCH(c, launch_p2c, c);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+int echo_gpu_upload(EchoCtx* c, const double* v, const double* u, double t) {
+  return upload_impl(c, v, u, t, cudaMemcpyHostToDevice);
+}
+int echo_gpu_upload_device(EchoCtx* c, const double* v, const double* u, double t) {
+  return upload_impl(c, v, u, t, cudaMemcpyDeviceToDevice);
+}
+
+int echo_gpu_put_state(EchoCtx* c, const double* v, const double* u) {
+  if (!c || !v || !u) return ECHO_ERR_ARG;
+  size_t bytes = sizeof(double) * c->nv * c->g.ncell;
+  CK(cudaMemcpyAsync(c->d_v[c->vcur], v, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_u[c->ucur], u, bytes, cudaMemcpyHostToDevice, c->stream));
+  return ECHO_OK;
+}
+
+int echo_gpu_get_state(EchoCtx* c, double* v, double* u) {
+  if (!c) return ECHO_ERR_ARG;
+  size_t bytes = sizeof(double) * c->nv * c->g.ncell;
+  if (v) CK(cudaMemcpyAsync(v, c->d_v[c->vcur], bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (u) CK(cudaMemcpyAsync(u, c->d_u[c->ucur], bytes, cudaMemcpyDeviceToHost, c->stream));
+  return ECHO_OK;
+}
+
+static int download_impl(EchoCtx* c, double* v, double* u, cudaMemcpyKind kind) {
+  if (!c) return ECHO_ERR_ARG;
+  size_t bytes = sizeof(double) * c->nv * c->g.ncell;
+  if (v) CK(cudaMemcpyAsync(v, c->d_v[c->vcur], bytes, kind, c->stream));
+  if (u) CK(cudaMemcpyAsync(u, c->d_u[c->ucur], bytes, kind, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ECHO_OK;
+}
+int echo_gpu_download(EchoCtx* c, double* v, double* u) { return download_impl(c, v, u, cudaMemcpyDeviceToHost); }
+int echo_gpu_download_device(EchoCtx* c, double* v, double* u) {
+  return download_impl(c, v, u, cudaMemcpyDeviceToDevice);
+}
+
+int echo_gpu_set_tout(EchoCtx* c, double tout) {
+  if (!c) return ECHO_ERR_ARG;
+  CK(cudaMemcpyAsync(&c->d_sc->tout, &tout, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ECHO_OK;
+}
+
+static int read_scalars(EchoCtx* c) {
+  CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+static int errcode_of(const DevScalars* s, int* cell) {
+  if (s->err_key == ~0ull) {
+    if (cell) *cell = -1;
+    return 0;
+  }
+  if (cell) *cell = (int)(s->err_key >> 20);
+  return (int)(s->err_key & 0xFFFFFull);
+}
+
+int echo_gpu_evolve_main(EchoCtx* c, int irk, double* dt, int* errcode) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c || irk < 1 || irk > c->p.nrk) return ECHO_ERR_ARG;
+  if (irk == 1) snapshot_vnewstep(c);
+  enqueue_stage(c, irk);
+  CK(cudaGetLastError());
+  int r = read_scalars(c);
+  if (r) return r;
+  if (dt) *dt = c->h_sc->dt;
+  if (errcode) *errcode = errcode_of(c->h_sc, nullptr);
+  return ECHO_OK;
+}
+
+int echo_gpu_end_step(EchoCtx* c) {
+  if (!c) return ECHO_ERR_ARG;
+  end_step(c);
+  CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+int echo_gpu_step(EchoCtx* c, double* dt, int* errcode) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c) return ECHO_ERR_ARG;
+  enqueue_step(c);
+  CK(cudaGetLastError());
+  int r = read_scalars(c);
+  if (r) return r;
+  if (dt) *dt = c->h_sc->dt;
+  if (errcode) *errcode = errcode_of(c->h_sc, nullptr);
+  return ECHO_OK;
+}
+
+int echo_gpu_run(EchoCtx* c, int nsteps) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c || nsteps < 0) return ECHO_ERR_ARG;
+  for (int s = 0; s < nsteps; s++) {
+    // buffer roles at step start: which u/v buffer is current and which
+    // vnewstep/vold buffer is which; they repeat, so graphs are cached per key
+    int key = c->ucur | (c->vcur << 1) | (c->vn << 2);
+    if (!c->graph_ok[key]) {
+      cudaGraph_t gr;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_step(c);  // records the launches and advances the roles
+      CK(cudaStreamEndCapture(c->stream, &gr));
+      CK(cudaGraphInstantiate(&c->graph[key], gr, 0));
+      cudaGraphDestroy(gr);
+      c->graph_ok[key] = true;
+    } else {
+      advance_roles(c);
+    }
+    CK(cudaGraphLaunch(c->graph[key], c->stream));
+  }
+  CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+int echo_gpu_stream(EchoCtx* c, void** stream) {
+  if (!c || !stream) return ECHO_ERR_ARG;
+  *stream = (void*)c->stream;
+  return ECHO_OK;
+}
+
+int echo_gpu_profile_step(EchoCtx* c, double* ms, int* launches) {
+  if (!c || !ms) return ECHO_ERR_ARG;
+  (void)cudaGetLastError();
+  std::vector<std::pair<int, cudaEvent_t>> marks;
+  cudaEvent_t start;
+  CK(cudaEventCreate(&start));
+  CK(cudaEventRecord(start, c->stream));
+  c->marks = &marks;
+  enqueue_step(c);
+  c->marks = nullptr;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  for (int k = 0; k < PK_N; k++) {
+    ms[k] = 0.0;
+    if (launches) launches[k] = 0;
+  }
+  cudaEvent_t prev = start;
+  for (auto& m : marks) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, prev, m.second);
+    ms[m.first] += t;
+    if (launches) launches[m.first] += 1;
+    prev = m.second;
+  }
+  for (auto& m : marks) cudaEventDestroy(m.second);
+  cudaEventDestroy(start);
+  return ECHO_OK;
+}
+
+int echo_gpu_sync(EchoCtx* c) {
+  if (!c) return ECHO_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+int echo_gpu_stats(EchoCtx* c, EchoStats* st) {
+  if (!c || !st) return ECHO_ERR_ARG;
+  int r = read_scalars(c);
+  if (r) return r;
+  const DevScalars* s = c->h_sc;
+  st->dt = s->dt;
+  st->t = s->t;
+  st->glm_ch = s->glm_ch;
+  st->c2p_iters = (long long)s->c2p_iters;
+  st->c2p_cells = (long long)c->g.ncell;
+  st->repairs = (long long)s->repairs;
+  st->seed_fallbacks = (long long)s->fallbacks;
+  st->errcode = errcode_of(s, &st->err_cell);
+  return ECHO_OK;
+}
+
+int echo_gpu_rhs(EchoCtx* c, double* du, double* amax3) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c) return ECHO_ERR_ARG;
+  size_t nvc = (size_t)c->nv * c->g.ncell;
+  if (!c->d_du) CK(cudaMalloc(&c->d_du, sizeof(double) * nvc));
+  CK(cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream));
+  for (int d = 0; d < 3; d++) {
+    int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
+    if (n > 1) DISPATCH(c, launch_faces, c, d);
+  }
+  DISPATCH(c, launch_update, c, 1, MODE_RHS, c->d_du);
+  CK(cudaGetLastError());
+  if (du) CK(cudaMemcpyAsync(du, c->d_du, sizeof(double) * nvc, cudaMemcpyDeviceToHost, c->stream));
+  int r = read_scalars(c);
+  if (r) return r;
+  if (amax3)
+    for (int d = 0; d < 3; d++) {
+      unsigned long long b = c->h_sc->amax_bits[d];
+      double x;
+      memcpy(&x, &b, sizeof(x));
+      amax3[d] = x;
+    }
+  return errcode_of(c->h_sc, nullptr) ? 1 : ECHO_OK;
+}
+
+}  // extern "C"
+

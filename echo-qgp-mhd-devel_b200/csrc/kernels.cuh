@@ -1,0 +1,697 @@
+// kernels.cuh -- the device kernels of one RK stage.
+//
+//   faces<KIND,DIR>   one thread per cell face along DIR: boundary ghosts,
+//                     reconstruction, the p<=0 / v^2>=1 fix-ups, GLM, two
+//                     system_flux calls and the HLL flux (evolve_df[xyz],
+//                     evolve.f90:302-685; work_fup[xyz], work.f90:143-416);
+//                     writes the face flux and the max signal speed.
+//   stage_scalars     the scalar logic of evolve_main (dt, CFL reduction
+//                     result, GLM speed and damping factor).
+//   update<KIND>      one thread per cell: flux divergence + sources + RK
+//                     combination + con2prim (evolve.f90:156-203,689-868).
+//   repair<KIND>      the neighbour-average repair of failed cells in the
+//                     reference's loop order (evolve.f90:795-842).
+//   smooth<KIND>      evolve_smooth_viscosity (evolve.f90:1159-1207).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "c2p.cuh"
+
+namespace echo {
+
+// Device-resident scalars of the run.  Kept on the device so a whole step
+// needs no host round trip (and can be captured in a CUDA graph).
+struct DevScalars {
+  double t, t3, dt, tout, dtout, tmax, timeold, timeinterval, g3old;
+  double glm_ch, glm_ch_old, aflux[3], expfact;
+  unsigned long long amax_bits[3];
+  unsigned long long err_key;  // (cell << 20) | code, min over failures
+  int nfail, pad;
+  unsigned long long c2p_iters, c2p_cells, repairs, fallbacks;
+};
+
+struct Grid {
+  int nx, ny, nz;
+  size_t ncell;
+  double ddx, ddy, ddz;
+};
+
+// boundary codes for one sweep direction: bc[k][side]
+struct BcDir {
+  signed char c[ECHO_MAX_NV][2];
+};
+
+// ---------------------------------------------------------------------------
+// stencil loads with the ghost fill of evolve_bc[xyz] (evolve.f90:872-1127)
+// ---------------------------------------------------------------------------
+// Value of variable array `a` (one variable, already offset) at pencil index
+// j (1-based, may be a ghost in [-2, n+3]); `base` is the linear index of
+// pencil cell 1 and `stride` the step between pencil cells.
+__device__ __forceinline__ double ghost_val(const double* __restrict__ a, size_t base, long long stride,
+                                            int n, int j, int code_l, int code_r) {
+  if (j >= 1 && j <= n) return __ldg(a + base + (long long)(j - 1) * stride);
+  auto at = [&](int q) { return __ldg(a + base + (long long)(q - 1) * stride); };
+  if (j <= 0) {
+    switch (code_l) {
+      case 0: return at(j + n);
+      case 1: return at(1 - j);
+      case -1: return -at(1 - j);
+      case 3: {
+        double w1 = at(1), w2 = at(2), w3 = at(3);
+        double w0 = w3 - 3. * (w2 - w1);
+        if (j == 0) return w0;
+        double wm1 = w2 - 3. * (w1 - w0);
+        if (j == -1) return wm1;
+        return w1 - 3. * (w0 - wm1);
+      }
+      default: return at(1);
+    }
+  }
+  switch (code_r) {
+    case 0: return at(j - n);
+    case 1: return at(2 * n + 1 - j);
+    case -1: return -at(2 * n + 1 - j);
+    case 3: {
+      double a2 = at(n - 2), a1 = at(n - 1), a0 = at(n);
+      double p1 = a2 - 3. * (a1 - a0);
+      if (j == n + 1) return p1;
+      double p2 = a1 - 3. * (a0 - p1);
+      if (j == n + 2) return p2;
+      return a0 - 3. * (p1 - p2);
+    }
+    default: return at(n);
+  }
+}
+
+// index and sign of the cell that ghost j (1-based pencil index) copies for
+// boundary codes 0 (periodic), +-1 (reflecting) and 2 (outflow)
+__device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, double& sg) {
+  q = j;
+  sg = 1.0;
+  if (j < 1) {
+    q = cl == 0 ? j + n : (cl == 1 || cl == -1) ? 1 - j : 1;
+    if (cl == -1) sg = -1.0;
+  } else if (j > n) {
+    q = cr == 0 ? j - n : (cr == 1 || cr == -1) ? 2 * n + 1 - j : n;
+    if (cr == -1) sg = -1.0;
+  }
+}
+
+struct FaceArgs {
+  DevPhys P;
+  Grid g;
+  BcDir bc;
+  int bc_uniform;   // every variable has the same codes, none is 3 (extrapolation)
+  int bc_signed;    // some code is -1 (the ghost changes sign)
+  const double* __restrict__ v;   // primitives, nv * ncell
+  double* __restrict__ F;         // face fluxes, nv * nfaces
+  double* __restrict__ WD;        // viscous: wdl(4), wdr(4) per face, or null
+  DevScalars* sc;
+  int coordinates;
+};
+
+// face index layout for DIR: (i fastest in x, then the other two)
+//   DIR 0: F[k][iz][iy][i],  i = 0..nx
+//   DIR 1: F[k][iz][j][ix],  j = 0..ny
+//   DIR 2: F[k][kz][iy][ix], kz = 0..nz
+template <int KIND, int DIR>
+__global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) faces_kernel(FaceArgs A) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  const Grid& g = A.g;
+  const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
+  const size_t nfaces = DIR == 0 ? (size_t)(g.nx + 1) * g.ny * g.nz
+                        : DIR == 1 ? (size_t)g.nx * (g.ny + 1) * g.nz
+                                   : (size_t)g.nx * g.ny * (g.nz + 1);
+  size_t fid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double amax_local = 0.0;
+  if (fid < nfaces) {
+    int i, a, b;  // face index along DIR, transverse coordinates (1-based)
+    size_t base;
+    long long stride;
+    if (DIR == 0) {
+      i = (int)(fid % (g.nx + 1));
+      size_t r = fid / (g.nx + 1);
+      a = (int)(r % g.ny) + 1;
+      b = (int)(r / g.ny) + 1;
+      base = ((size_t)(b - 1) * g.ny + (a - 1)) * g.nx;
+      stride = 1;
+    } else if (DIR == 1) {
+      a = (int)(fid % g.nx) + 1;
+      size_t r = fid / g.nx;
+      i = (int)(r % (g.ny + 1));
+      b = (int)(r / (g.ny + 1)) + 1;
+      base = (size_t)(b - 1) * g.ny * g.nx + (a - 1);
+      stride = g.nx;
+    } else {
+      a = (int)(fid % g.nx) + 1;
+      size_t r = fid / g.nx;
+      b = (int)(r % g.ny) + 1;
+      i = (int)(r / g.ny);
+      base = (size_t)(b - 1) * g.nx + (a - 1);
+      stride = (long long)g.nx * g.ny;
+    }
+    const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+    double wl[NV], wr[NV], w0[NV];
+    // reconstruction of every variable (work_rec(n,1,nv,0))
+    if (A.bc_uniform) {
+      long long off[6];
+      double sg[6];
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        int qq;
+        map_ghost(i - 2 + q, n, A.bc.c[0][0], A.bc.c[0][1], qq, sg[q]);
+        off[q] = (long long)base + (long long)(qq - 1) * stride;
+      }
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        const double* vk = A.v + (size_t)k * g.ncell;
+        double s[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) s[q] = __ldg(vk + off[q]);
+        if (A.bc_signed) {
+#pragma unroll
+          for (int q = 0; q < 6; q++) s[q] = sg[q] * s[q];
+        }
+        w0[k] = s[2];
+        recon_face(A.P.recal, s, wl[k], wr[k]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        const double* vk = A.v + (size_t)k * g.ncell;
+        double s[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) s[q] = ghost_val(vk, base, stride, n, i - 2 + q, A.bc.c[k][0], A.bc.c[k][1]);
+        w0[k] = s[2];
+        recon_face(A.P.recal, s, wl[k], wr[k]);
+      }
+    }
+    // u^mu reconstruction for the viscous derivatives (work_rec(n,1,4,1))
+    if (T::VISC) {
+      double s[4][6];
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        int j = i - 2 + q;
+        double vx = ghost_val(A.v + (size_t)KVX * g.ncell, base, stride, n, j, A.bc.c[KVX][0], A.bc.c[KVX][1]);
+        double vy = ghost_val(A.v + (size_t)KVY * g.ncell, base, stride, n, j, A.bc.c[KVY][0], A.bc.c[KVY][1]);
+        double vz = ghost_val(A.v + (size_t)KVZ * g.ncell, base, stride, n, j, A.bc.c[KVZ][0], A.bc.c[KVZ][1]);
+        double gg = 1. / sqrt(1. - vx * vx - vy * vy - M.g3 * (vz * vz));
+        s[0][q] = gg;
+        s[1][q] = gg * vx;
+        s[2][q] = gg * vy;
+        s[3][q] = gg * vz;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        double l, r;
+        recon_face(A.P.recal, s[c], l, r);
+        A.WD[(size_t)c * nfaces + fid] = l;
+        A.WD[(size_t)(4 + c) * nfaces + fid] = r;
+      }
+    }
+    // fix-ups (evolve.f90:334-369); w0 = the cell left of the face
+    {
+      double v2;
+      if (wr[KPR] <= 0) wr[KPR] = w0[KPR];
+      v2 = 0;
+      v2 = v2 + wr[KVX] * wr[KVX] * M.g1;
+      v2 = v2 + wr[KVY] * wr[KVY] * M.g2;
+      v2 = v2 + wr[KVZ] * wr[KVZ] * M.g3;
+      if (v2 >= 1.) {
+        wr[KVX] = w0[KVX];
+        wr[KVY] = w0[KVY];
+        wr[KVZ] = w0[KVZ];
+        v2 = 0;
+        v2 = v2 + wr[KVX] * wr[KVX] * M.g1;
+        v2 = v2 + wr[KVY] * wr[KVY] * M.g2;
+        v2 = v2 + wr[KVZ] * wr[KVZ] * M.g3;
+        if (v2 >= 1) {
+#pragma unroll
+          for (int k = KVX; k <= KVZ; k++) {
+            w0[k] = w0[k] * A.P.maxspeed / (sqrt(v2));
+            wr[k] = w0[k];
+          }
+        }
+      }
+      if (wl[KPR] <= 0) wl[KPR] = w0[KPR];
+      v2 = 0;
+      v2 = v2 + wl[KVX] * wl[KVX] * M.g1;
+      v2 = v2 + wl[KVY] * wl[KVY] * M.g2;
+      v2 = v2 + wl[KVZ] * wl[KVZ] * M.g3;
+      if (v2 >= 1.) {
+        wl[KVX] = w0[KVX];
+        wl[KVY] = w0[KVY];
+        wl[KVZ] = w0[KVZ];
+        v2 = 0;
+        v2 = v2 + wl[KVX] * wl[KVX] * M.g1;
+        v2 = v2 + wl[KVY] * wl[KVY] * M.g2;
+        v2 = v2 + wl[KVZ] * wl[KVZ] * M.g3;
+        if (v2 >= 1) {
+#pragma unroll
+          for (int k = KVX; k <= KVZ; k++) {
+            w0[k] = w0[k] * A.P.maxspeed / (sqrt(v2));
+            wl[k] = w0[k];
+          }
+        }
+      }
+    }
+    // GLM upwinding (work_glm[xyz], work.f90:67-139)
+    if (T::GLM) {
+      const int kb = DIR == 0 ? KBX : DIR == 1 ? KBY : KBZ;
+      double ch = A.sc->glm_ch_old;
+      wl[KGLM] = 0.5 * (wl[KGLM] + wr[KGLM]) - (wr[kb] - wl[kb]) * ch / 2;
+      wr[KGLM] = wl[KGLM];
+      wl[kb] = 0.5 * (wl[kb] + wr[kb]) - (wr[KGLM] - wl[KGLM]) / (2 * ch);
+      wr[kb] = wl[kb];
+    }
+    // HLL (work.f90:195-229)
+    double ul[NV], ur[NV], fl[NV], fr[NV];
+    double vflp, vflm, vfrp, vfrm;
+    int err = system_flux<KIND, DIR + 1>(A.P, M, wl, ul, fl, vflp, vflm);
+    if (!err) err = system_flux<KIND, DIR + 1>(A.P, M, wr, ur, fr, vfrp, vfrm);
+    if (err) {
+      size_t cell = base + (size_t)((i >= 1 ? i : 1) - 1) * stride;
+      atomicMin(&A.sc->err_key, ((unsigned long long)cell << 20) | (unsigned long long)err);
+#pragma unroll
+      for (int k = 0; k < NV; k++) A.F[(size_t)k * nfaces + fid] = 0.0;
+    } else {
+      double ap = 0., am = 0.;
+      if (vflp > ap) ap = vflp;
+      if (vfrp > ap) ap = vfrp;
+      if (-vflm > am) am = -vflm;
+      if (-vfrm > am) am = -vfrm;
+      amax_local = ap > am ? ap : am;
+      double a1 = (ap == 0.0 && am == 0.0) ? 1. : 1. / (ap + am);
+#pragma unroll
+      for (int k = 0; k < NV; k++)
+        A.F[(size_t)k * nfaces + fid] = a1 * (ap * fl[k] + am * fr[k] - ap * am * (ur[k] - ul[k]));
+      // GLM speed of the reference: the last face of the last pencil (work.f90:217,310,401)
+      int na = DIR == 0 ? g.ny : g.nx;
+      int nb = DIR == 2 ? g.ny : g.nz;
+      if (i == n && a == na && b == nb) A.sc->aflux[DIR] = amax_local;
+    }
+  }
+  // block max of the signal speed -> one atomic per block (CFL reduction, evolve.f90:723-764)
+  __shared__ double red[4];
+  double m = amax_local;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double x = __shfl_xor_sync(0xffffffffu, m, o);
+    m = x > m ? x : m;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = red[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) mm = red[w] > mm ? red[w] : mm;
+    if (mm > 0.0) atomicMax(&A.sc->amax_bits[DIR], (unsigned long long)__double_as_longlong(mm));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scalar logic of evolve_main (evolve.f90:156-201) and evolve_dt (:723-764)
+// ---------------------------------------------------------------------------
+struct ScalarArgs {
+  DevScalars* sc;
+  Grid g;
+  double cfl, maxdt, glm_alpha;
+  int irk, nrk, divclean;
+};
+
+static __global__ void stage_scalars_kernel(ScalarArgs A) {
+  DevScalars* sc = A.sc;
+  // glm_ch = glm_ch_old (start of stage); glm_ch_old = maxval(aflux) (end of sweeps)
+  sc->glm_ch = sc->glm_ch_old;
+  double m = sc->aflux[0];
+  if (sc->aflux[1] > m) m = sc->aflux[1];
+  if (sc->aflux[2] > m) m = sc->aflux[2];
+  sc->glm_ch_old = m;
+  if (A.irk == 1) {
+    double amax;
+    if (A.divclean) {
+      amax = 1;
+    } else {
+      amax = 0.;
+      double c;
+      if (A.g.nx > 1) {
+        c = A.g.ddx * __longlong_as_double((long long)sc->amax_bits[0]);
+        if (c > amax) amax = c;
+      }
+      if (A.g.ny > 1) {
+        c = A.g.ddy * __longlong_as_double((long long)sc->amax_bits[1]);
+        if (c > amax) amax = c;
+      }
+      if (A.g.nz > 1) {
+        c = A.g.ddz * __longlong_as_double((long long)sc->amax_bits[2]);
+        if (c > amax) amax = c;
+      }
+      if (amax == 0) {
+        if (A.g.nx > 1 && A.g.ddx > amax) amax = A.g.ddx;
+        if (A.g.ny > 1 && A.g.ddy > amax) amax = A.g.ddy;
+        if (A.g.nz > 1 && A.g.ddz > amax) amax = A.g.ddz;
+      }
+    }
+    double dtl = A.cfl / amax;
+    if (A.maxdt < dtl) dtl = A.maxdt;
+    if (sc->tout - sc->t < dtl) dtl = sc->tout - sc->t;
+    if (fabs(sc->t + sc->dt - sc->tout) < 1.e-9) {
+      dtl = sc->tout - sc->t;
+    } else {
+      if ((sc->t + 2. * dtl - sc->tout) > 1.e-9) dtl = (sc->tout - sc->t) / 2.;
+    }
+    sc->dt = dtl;
+  }
+  if (A.divclean) sc->expfact = exp(-sc->glm_ch * sc->glm_ch * A.glm_alpha * (sc->dt / 2.));
+  sc->amax_bits[0] = sc->amax_bits[1] = sc->amax_bits[2] = 0ull;
+}
+
+// end of step (echo.f90:211-241)
+static __global__ void end_step_kernel(DevScalars* sc, int coordinates) {
+  sc->timeold = sc->t;
+  sc->t = sc->t + sc->dt;
+  double g3 = coordinates == ECHO_BJORKEN ? sc->timeold * sc->timeold : 1.;
+  sc->g3old = g3;
+  sc->t3 = pow(sc->t, 3.);
+  sc->timeinterval = sc->dt;
+  if ((sc->t > sc->tout) || ((sc->tout - sc->t) < 1.e-10)) {
+    sc->tout = sc->tout + sc->dtout;
+    if ((fabs(sc->tout - sc->tmax) < 1.e-10) || (sc->tout > sc->tmax)) sc->tout = sc->tmax;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-cell update
+// ---------------------------------------------------------------------------
+enum { MODE_RK = 0, MODE_RHS = 1 };
+
+struct UpdateArgs {
+  DevPhys P;
+  Grid g;
+  const double* __restrict__ Fx;
+  const double* __restrict__ Fy;
+  const double* __restrict__ Fz;
+  const double* __restrict__ WDx;
+  const double* __restrict__ WDy;
+  const double* __restrict__ WDz;
+  const double* __restrict__ vin;    // stage input primitives (guess for con2prim)
+  double* __restrict__ vout;         // new primitives
+  double* uin;                       // current conserved (updated in place)
+  double* uout;                      // written u (== uin except stage 1)
+  double* u0;                        // u at the start of the step
+  const double* __restrict__ vnew;   // vnewstep (viscous time derivatives)
+  const double* __restrict__ vold;   // vold
+  double* du_out;                    // MODE_RHS: du
+  unsigned char* fail;
+  DevScalars* sc;
+  double c1, c2;
+  int irk, nrk, divclean, coordinates, algo, mode;
+  double tol;
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  const Grid& g = A.g;
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_iters = 0;
+  if (c < g.ncell) {
+    int ix = (int)(c % g.nx);
+    size_t r = c / g.nx;
+    int iy = (int)(r % g.ny);
+    int iz = (int)(r / g.ny);
+    const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+    const size_t nfx = (size_t)(g.nx + 1) * g.ny * g.nz;
+    const size_t nfy = (size_t)g.nx * (g.ny + 1) * g.nz;
+    const size_t nfz = (size_t)g.nx * g.ny * (g.nz + 1);
+    const size_t fx = ((size_t)iz * g.ny + iy) * (g.nx + 1) + ix;       // face ix-1/2 -> index ix
+    const size_t fy = ((size_t)iz * (g.ny + 1) + iy) * g.nx + ix;
+    const size_t fz = ((size_t)iz * g.ny + iy) * g.nx + ix;
+    double vv[NV], src[NV], du[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) vv[k] = A.vin[(size_t)k * g.ncell + c];
+    // flux divergence in the reference's order: du = 0; += x; += y; += z
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double d = 0.;
+      if (g.nx > 1) d = d + g.ddx * (A.Fx[(size_t)k * nfx + fx + 1] - A.Fx[(size_t)k * nfx + fx]);
+      if (g.ny > 1) d = d + g.ddy * (A.Fy[(size_t)k * nfy + fy + g.nx] - A.Fy[(size_t)k * nfy + fy]);
+      if (g.nz > 1)
+        d = d + g.ddz * (A.Fz[(size_t)k * nfz + fz + (size_t)g.nx * g.ny] - A.Fz[(size_t)k * nfz + fz]);
+      du[k] = d;
+    }
+    // sources (evolve_src, evolve.f90:689-718)
+    double dv[NDER];
+    if (T::VISC) {
+#pragma unroll
+      for (int q = 0; q < NDER; q++) dv[q] = 0.;
+      const int dk[3][4] = {{DTX, DXX, DYX, DZX}, {DTY, DXY, DYY, DZY}, {DTZ, DXZ, DYZ, DZZ}};
+      if (g.nx > 1) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dv[dk[0][q]] = g.ddx * 0.5 *
+                         (A.WDx[(size_t)q * nfx + fx + 1] + A.WDx[(size_t)(4 + q) * nfx + fx + 1] -
+                          A.WDx[(size_t)q * nfx + fx] - A.WDx[(size_t)(4 + q) * nfx + fx]);
+      }
+      if (g.ny > 1) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dv[dk[1][q]] = g.ddy * 0.5 *
+                         (A.WDy[(size_t)q * nfy + fy + g.nx] + A.WDy[(size_t)(4 + q) * nfy + fy + g.nx] -
+                          A.WDy[(size_t)q * nfy + fy] - A.WDy[(size_t)(4 + q) * nfy + fy]);
+      }
+      if (g.nz > 1) {
+        size_t s = (size_t)g.nx * g.ny;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dv[dk[2][q]] = g.ddz * 0.5 *
+                         (A.WDz[(size_t)q * nfz + fz + s] + A.WDz[(size_t)(4 + q) * nfz + fz + s] -
+                          A.WDz[(size_t)q * nfz + fz] - A.WDz[(size_t)(4 + q) * nfz + fz]);
+      }
+      // dts (viscous.f90:56-97)
+      double ti = A.sc->timeinterval;
+      if (ti != 0) {
+        double vxo = A.vold[1 * g.ncell + c], vyo = A.vold[2 * g.ncell + c], vzo = A.vold[3 * g.ncell + c];
+        double vx = A.vnew[1 * g.ncell + c], vy = A.vnew[2 * g.ncell + c], vz = A.vnew[3 * g.ncell + c];
+        double gamma1 = 1. / sqrt(1. - M.g1 * (vxo * vxo) - M.g2 * (vyo * vyo) - A.sc->g3old * (vzo * vzo));
+        double gamma2 = 1. / sqrt(1. - M.g1 * (vx * vx) - M.g2 * (vy * vy) - M.g3 * (vz * vz));
+        dv[DTT] = (gamma2 - gamma1) / (ti);
+        dv[DXT] = (gamma2 * vx - gamma1 * vxo) / ti;
+        dv[DYT] = (gamma2 * vy - gamma1 * vyo) / ti;
+        dv[DZT] = (gamma2 * vz - gamma1 * vzo) / ti;
+      }
+    }
+    {
+      double vs[NV];
+#pragma unroll
+      for (int k = 0; k < NV; k++) vs[k] = vv[k];
+      int err = system_source<KIND>(A.P, M, vs, dv, src);
+      if (err) atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
+    }
+#pragma unroll
+    for (int k = 0; k < NV; k++) du[k] = du[k] - src[k];
+    if (A.mode == MODE_RHS) {
+#pragma unroll
+      for (int k = 0; k < NV; k++) A.du_out[(size_t)k * g.ncell + c] = du[k];
+    } else {
+      // RK combination (evolve.f90:196-201)
+      const double dt = A.sc->dt;
+      double uu[NV];
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        double ui = A.uin[(size_t)k * g.ncell + c];
+        if (T::GLM && k == KGLM && A.irk == 1) {
+          ui = ui * A.sc->expfact;
+          A.uin[(size_t)k * g.ncell + c] = ui;  // u0 = u after the GLM half step
+        }
+        double u0 = A.irk == 1 ? ui : A.u0[(size_t)k * g.ncell + c];
+        uu[k] = A.c1 * u0 + A.c2 * (ui - dt * du[k]);
+      }
+      if (T::GLM && A.irk == A.nrk) uu[KGLM] = uu[KGLM] * A.sc->expfact;
+#pragma unroll
+      for (int k = 0; k < NV; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
+      // con2prim (evolve_u2v, evolve.f90:789-866)
+      int it = 0;
+      int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+      my_iters = (unsigned long long)it;
+      if (err) {
+        A.fail[c] = 1;
+        atomicAdd(&A.sc->nfail, 1);
+      } else {
+        A.fail[c] = 0;
+#pragma unroll
+        for (int k = 0; k < NV; k++) A.vout[(size_t)k * g.ncell + c] = vv[k];
+      }
+    }
+  }
+  if (A.mode == MODE_RK) {
+    // per-block sum of iteration counts
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+    if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// repair of failed cells (evolve.f90:795-842) in Fortran loop order
+// ---------------------------------------------------------------------------
+struct RepairArgs {
+  DevPhys P;
+  Grid g;
+  const double* __restrict__ vold;  // stage input primitives (old v)
+  double* vnew;                     // new primitives (filled for good cells)
+  double* u;                        // conserved after the RK update
+  unsigned char* fail;
+  DevScalars* sc;
+  int coordinates, algo;
+  double maxspeed, tol;
+};
+
+template <int KIND>
+__device__ double flat_v(const RepairArgs& A, long long off, size_t cell) {
+  // Fortran flat address into v: cells before `cell` hold their new value
+  size_t tot = A.g.ncell * Traits<KIND>::NV;
+  if (off < 0 || (size_t)off >= tot) return 0.;
+  size_t cc = (size_t)off % A.g.ncell;
+  return cc < cell ? A.vnew[off] : A.vold[off];
+}
+__device__ __forceinline__ double flat_u(const double* u, size_t tot, long long off) {
+  if (off < 0 || (size_t)off >= tot) return 0.;
+  return u[off];
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(256) repair_kernel(RepairArgs A) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  if (A.sc->nfail == 0) return;
+  const Grid& g = A.g;
+  __shared__ int s_any, s_stop;
+  const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  if (threadIdx.x == 0) s_stop = 0;
+  for (size_t chunk = 0; chunk < g.ncell; chunk += blockDim.x) {
+    size_t c = chunk + threadIdx.x;
+    int f = (c < g.ncell) ? A.fail[c] : 0;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    if (f) atomicOr(&s_any, 1);
+    __syncthreads();
+    int any = s_any;
+    __syncthreads();  // everyone has read s_any before thread 0 resets it
+    if (!any) continue;
+    if (threadIdx.x == 0) {
+      for (unsigned t = 0; t < blockDim.x && chunk + t < g.ncell; t++) {
+        size_t cell = chunk + t;
+        if (!A.fail[cell]) continue;
+        A.sc->repairs++;
+        double uu[NV], vv[NV];
+        int it;
+        for (int k = 0; k < NV; k++) vv[k] = A.vold[(size_t)k * g.ncell + cell];
+        for (int k = 0; k < NV; k++) uu[k] = A.u[(size_t)k * g.ncell + cell];
+        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+        size_t totu = g.ncell * NV;
+        long long nx = g.nx, nxy = (long long)g.nx * g.ny;
+        for (int k = 0; k < NV; k++) {
+          long long o = (long long)k * g.ncell + (long long)cell;
+          double s = flat_u(A.u, totu, o - 1) + flat_u(A.u, totu, o + 1) + flat_u(A.u, totu, o - nx) +
+                     flat_u(A.u, totu, o + nx) + flat_u(A.u, totu, o - nxy) + flat_u(A.u, totu, o + nxy);
+          A.u[o] = s / 6.;
+          uu[k] = A.u[o];
+        }
+        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+        double v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
+        if (v2 > 1) {
+          double fac = A.maxspeed / sqrt(v2);
+          vv[KVX] = fac * vv[KVX];
+          vv[KVY] = fac * vv[KVY];
+          vv[KVZ] = fac * vv[KVZ];
+        }
+        if (vv[KPR] < 0) {
+          long long o = (long long)KPR * g.ncell + (long long)cell;
+          double pxl = flat_v<KIND>(A, o - 1, cell), pxr = flat_v<KIND>(A, o + 1, cell);
+          double pyl = flat_v<KIND>(A, o - nx, cell), pyr = flat_v<KIND>(A, o + nx, cell);
+          double pzl = flat_v<KIND>(A, o - nxy, cell), pzr = flat_v<KIND>(A, o + nxy, cell);
+          vv[KPR] = (pxl + pxr + pyl + pyr + pzl + pzr) / 6.;
+        }
+        (void)prim2cons<KIND>(A.P, M, vv, uu);
+        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+        v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
+        bool ok = (vv[KPR] > 0) && (v2 < 1);
+        if (T::VISC && A.P.obtained_zz) A.vnew[(size_t)KPIZZ * g.ncell + cell] = vv[KPIZZ];
+        for (int k = 0; k < NV; k++) A.u[(size_t)k * g.ncell + cell] = uu[k];
+        if (!ok) {
+          // the run crashes here (evolve.f90:836-858): stop repairing
+          atomicMin(&A.sc->err_key, ((unsigned long long)cell << 20) | 1ull);
+          s_stop = 1;
+          break;
+        }
+        for (int k = 0; k < NV; k++) A.vnew[(size_t)k * g.ncell + cell] = vv[k];
+      }
+    }
+    __syncthreads();
+    if (s_stop) break;
+  }
+}
+
+// evolve_smooth_viscosity (evolve.f90:1159-1207)
+struct SmoothArgs {
+  DevPhys P;
+  Grid g;
+  double* v;
+  double* u;
+  DevScalars* sc;
+  int coordinates;
+  double smooth_pressure;
+};
+
+template <int KIND>
+__global__ void smooth_kernel(SmoothArgs A) {
+  typedef Traits<KIND> T;
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= A.g.ncell) return;
+  double pr = A.v[(size_t)KPR * A.g.ncell + c];
+  if (!(pr < A.smooth_pressure)) return;
+  const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  double vv[T::NV], uu[T::NV];
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) vv[k] = A.v[(size_t)k * A.g.ncell + c];
+  double rr = vv[KPR] / A.smooth_pressure;
+  double fac = rr * rr;
+#pragma unroll
+  for (int k = KPIBU; k <= KPIZZ; k++) vv[k] = vv[k] * fac;
+  if (A.P.obtained_zz) {
+    Pit pi;
+    derived_pi_zz(M, vv, pi);
+    vv[KPIZZ] = pi.zz;
+  }
+  int err = prim2cons<KIND>(A.P, M, vv, uu);
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) {
+    A.v[(size_t)k * A.g.ncell + c] = vv[k];
+    A.u[(size_t)k * A.g.ncell + c] = uu[k];
+  }
+  if (err) atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
+}
+
+// system_prim2cons over the grid (state upload without u)
+template <int KIND>
+__global__ void prim2cons_kernel(DevPhys P, Grid g, int coordinates, DevScalars* sc, double* v, double* u) {
+  typedef Traits<KIND> T;
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.ncell) return;
+  const Metric M = make_metric(coordinates, sc->t, sc->t3);
+  double vv[T::NV], uu[T::NV];
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) vv[k] = v[(size_t)k * g.ncell + c];
+  int err = prim2cons<KIND>(P, M, vv, uu);
+  if (err) atomicMin(&sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) {
+    v[(size_t)k * g.ncell + c] = vv[k];
+    u[(size_t)k * g.ncell + c] = uu[k];
+  }
+}
+
+}  // namespace echo

@@ -1,0 +1,167 @@
+// unit_tests.cu -- kernel-level entry points for parity tests
+// (echo_gpu_test_recon, echo_gpu_test_c2p in include/echo_gpu.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../../include/echo_gpu.h"
+#include "ctx.cuh"
+
+#define CK(x)                                                                               \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess) {                                                                \
+      fprintf(stderr, "echo_gpu: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), __FILE__, \
+              __LINE__);                                                                    \
+      return ECHO_ERR_CUDA;                                                                 \
+    }                                                                                       \
+  } while (0)
+
+bool echo_make_buckets(const double* arr, int n, std::vector<int>& bk, long long& k0);
+int echo_kind_of(const EchoParams* p);
+int echo_nv_of(int kind);
+
+// ---------------------------------------------------------------------------
+// kernel-level entry points for parity tests
+// ---------------------------------------------------------------------------
+namespace echo {
+__global__ void recon_test_kernel(int recal, int m, int n, const double* f, double* gl, double* gr) {
+  size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= (size_t)m * (n + 1)) return;
+  int row = (int)(id / (n + 1)), i = (int)(id % (n + 1));
+  const double* fr = f + (size_t)row * (n + 8) + 4;  // fr[j] = f(j)
+  double s[6];
+  for (int q = 0; q < 6; q++) s[q] = fr[i - 2 + q];
+  double l, r;
+  recon_face(recal, s, l, r);
+  gl[id] = l;
+  gr[id] = r;
+}
+
+template <int KIND>
+__global__ void c2p_test_kernel(DevPhys P, Metric M, int algo, double tol, int ncells, const double* u, double* v,
+                                int* err, int* iters) {
+  typedef Traits<KIND> T;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  double uu[T::NV], vv[T::NV];
+  for (int k = 0; k < T::NV; k++) {
+    uu[k] = u[(size_t)c * T::NV + k];
+    vv[k] = v[(size_t)c * T::NV + k];
+  }
+  int it = 0;
+  int e = cons2prim<KIND>(P, M, algo, tol, uu, vv, &it);
+  for (int k = 0; k < T::NV; k++) v[(size_t)c * T::NV + k] = vv[k];
+  if (err) err[c] = e;
+  if (iters) iters[c] = it;
+}
+}  // namespace echo
+
+template <int KIND>
+static void launch_c2p_test(DevPhys P, Metric M, int algo, double tol, int ncells, const double* u, double* v,
+                            int* err, int* iters) {
+  c2p_test_kernel<KIND><<<(ncells + 127) / 128, 128>>>(P, M, algo, tol, ncells, u, v, err, iters);
+}
+
+extern "C" int echo_gpu_test_recon(int recal, int m, int n, const double* f, double* gl, double* gr) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (m <= 0 || n <= 0 || !f || !gl || !gr) return ECHO_ERR_ARG;
+  size_t nf = (size_t)m * (n + 8), nfc = (size_t)m * (n + 1);
+  double *df, *dl, *dr;
+  CK(cudaMalloc(&df, nf * sizeof(double)));
+  CK(cudaMalloc(&dl, nfc * sizeof(double)));
+  CK(cudaMalloc(&dr, nfc * sizeof(double)));
+  CK(cudaMemcpy(df, f, nf * sizeof(double), cudaMemcpyHostToDevice));
+  recon_test_kernel<<<(unsigned)((nfc + 127) / 128), 128>>>(recal, m, n, df, dl, dr);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(gl, dl, nfc * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(gr, dr, nfc * sizeof(double), cudaMemcpyDeviceToHost));
+  cudaFree(df);
+  cudaFree(dl);
+  cudaFree(dr);
+  return ECHO_OK;
+}
+
+extern "C" int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, int n_eos, int ncells, double g3,
+                                 double gp, const double* u, double* v, int* err, int* iters) {
+  if (!p || ncells <= 0 || !u || !v) return ECHO_ERR_ARG;
+  (void)cudaGetLastError();
+  int kind = echo_kind_of(p), nv = echo_nv_of(kind);
+  size_t nb = (size_t)ncells * nv * sizeof(double);
+  double *du, *dv, *dtab = nullptr;
+  int *derr, *dit;
+  CK(cudaMalloc(&du, nb));
+  CK(cudaMalloc(&dv, nb));
+  CK(cudaMalloc(&derr, ncells * sizeof(int)));
+  CK(cudaMalloc(&dit, ncells * sizeof(int)));
+  CK(cudaMemcpy(du, u, nb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dv, v, nb, cudaMemcpyHostToDevice));
+  DevPhys P;
+  memset(&P, 0, sizeof(P));
+  int* dbk = nullptr;
+  if (eos_table && n_eos > 0) {
+    std::vector<double> cols((size_t)4 * n_eos);
+    for (int i = 0; i < n_eos; i++)
+      for (int q = 0; q < 4; q++) cols[(size_t)q * n_eos + i] = eos_table[4 * i + q];
+    CK(cudaMalloc(&dtab, sizeof(double) * 4 * n_eos));
+    CK(cudaMemcpy(dtab, cols.data(), sizeof(double) * 4 * n_eos, cudaMemcpyHostToDevice));
+    P.nt = n_eos;
+    P.tT = dtab;
+    P.te = dtab + n_eos;
+    P.tp = dtab + 2 * n_eos;
+    P.tc = dtab + 3 * n_eos;
+    std::vector<int> be, bp;
+    long long ke0 = 0, kp0 = 0;
+    if (echo_make_buckets(cols.data() + n_eos, n_eos, be, ke0) && echo_make_buckets(cols.data() + 2 * n_eos, n_eos, bp, kp0)) {
+      CK(cudaMalloc(&dbk, sizeof(int) * (be.size() + bp.size())));
+      CK(cudaMemcpy(dbk, be.data(), sizeof(int) * be.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(dbk + be.size(), bp.data(), sizeof(int) * bp.size(), cudaMemcpyHostToDevice));
+      P.bke = dbk;
+      P.bkp = dbk + be.size();
+      P.bke0 = ke0;
+      P.bkp0 = kp0;
+      P.nbke = (int)be.size();
+      P.nbkp = (int)bp.size();
+    }
+  }
+  P.eqstate = p->eqstate;
+  P.coordinates = p->coordinates;
+  P.recal = p->recal;
+  P.obtained_zz = p->obtained_zz;
+  P.init_type = p->init_type;
+  P.bulkvis = p->bulkvis;
+  P.maxspeed = p->maxspeed;
+  P.eta_over_s = p->eta_over_s;
+  P.tau_pi_coeff = p->tau_pi_coeff;
+  P.enezero = p->enezero;
+  P.przero = p->przero;
+  P.glm_alpha = p->glm_alpha;
+  Metric M;
+  M.g0 = -1.;
+  M.g1 = 1.;
+  M.g2 = 1.;
+  M.g3 = g3;
+  M.gp = gp;
+  M.gm = 1. / gp;
+  M.t = gp;
+  M.t3 = pow(gp, 3.);
+  switch (kind) {
+    case KIND_HD: launch_c2p_test<KIND_HD>(P, M, p->algo_solver, p->c2p_tol, ncells, du, dv, derr, dit); break;
+    case KIND_VISC: launch_c2p_test<KIND_VISC>(P, M, p->algo_solver, p->c2p_tol, ncells, du, dv, derr, dit); break;
+    case KIND_MHD: launch_c2p_test<KIND_MHD>(P, M, p->algo_solver, p->c2p_tol, ncells, du, dv, derr, dit); break;
+    default: launch_c2p_test<KIND_MHDGLM>(P, M, p->algo_solver, p->c2p_tol, ncells, du, dv, derr, dit); break;
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(v, dv, nb, cudaMemcpyDeviceToHost));
+  if (err) CK(cudaMemcpy(err, derr, ncells * sizeof(int), cudaMemcpyDeviceToHost));
+  if (iters) CK(cudaMemcpy(iters, dit, ncells * sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(du);
+  cudaFree(dv);
+  cudaFree(derr);
+  cudaFree(dit);
+  cudaFree(dtab);
+  cudaFree(dbk);
+  return ECHO_OK;
+}

@@ -1,0 +1,231 @@
+"""ctypes binding of libechogpu.so and the host-side mirror of the
+reference's step interface.
+
+``Evolve`` mirrors the Fortran module `evolve` (evolve.f90): evolve_main(irk)
+returns dt and raises on a crashed stage exactly where the reference sets
+run_crashed; step() is one iteration of the time loop of echo.f90:185-262.
+There is no CPU fallback: constructing an ``Evolve`` without the CUDA
+library or without a GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .params import EchoParams
+
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(_ROOT, "lib")
+_libs: dict[str, ctypes.CDLL] = {}
+
+D = ctypes.POINTER(ctypes.c_double)
+I = ctypes.POINTER(ctypes.c_int)
+P = ctypes.c_void_p
+
+
+class EchoStats(ctypes.Structure):
+    _fields_ = [
+        ("dt", ctypes.c_double), ("t", ctypes.c_double), ("glm_ch", ctypes.c_double),
+        ("c2p_iters", ctypes.c_longlong), ("c2p_cells", ctypes.c_longlong),
+        ("repairs", ctypes.c_longlong), ("seed_fallbacks", ctypes.c_longlong),
+        ("errcode", ctypes.c_int), ("err_cell", ctypes.c_int),
+    ]
+
+
+FUNCTIONS = {
+    "echo_gpu_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.POINTER(P)]),
+    "echo_gpu_free": (ctypes.c_int, [P]),
+    "echo_gpu_nv": (ctypes.c_int, [P]),
+    "echo_gpu_upload": (ctypes.c_int, [P, D, D, ctypes.c_double]),
+    "echo_gpu_download": (ctypes.c_int, [P, D, D]),
+    "echo_gpu_upload_device": (ctypes.c_int, [P, P, P, ctypes.c_double]),
+    "echo_gpu_download_device": (ctypes.c_int, [P, P, P]),
+    "echo_gpu_set_tout": (ctypes.c_int, [P, ctypes.c_double]),
+    "echo_gpu_evolve_main": (ctypes.c_int, [P, ctypes.c_int, D, I]),
+    "echo_gpu_end_step": (ctypes.c_int, [P]),
+    "echo_gpu_step": (ctypes.c_int, [P, D, I]),
+    "echo_gpu_run": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_gpu_stats": (ctypes.c_int, [P, ctypes.POINTER(EchoStats)]),
+    "echo_gpu_sync": (ctypes.c_int, [P]),
+    "echo_gpu_rhs": (ctypes.c_int, [P, D, D]),
+    "echo_gpu_stream": (ctypes.c_int, [P, ctypes.POINTER(P)]),
+    "echo_gpu_put_state": (ctypes.c_int, [P, P, P]),
+    "echo_gpu_get_state": (ctypes.c_int, [P, P, P]),
+    "echo_gpu_profile_step": (ctypes.c_int, [P, D, I]),
+    "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
+    "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, D, D, I, I]),
+}
+
+
+def library_path(exact: bool = False) -> str:
+    return os.path.join(LIBDIR, "libechogpu_exact.so" if exact else "libechogpu.so")
+
+
+def load(exact: bool = False) -> ctypes.CDLL:
+    """Load the CUDA library; raises if it has not been built."""
+    path = library_path(exact)
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library {path} is missing: run __graft_entry__.build()")
+    L = ctypes.CDLL(path)
+    for name, (res, args) in FUNCTIONS.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _libs[path] = L
+    return L
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(D)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(I)
+
+
+class CrashError(RuntimeError):
+    """A stage failed: the reference would set run_crashed (echo.f90:206)."""
+
+    def __init__(self, code: int, cell: int = -1):
+        super().__init__(f"run crashed, reference error code {code} at cell {cell}")
+        self.code = code
+        self.cell = cell
+
+
+class Evolve:
+    """Device-resident state and the step of evolve.f90 behind the C-ABI."""
+
+    def __init__(self, params: EchoParams, eos_table=None, exact: bool = False):
+        self.lib = load(exact)
+        self.params = params
+        self._tab = None if eos_table is None else np.ascontiguousarray(eos_table, dtype=np.float64)
+        n = 0 if self._tab is None else len(self._tab)
+        h = P()
+        rc = self.lib.echo_gpu_init(ctypes.byref(params), _dp(self._tab), n, ctypes.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"echo_gpu_init failed with status {rc}")
+        self.h = h
+        self.nv = self.lib.echo_gpu_nv(h)
+        self.ncell = params.nx * params.ny * params.nz
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.echo_gpu_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed with status {rc}")
+
+    def upload(self, v, u=None, t: float = 0.4):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        u = None if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        self._check(self.lib.echo_gpu_upload(self.h, _dp(v), _dp(u), t), "upload")
+
+    def upload_device(self, v_ptr: int, u_ptr: int | None, t: float):
+        self._check(self.lib.echo_gpu_upload_device(self.h, v_ptr, u_ptr, t), "upload_device")
+
+    def download(self):
+        v = np.empty(self.ncell * self.nv)
+        u = np.empty(self.ncell * self.nv)
+        self._check(self.lib.echo_gpu_download(self.h, _dp(v), _dp(u)), "download")
+        return v, u
+
+    def download_device(self, v_ptr: int, u_ptr: int | None):
+        self._check(self.lib.echo_gpu_download_device(self.h, v_ptr, u_ptr), "download_device")
+
+    def put_state(self, v_host_ptr: int, u_host_ptr: int):
+        self._check(self.lib.echo_gpu_put_state(self.h, v_host_ptr, u_host_ptr), "put_state")
+
+    def get_state(self, v_host_ptr: int, u_host_ptr: int | None):
+        self._check(self.lib.echo_gpu_get_state(self.h, v_host_ptr, u_host_ptr), "get_state")
+
+    def set_tout(self, tout: float):
+        self._check(self.lib.echo_gpu_set_tout(self.h, tout), "set_tout")
+
+    def evolve_main(self, irk: int) -> float:
+        dt = ctypes.c_double(0)
+        code = ctypes.c_int(0)
+        self._check(self.lib.echo_gpu_evolve_main(self.h, irk, ctypes.byref(dt), ctypes.byref(code)),
+                    "evolve_main")
+        if code.value:
+            raise CrashError(code.value)
+        return dt.value
+
+    def end_step(self):
+        self._check(self.lib.echo_gpu_end_step(self.h), "end_step")
+
+    def step(self) -> float:
+        dt = ctypes.c_double(0)
+        code = ctypes.c_int(0)
+        self._check(self.lib.echo_gpu_step(self.h, ctypes.byref(dt), ctypes.byref(code)), "step")
+        if code.value:
+            raise CrashError(code.value)
+        return dt.value
+
+    def run(self, nsteps: int):
+        self._check(self.lib.echo_gpu_run(self.h, nsteps), "run")
+
+    def sync(self):
+        self._check(self.lib.echo_gpu_sync(self.h), "sync")
+
+    def stats(self) -> EchoStats:
+        st = EchoStats()
+        self._check(self.lib.echo_gpu_stats(self.h, ctypes.byref(st)), "stats")
+        return st
+
+    def stream_handle(self) -> int:
+        s = P()
+        self._check(self.lib.echo_gpu_stream(self.h, ctypes.byref(s)), "stream")
+        return s.value or 0
+
+    KERNEL_CLASSES = ("faces_x", "faces_y", "faces_z", "stage_scalars", "update_c2p", "repair", "end_step")
+
+    def profile_step(self):
+        ms = np.zeros(7)
+        n = np.zeros(7, dtype=np.int32)
+        self._check(self.lib.echo_gpu_profile_step(self.h, _dp(ms), _ip(n)), "profile_step")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def rhs(self):
+        du = np.empty(self.ncell * self.nv)
+        am = np.empty(3)
+        rc = self.lib.echo_gpu_rhs(self.h, _dp(du), _dp(am))
+        if rc < 0:
+            raise RuntimeError(f"rhs failed with status {rc}")
+        return du, am
+
+
+def unit_recon(recal: int, f: np.ndarray, n: int, exact: bool = True):
+    L = load(exact)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    m = f.shape[0]
+    gl = np.empty((m, n + 1))
+    gr = np.empty((m, n + 1))
+    rc = L.echo_gpu_test_recon(recal, m, n, _dp(f), _dp(gl), _dp(gr))
+    if rc:
+        raise RuntimeError(f"test_recon status {rc}")
+    return gl, gr
+
+
+def unit_c2p(params, eos_table, g3, gp, u, vguess, exact: bool = True):
+    L = load(exact)
+    tab = None if eos_table is None else np.ascontiguousarray(eos_table, dtype=np.float64)
+    n = 0 if tab is None else len(tab)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    v = np.ascontiguousarray(vguess, dtype=np.float64).copy()
+    nc = u.shape[0]
+    err = np.zeros(nc, dtype=np.int32)
+    it = np.zeros(nc, dtype=np.int32)
+    rc = L.echo_gpu_test_c2p(ctypes.byref(params), _dp(tab), n, nc, g3, gp, _dp(u), _dp(v), _ip(err), _ip(it))
+    if rc:
+        raise RuntimeError(f"test_c2p status {rc}")
+    return v, err, it

@@ -134,6 +134,13 @@ int echo_gpu_upload_device(EchoCtx* ctx, const double* d_v, const double* d_u,
                            double t);
 int echo_gpu_download_device(EchoCtx* ctx, double* d_v, double* d_u);
 
+/* Asynchronous state transfer on the context's stream that keeps the run's
+ * bookkeeping (time, dt, GLM speed, vold): what a host driver that owns the
+ * arrays between steps calls around each echo_gpu_run.  Host buffers should
+ * be page-locked for the copies to overlap nothing else on the stream. */
+int echo_gpu_put_state(EchoCtx* ctx, const double* v, const double* u);
+int echo_gpu_get_state(EchoCtx* ctx, double* v, double* u);
+
 /* tout of the driver loop (echo.f90:172,243-250); evolve_main clips dt to it */
 int echo_gpu_set_tout(EchoCtx* ctx, double tout);
 
@@ -158,6 +165,16 @@ int echo_gpu_run(EchoCtx* ctx, int nsteps);
 
 int echo_gpu_stats(EchoCtx* ctx, EchoStats* st);
 int echo_gpu_sync(EchoCtx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events against the library's launches. */
+int echo_gpu_stream(EchoCtx* ctx, void** stream);
+
+/* Runs one full step with a CUDA event after every launch group and returns
+ * the device time per kernel class (ms[7]: faces x, faces y, faces z, stage
+ * scalars, update+con2prim, repair(+smoothing), end of step) and the number
+ * of launches of each class.  The step is a real step of the run. */
+int echo_gpu_profile_step(EchoCtx* ctx, double* ms, int* launches);
 
 /* ---- pieces of the step, for parity tests against the oracle ----------- */
 

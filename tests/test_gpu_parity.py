@@ -1,0 +1,122 @@
+"""CUDA step vs the CPU oracle on the same seeded inputs.
+
+Tolerances (relative L-inf per variable, see helpers.rel_linf):
+  exact build (--fmad=false): 1e-13 -- the arithmetic is the oracle's
+      operation for operation; the only admitted differences come from
+      exp()/pow() of the CUDA math library vs libm in the last place.
+  product build (--fmad=true): 1e-12 after the stated number of steps --
+      the agreement the reference's own parity requirement states.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as O
+from echo_gpu import params as P
+from echo_gpu.lib import Evolve, unit_c2p, unit_recon
+from helpers import CASES, rel_linf, setup
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(cfg, steps, exact=True, use_run=False):
+    pc, tab, v = setup(cfg)
+    o = O.Oracle(pc, tab)
+    o.set_state(v, None, cfg.tstart)
+    v0, u0 = o.state()
+    g = Evolve(pc, tab, exact=exact)
+    g.upload(v0, u0, cfg.tstart)
+    for _ in range(steps):
+        o.step()
+    if use_run:
+        g.run(steps)
+        g.sync()
+    else:
+        for _ in range(steps):
+            g.step()
+    vo, uo = o.state()
+    vg, ug = g.download()
+    st = g.stats()
+    assert st.errcode == 0
+    assert abs(st.t - o.t) <= 1e-14 * o.t
+    return rel_linf(vg, vo, o.nv), rel_linf(ug, uo, o.nv), o, g
+
+
+@pytest.mark.parametrize("case,steps", [("hd2d", 20), ("rmhd3d", 6), ("visc2d", 8)])
+def test_step_parity_exact(case, steps):
+    ev, eu, o, g = _pair(CASES[case](), steps, exact=True)
+    assert ev <= 1e-13 and eu <= 1e-13, (ev, eu)
+
+
+@pytest.mark.parametrize("case,steps", [("hd2d", 20), ("rmhd3d", 6), ("visc2d", 8)])
+def test_step_parity_fast(case, steps):
+    ev, eu, o, g = _pair(CASES[case](), steps, exact=False)
+    assert ev <= 1e-12 and eu <= 1e-12, (ev, eu)
+
+
+@pytest.mark.parametrize("rec", list(P.REC))
+def test_reconstructions_in_step(rec):
+    cfg = CASES["hd2d"]().replace(recal=rec)
+    ev, eu, _, _ = _pair(cfg, 5, exact=True)
+    assert ev <= 1e-13 and eu <= 1e-13, (rec, ev, eu)
+
+
+@pytest.mark.parametrize("bc", [0, 1, 2, 3])
+def test_boundaries(bc):
+    cfg = CASES["hd2d"]().replace(boundary=bc, maxdt=0.02)
+    ev, eu, _, _ = _pair(cfg, 3, exact=True)
+    assert ev <= 1e-13 and eu <= 1e-13, (bc, ev, eu)
+
+
+def test_minkowski_rk3():
+    cfg = CASES["hd2d"]().replace(coordinates=P.MINKOWSKI, nrk=P.RK3)
+    ev, eu, _, _ = _pair(cfg, 5, exact=True)
+    assert ev <= 1e-13 and eu <= 1e-13
+
+
+def test_graph_run_matches_steps():
+    ev, eu, _, _ = _pair(CASES["rmhd3d"](), 4, exact=True, use_run=True)
+    assert ev <= 1e-13 and eu <= 1e-13
+
+
+@pytest.mark.parametrize("rec", list(P.REC))
+def test_recon_kernel_bitexact(rec):
+    rng = np.random.default_rng(3)
+    n = 33
+    f = rng.standard_normal((17, n + 8))
+    f[:4] = np.cumsum(f[:4], axis=1)  # smooth rows exercise the other branches
+    gl_o, gr_o = O.recon(P.REC[rec], f, n)
+    gl_g, gr_g = unit_recon(P.REC[rec], f, n, exact=True)
+    assert np.array_equal(gl_o, gl_g) and np.array_equal(gr_o, gr_g)
+
+
+@pytest.mark.parametrize("case", ["hd2d", "rmhd3d", "visc2d"])
+def test_c2p_kernel(case):
+    cfg = CASES[case]()
+    pc, tab, v = setup(cfg)
+    nv = cfg.nv
+    cells = v.reshape(nv, -1).T.copy()
+    t = 0.7
+    g3, gp = t * t, t
+    cells_p, u, bad = O.prim2cons(pc, tab, g3, gp, cells)
+    assert bad == 0
+    guess = cells_p * (1 + 1e-3)
+    vo, eo, io = O.c2p(pc, tab, g3, gp, u, guess)
+    vg, eg, ig = unit_c2p(pc, tab, g3, gp, u, guess, exact=True)
+    assert np.array_equal(eo, eg)
+    assert rel_linf(vg.T.copy(), vo.T.copy(), nv) <= 1e-14
+    # the inversion recovers the primitives it started from
+    assert rel_linf(vo.T.copy(), cells_p.T.copy(), nv) <= 1e-9
+
+
+def test_rhs_parity():
+    cfg = CASES["rmhd3d"]()
+    pc, tab, v = setup(cfg)
+    o = O.Oracle(pc, tab)
+    o.set_state(v, None, cfg.tstart)
+    v0, u0 = o.state()
+    g = Evolve(pc, tab, exact=True)
+    g.upload(v0, u0, cfg.tstart)
+    du_o, am_o = o.rhs()
+    du_g, am_g = g.rhs()
+    assert rel_linf(du_g, du_o, cfg.nv) <= 1e-13
+    assert np.allclose(am_g, am_o, rtol=0, atol=0)
