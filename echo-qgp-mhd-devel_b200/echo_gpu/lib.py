@@ -52,6 +52,7 @@ FUNCTIONS = {
     "echo_gpu_rhs": (ctypes.c_int, [P, D, D]),
     "echo_gpu_stream": (ctypes.c_int, [P, ctypes.POINTER(P)]),
     "echo_gpu_put_state": (ctypes.c_int, [P, P, P]),
+    "echo_gpu_rhs_noalloc": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double, P, P, P, I]),
     "echo_gpu_get_state": (ctypes.c_int, [P, P, P]),
     "echo_gpu_profile_step": (ctypes.c_int, [P, D, I]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),

@@ -196,6 +196,36 @@ int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, int n_eos,
                       int ncells, double g3, double gp, const double* u,
                       double* v, int* err, int* iters);
 
+/* ---- allocation-free stage right-hand side ------------------------------ */
+
+/* No counterpart in the reference.  The du of one explicit stage -- what
+ * echo_gpu_rhs returns: the three flux sweeps plus the sources, at time t,
+ * from primitives d_v -- for callers that cannot allocate device memory:
+ * a code coupled to this library inside a GPU application whose memory
+ * belongs to another allocator (a framework pool, or a solver that reserves
+ * HBM up front), or a driver that must not allocate between graph captures.
+ *
+ * The caller passes device pointers: d_v and d_du (nx*ny*nz*nv doubles,
+ * Fortran order) and, for a tabulated EoS, d_eos_cols = the four columns
+ * T, e, p, c_s^2 of the table stored one after the other (4*n_eos doubles).
+ * The function calls no cudaMalloc, cudaFree or allocating library routine:
+ * the face fluxes go to a fixed file-scope device array of
+ * ECHO_NOALLOC_SCRATCH_DOUBLES doubles (32 MiB, held by every GPU that loads
+ * the library until the process exits); a grid whose faces need more,
+ * nv * (faces in x + y + z) doubles (+8 per face for viscous runs), is
+ * rejected with ECHO_ERR_ARG and a message.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress) with the
+ * device current; make that first call before any stream capture.  All
+ * calls share the array, which keeps the last call's contents, so calls
+ * that overlap on the GPU (other streams, other host threads) race.
+ * Launches go to `stream` (a cudaStream_t, may be NULL).  If errcode is not
+ * NULL the call synchronises the stream and returns the first reference
+ * error code found (0 = none). */
+#define ECHO_NOALLOC_SCRATCH_DOUBLES (4 * 1024 * 1024)
+int echo_gpu_rhs_noalloc(const EchoParams* p, const double* d_eos_cols,
+                         int n_eos, double t, const double* d_v, double* d_du,
+                         void* stream, int* errcode);
+
 #ifdef __cplusplus
 }
 #endif
