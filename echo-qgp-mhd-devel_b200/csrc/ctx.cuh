@@ -32,6 +32,7 @@ struct EchoCtx {
   double* d_tab;
   int* d_bk;                // EoS bracket accelerators
   double* d_du;             // scratch for echo_gpu_rhs
+  double* d_dussp[4];       // IMEX-SSP stage right-hand sides du(:,:,:,:,1..4)
   unsigned char* d_fail;
   DevScalars* d_sc;
   DevScalars* h_sc;         // pinned mirror
@@ -63,9 +64,12 @@ template <int KIND>
 void launch_faces(EchoCtx* c, int dir);
 template <int KIND>
 void launch_update(EchoCtx* c, int irk, int mode, double* du_out);
+// what: 1 = repair only, 2 = smoothing only, 3 = both
 template <int KIND>
-void launch_repair_smooth(EchoCtx* c);
+void launch_repair_smooth(EchoCtx* c, int what = 3);
 template <int KIND>
 void launch_p2c(EchoCtx* c);
+template <int KIND>
+void launch_ssp_combine(EchoCtx* c, int stage);
 
 }  // namespace echo

@@ -70,7 +70,7 @@ int echo_nv_of(int kind) {
     }                                                             \
   } while (0)
 
-static void launch_scalars(EchoCtx* c, int irk) {
+static void launch_scalars(EchoCtx* c, int irk, int mode = 0) {
   ScalarArgs S;
   S.sc = c->d_sc;
   S.g = c->g;
@@ -80,11 +80,61 @@ static void launch_scalars(EchoCtx* c, int irk) {
   S.irk = irk;
   S.nrk = c->p.nrk;
   S.divclean = c->p.divclean;
+  S.mode = mode;
   stage_scalars_kernel<<<1, 1, 0, c->stream>>>(S);
+}
+
+// the three flux sweeps of a stage; the CFL maxima start from zero
+static void enqueue_sweeps(EchoCtx* c) {
+  cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream);
+  for (int d = 0; d < 3; d++) {
+    int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
+    if (n > 1) {
+      DISPATCH(c, launch_faces, c, d);
+      mark(c, PK_FACES_X + d);
+    }
+  }
+}
+
+// IMEX-SSP3(4,3,3) stage (evolve.f90:204-267), all asynchronous
+static void enqueue_stage_ssp(EchoCtx* c, int irk) {
+  if (irk == 1) {
+    launch_scalars(c, 1, 1);  // dt from the previous stage's speeds
+  } else {
+    if (irk == 2) c->ucur = 1 - c->ucur;  // U[ucur] becomes the u built from u0 = U[1-ucur]
+    cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
+    cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
+    DISPATCH(c, launch_ssp_combine, c, irk);
+    mark(c, PK_UPDATE);
+    // smoothing at the end of these stages would act only on values the next
+    // combination overwrites, so the reference's smoothing survives only
+    // after the final combination
+    DISPATCH(c, launch_repair_smooth, c, 1);
+    mark(c, PK_REPAIR);
+    c->vcur = 1 - c->vcur;
+  }
+  enqueue_sweeps(c);
+  launch_scalars(c, irk, 2);
+  mark(c, PK_SCALARS);
+  DISPATCH(c, launch_update, c, irk, MODE_RHS, c->d_dussp[irk - 1]);
+  mark(c, PK_UPDATE);
+  if (irk == 4) {
+    cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
+    DISPATCH(c, launch_ssp_combine, c, 5);
+    mark(c, PK_UPDATE);
+    DISPATCH(c, launch_repair_smooth, c, 3);
+    mark(c, PK_REPAIR);
+    c->vcur = 1 - c->vcur;
+  }
 }
 
 // one explicit RK stage, all asynchronous
 static void enqueue_stage(EchoCtx* c, int irk) {
+  if (c->p.nrk == ECHO_SSP) {
+    enqueue_stage_ssp(c, irk);
+    return;
+  }
+  cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream);
   for (int d = 0; d < 3; d++) {
     int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
     if (n > 1) {
@@ -98,7 +148,7 @@ static void enqueue_stage(EchoCtx* c, int irk) {
   mark(c, PK_SCALARS);
   DISPATCH(c, launch_update, c, irk, MODE_RK, (double*)nullptr);
   mark(c, PK_UPDATE);
-  DISPATCH(c, launch_repair_smooth, c);
+  DISPATCH(c, launch_repair_smooth, c, 3);
   mark(c, PK_REPAIR);
   if (irk == 1) c->ucur = 1 - c->ucur;
   c->vcur = 1 - c->vcur;
@@ -142,7 +192,7 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   if (!p || !out) return ECHO_ERR_ARG;
   *out = nullptr;
   if (p->mhd > 1 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
-  if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3) return ECHO_ERR_UNSUPPORTED;
+  if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3 && p->nrk != ECHO_SSP) return ECHO_ERR_UNSUPPORTED;
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return ECHO_ERR_ARG;
   if ((p->nx > 1 && p->nx < 3) || (p->ny > 1 && p->ny < 3) || (p->nz > 1 && p->nz < 3)) return ECHO_ERR_ARG;
   if (p->eqstate == ECHO_EOS_TABLE && (!eos_table || n_eos < 2)) return ECHO_ERR_ARG;
@@ -197,6 +247,10 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   for (int i = 0; i < 2; i++) {
     CK(cudaMalloc(&c->d_vh[i], sizeof(double) * 4 * c->g.ncell));
     CK(cudaMemset(c->d_vh[i], 0, sizeof(double) * 4 * c->g.ncell));
+  }
+  for (int q = 0; q < 4; q++) {
+    c->d_dussp[q] = nullptr;
+    if (p->nrk == ECHO_SSP) CK(cudaMalloc(&c->d_dussp[q], sizeof(double) * nvc));
   }
   CK(cudaMalloc(&c->d_fail, c->g.ncell));
   CK(cudaMemset(c->d_fail, 0, c->g.ncell));
@@ -272,6 +326,7 @@ int echo_gpu_free(EchoCtx* c) {
     cudaFree(c->d_F[d]);
     cudaFree(c->d_WD[d]);
   }
+  for (int q = 0; q < 4; q++) cudaFree(c->d_dussp[q]);
   cudaFree(c->d_fail);
   cudaFree(c->d_sc);
   cudaFree(c->d_tab);

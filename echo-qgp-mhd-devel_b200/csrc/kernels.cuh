@@ -318,17 +318,21 @@ struct ScalarArgs {
   Grid g;
   double cfl, maxdt, glm_alpha;
   int irk, nrk, divclean;
+  int mode;  // 0: explicit RK stage (after the sweeps); 1: IMEX-SSP dt (before the
+             // sweeps of stage 1, from the previous stage's speeds); 2: IMEX-SSP GLM
 };
 
 static __global__ void stage_scalars_kernel(ScalarArgs A) {
   DevScalars* sc = A.sc;
-  // glm_ch = glm_ch_old (start of stage); glm_ch_old = maxval(aflux) (end of sweeps)
-  sc->glm_ch = sc->glm_ch_old;
-  double m = sc->aflux[0];
-  if (sc->aflux[1] > m) m = sc->aflux[1];
-  if (sc->aflux[2] > m) m = sc->aflux[2];
-  sc->glm_ch_old = m;
-  if (A.irk == 1) {
+  if (A.mode != 1) {
+    // glm_ch = glm_ch_old (start of stage); glm_ch_old = maxval(aflux) (end of sweeps)
+    sc->glm_ch = sc->glm_ch_old;
+    double m = sc->aflux[0];
+    if (sc->aflux[1] > m) m = sc->aflux[1];
+    if (sc->aflux[2] > m) m = sc->aflux[2];
+    sc->glm_ch_old = m;
+  }
+  if (A.irk == 1 && A.mode != 2) {
     double amax;
     if (A.divclean) {
       amax = 1;
@@ -363,8 +367,7 @@ static __global__ void stage_scalars_kernel(ScalarArgs A) {
     }
     sc->dt = dtl;
   }
-  if (A.divclean) sc->expfact = exp(-sc->glm_ch * sc->glm_ch * A.glm_alpha * (sc->dt / 2.));
-  sc->amax_bits[0] = sc->amax_bits[1] = sc->amax_bits[2] = 0ull;
+  if (A.divclean && A.mode != 1) sc->expfact = exp(-sc->glm_ch * sc->glm_ch * A.glm_alpha * (sc->dt / 2.));
 }
 
 // end of step (echo.f90:211-241)
@@ -532,6 +535,77 @@ __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
     for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
     if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
   }
+}
+
+// ---------------------------------------------------------------------------
+// IMEX-SSP3(4,3,3) stage combinations (evolve.f90:235-266) + con2prim.  The
+// stiff right-hand sides du_stiff are exact zeros without resistivity; they
+// are kept as explicit 0.0 terms so the arithmetic is the reference's.
+// ---------------------------------------------------------------------------
+struct SspArgs {
+  DevPhys P;
+  Grid g;
+  const double* __restrict__ u0;
+  const double* __restrict__ du1;
+  const double* __restrict__ du2;
+  const double* __restrict__ du3;
+  const double* __restrict__ du4;
+  double* __restrict__ uout;
+  const double* __restrict__ vin;
+  double* __restrict__ vout;
+  unsigned char* fail;
+  DevScalars* sc;
+  int stage;  // 2, 3, 4: the combination that opens stage irk; 5: the final one
+  int coordinates, algo, divclean;
+  double tol;
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  const double alpha_imex = 0.24169426078821, beta_imex = 0.06042356519705, eta_imex = 0.12915286960590;
+  const double delta_imex = 0.5 - beta_imex - eta_imex - alpha_imex;
+  const Grid& g = A.g;
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_iters = 0;
+  if (c < g.ncell) {
+    const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+    const double dt = A.sc->dt, ds = 0.0;
+    double uu[NV], vv[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      size_t i = (size_t)k * g.ncell + c;
+      double u0 = A.u0[i];
+      if (A.stage == 2) {
+        uu[k] = u0 + dt * alpha_imex * ds;
+      } else if (A.stage == 3) {
+        uu[k] = u0 - dt * (A.du2[i] + (1. - alpha_imex) * ds);
+      } else if (A.stage == 4) {
+        uu[k] = u0 - dt * (A.du2[i] / 4. + A.du3[i] / 4. + beta_imex * ds + eta_imex * ds + delta_imex * ds);
+      } else {
+        uu[k] = u0 - dt * (A.du2[i] / 6. + A.du3[i] / 6. + A.du4[i] * 2. / 3. + ds / 6. + ds / 6. + ds * 2. / 3.);
+      }
+      vv[k] = A.vin[i];
+    }
+    if (T::GLM && A.stage == 5) uu[KGLM] = uu[KGLM] * A.sc->expfact;
+#pragma unroll
+    for (int k = 0; k < NV; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
+    int it = 0;
+    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+    my_iters = (unsigned long long)it;
+    if (err) {
+      A.fail[c] = 1;
+      atomicAdd(&A.sc->nfail, 1);
+    } else {
+      A.fail[c] = 0;
+#pragma unroll
+      for (int k = 0; k < NV; k++) A.vout[(size_t)k * g.ncell + c] = vv[k];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+  if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
 }
 
 // ---------------------------------------------------------------------------

@@ -53,8 +53,8 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   A.fail = c->d_fail;
   A.sc = c->d_sc;
   int nrk = c->p.nrk;
-  A.c1 = crk[nrk - 1][irk - 1][0];
-  A.c2 = crk[nrk - 1][irk - 1][1];
+  A.c1 = nrk <= 3 ? crk[nrk - 1][irk - 1][0] : 0.;
+  A.c2 = nrk <= 3 ? crk[nrk - 1][irk - 1][1] : 0.;
   A.irk = irk;
   A.nrk = nrk;
   A.divclean = c->p.divclean;
@@ -67,7 +67,7 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
 }
 
 template <int KIND>
-void launch_repair_smooth(EchoCtx* c) {
+void launch_repair_smooth(EchoCtx* c, int what) {
   RepairArgs R;
   R.P = c->P;
   R.g = c->g;
@@ -80,8 +80,8 @@ void launch_repair_smooth(EchoCtx* c) {
   R.algo = c->p.algo_solver;
   R.maxspeed = c->p.maxspeed;
   R.tol = c->p.c2p_tol;
-  repair_kernel<KIND><<<1, 256, 0, c->stream>>>(R);
-  if (KIND == KIND_VISC && c->p.enable_smooth_viscosity) {
+  if (what & 1) repair_kernel<KIND><<<1, 256, 0, c->stream>>>(R);
+  if ((what & 2) && KIND == KIND_VISC && c->p.enable_smooth_viscosity) {
     SmoothArgs S;
     S.P = c->P;
     S.g = c->g;
@@ -103,10 +103,37 @@ void launch_p2c(EchoCtx* c) {
 }
 
 
+// IMEX-SSP combination of stage `stage` (2..4) or the final one (5); the
+// caller has already made U[ucur] the u being built and U[1-ucur] = u0
+template <int KIND>
+void launch_ssp_combine(EchoCtx* c, int stage) {
+  SspArgs A;
+  A.P = c->P;
+  A.g = c->g;
+  A.u0 = c->d_u[1 - c->ucur];
+  A.du1 = c->d_dussp[0];
+  A.du2 = c->d_dussp[1];
+  A.du3 = c->d_dussp[2];
+  A.du4 = c->d_dussp[3];
+  A.uout = c->d_u[c->ucur];
+  A.vin = c->d_v[c->vcur];
+  A.vout = c->d_v[1 - c->vcur];
+  A.fail = c->d_fail;
+  A.sc = c->d_sc;
+  A.stage = stage;
+  A.coordinates = c->p.coordinates;
+  A.algo = c->p.algo_solver;
+  A.divclean = c->p.divclean;
+  A.tol = c->p.c2p_tol;
+  unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
+  ssp_combine_kernel<KIND><<<blocks, 128, 0, c->stream>>>(A);
+}
+
 }  // namespace echo
 
 #define ECHO_INSTANTIATE(K)                                                   \
   template void echo::launch_faces<K>(EchoCtx*, int);                         \
   template void echo::launch_update<K>(EchoCtx*, int, int, double*);          \
-  template void echo::launch_repair_smooth<K>(EchoCtx*);                      \
-  template void echo::launch_p2c<K>(EchoCtx*);
+  template void echo::launch_repair_smooth<K>(EchoCtx*, int);                      \
+  template void echo::launch_p2c<K>(EchoCtx*);                                \
+  template void echo::launch_ssp_combine<K>(EchoCtx*, int);

@@ -73,6 +73,17 @@ def test_minkowski_rk3():
     assert ev <= 1e-13 and eu <= 1e-13
 
 
+@pytest.mark.parametrize("case,steps", [("rmhd3d", 4), ("hd2d", 6), ("visc2d", 4)])
+def test_imex_ssp_parity(case, steps):
+    # IMEX-SSP3(4,3,3) (evolve.f90:204-267): the stiff terms are zero without
+    # resistivity; the reference also runs it for hydro (common.f90:2076-2083)
+    cfg = CASES[case]().replace(nrk=P.SSP)
+    ev, eu, _, _ = _pair(cfg, steps, exact=True)
+    assert ev <= 1e-13 and eu <= 1e-13, (ev, eu)
+    ev, eu, _, _ = _pair(cfg, steps, exact=False, use_run=True)
+    assert ev <= 1e-12 and eu <= 1e-12, (ev, eu)
+
+
 def test_graph_run_matches_steps():
     ev, eu, _, _ = _pair(CASES["rmhd3d"](), 4, exact=True, use_run=True)
     assert ev <= 1e-13 and eu <= 1e-13
