@@ -3,6 +3,7 @@
 // (system_source, system.f90:1587-1842; get_sigma, viscous.f90:283-393).
 #pragma once
 
+#include "mlp.cuh"
 #include "physics.cuh"
 
 namespace echo {
@@ -210,10 +211,14 @@ __device__ __forceinline__ int eos_energy_slope(const DevPhys& P, double rh, dou
   return 0;
 }
 
+// Newton on sist3 with the analytic Jacobian.  Converged when the relative
+// residual max(|F1|/(y+B^2)^2, |F2|/(|U|+B^2), |F3|/y) <= tol; one more
+// Newton correction is then applied (the error after it is ~ residual^2).
+// Returns the number of corrections made, or -1 (the caller falls back).
 static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, double tol, int maxit) {
   double xx = X[0], yy = X[1], pp = X[2];
-  for (int it = 1; it <= maxit; it++) {
-    if (!(xx < 1.0) || !(yy > 0.0)) return -1;
+  for (int it = 0; it <= maxit; it++) {
+    if (!(xx < 1.0) || !(xx >= 0.0) || !(yy > 0.0) || !(pp > 0.0)) return -1;
     double sq = sqrt(1. - xx);
     double rh = s.D * sq, en = 0, dedp = 0;
     if (eos_energy_slope(P, rh, pp, &en, &dedp)) return -1;
@@ -221,6 +226,7 @@ static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, doubl
     double F1 = ib * ib * xx - s.SB2 * iy2 * (2 * yy + s.B2) - s.S2;
     double F2 = yy - pp + 0.5 * (1. + xx) * s.B2 - 0.5 * s.SB2 * iy2 - s.U;
     double F3 = yy - (pp + en) * i1x;
+    double r = fmax(fabs(F1) / (ib * ib), fmax(fabs(F2) / (fabs(s.U) + s.B2), fabs(F3) / yy));
     // d(en)/dx through rh is zero: the tabulated and conformal e(p) do not depend on rh
     double J11 = ib * ib, J12 = 2 * ib * xx + 2 * s.SB2 * (2 * yy + s.B2) * iy3 - 2 * s.SB2 * iy2, J13 = 0.;
     double J21 = 0.5 * s.B2, J22 = 1. + s.SB2 * iy3, J23 = -1.;
@@ -234,21 +240,26 @@ static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, doubl
     double dx = (b1 * c11 + b2 * (J13 * J32 - J12 * J33) + b3 * (J12 * J23 - J13 * J22)) * idet;
     double dy = (b1 * c12 + b2 * (J11 * J33 - J13 * J31) + b3 * (J13 * J21 - J11 * J23)) * idet;
     double dp = (b1 * c13 + b2 * (J12 * J31 - J11 * J32) + b3 * (J11 * J22 - J12 * J21)) * idet;
+    if (r <= tol) {  // converged: polish and stop
+      xx += dx;
+      yy += dy;
+      pp += dp;
+      if (!(xx < 1.0) || !(yy > 0.0) || !(pp > 0.0)) return -1;
+      X[0] = xx;
+      X[1] = yy;
+      X[2] = pp;
+      return it + 1;
+    }
+    if (it == maxit) return -1;
     // damp steps that would leave the physical domain
     double lam = 1.0;
-    for (int k = 0; k < 30 && (xx + lam * dx >= 1.0 || yy + lam * dy <= 0.0 || pp + lam * dp <= 0.0); k++)
+    for (int k = 0; k < 30 && (xx + lam * dx >= 1.0 || xx + lam * dx < 0.0 || yy + lam * dy <= 0.0 ||
+                               pp + lam * dp <= 0.0);
+         k++)
       lam *= 0.5;
     xx += lam * dx;
     yy += lam * dy;
     pp += lam * dp;
-    double scale = fabs(yy) + fabs(s.U) + fabs(pp);
-    if (fabs(dx) <= tol * fmax(fabs(xx), 1e-300) + tol * 1e-3 && fabs(dy) <= tol * fabs(yy) &&
-        fabs(dp) <= tol * fabs(pp) && fabs(F2) <= 1e3 * tol * scale) {
-      X[0] = xx;
-      X[1] = yy;
-      X[2] = pp;
-      return it;
-    }
   }
   return -1;
 }
@@ -260,7 +271,7 @@ static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, doubl
 // ---------------------------------------------------------------------------
 template <int KIND>
 __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol, const double* u,
-                         double* v, int* iters) {
+                         double* v, int* iters, const float* seed = nullptr, int* seed_failed = nullptr) {
   typedef Traits<KIND> T;
   const double eps = 1.e-12;
   const double ntol = 1.e-12;
@@ -401,17 +412,41 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     X[2] = pr;
     Sist3 s = {B2, SB2, SS2, UU, DD};
     int nfev = 0;
-    if (algo == ECHO_C2P_NEWTON) {
-      double Xn[3] = {X[0], X[1], X[2]};
-      int it = newton3(P, s, Xn, tol, 30);
+    if (algo == ECHO_C2P_NEWTON || algo == ECHO_C2P_MLP) {
+      int it = -1, used = 0;
+      if (algo == ECHO_C2P_MLP && seed) {
+        // learned seed: x = v^2 and p = q U, y from sist3's third equation
+        double xs0 = (double)seed[0], ps0 = (double)seed[1] * UU;
+        xs0 = xs0 < 0. ? 0. : (xs0 > 0.99 ? 0.99 : xs0);
+        double Xs[3] = {xs0, 0., ps0};
+        double es = 0;
+        if (ps0 > 0. && !eos_energy(P, DD * sqrt(1 - xs0), &es, ps0)) {
+          Xs[1] = (ps0 + es) / (1 - xs0);
+          it = newton3(P, s, Xs, tol, 3);
+          used = it > 0 ? it : 3;
+          if (it > 0) {
+            X[0] = Xs[0];
+            X[1] = Xs[1];
+            X[2] = Xs[2];
+          }
+        }
+        if (it <= 0 && seed_failed) *seed_failed = 1;
+      }
+      if (it <= 0) {  // plain path: Newton from the previous primitives
+        double Xn[3] = {X[0], X[1], X[2]};
+        it = newton3(P, s, Xn, tol, 30);
+        if (it > 0) {
+          X[0] = Xn[0];
+          X[1] = Xn[1];
+          X[2] = Xn[2];
+          it += used;
+        }
+      }
       if (it > 0) {
-        X[0] = Xn[0];
-        X[1] = Xn[1];
-        X[2] = Xn[2];
         nfev = it;
       } else {
         (void)brentm3(P, s, X, 1.e-14, 1.e-14, 300, 3, &nfev);
-        nfev += 1000;  // marks a fallback in the iteration statistics
+        nfev += 1000;  // marks a bracketed fallback in the iteration statistics
       }
     } else {
       (void)brentm3(P, s, X, 1.e-14, 1.e-14, 300, 3, &nfev);

@@ -33,6 +33,8 @@ struct EchoCtx {
   int* d_bk;                // EoS bracket accelerators
   double* d_du;             // scratch for echo_gpu_rhs
   double* d_dussp[4];       // IMEX-SSP stage right-hand sides du(:,:,:,:,1..4)
+  unsigned* d_mlp_frag;     // learned con2prim seed: BF16 weight fragments
+  float* d_mlp_par;         //   biases and normalisation
   unsigned char* d_fail;
   DevScalars* d_sc;
   DevScalars* h_sc;         // pinned mirror

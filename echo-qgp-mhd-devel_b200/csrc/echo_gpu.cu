@@ -308,6 +308,8 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   }
   c->d_du = nullptr;
   c->marks = nullptr;
+  c->d_mlp_frag = nullptr;
+  c->d_mlp_par = nullptr;
   *out = c;
   return ECHO_OK;
 }
@@ -332,6 +334,8 @@ int echo_gpu_free(EchoCtx* c) {
   cudaFree(c->d_tab);
   cudaFree(c->d_bk);
   cudaFree(c->d_du);
+  cudaFree(c->d_mlp_frag);
+  cudaFree(c->d_mlp_par);
   cudaFreeHost(c->h_sc);
   cudaStreamDestroy(c->stream);
   free(c);
@@ -439,6 +443,7 @@ static int errcode_of(const DevScalars* s, int* cell) {
 }
 
 int echo_gpu_evolve_main(EchoCtx* c, int irk, double* dt, int* errcode) {
+  if (c && c->p.algo_solver == ECHO_C2P_MLP && !c->d_mlp_frag) return ECHO_ERR_ARG;  // no network loaded
   (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
   if (!c || irk < 1 || irk > c->p.nrk) return ECHO_ERR_ARG;
   if (irk == 1) snapshot_vnewstep(c);
@@ -459,6 +464,7 @@ int echo_gpu_end_step(EchoCtx* c) {
 }
 
 int echo_gpu_step(EchoCtx* c, double* dt, int* errcode) {
+  if (c && c->p.algo_solver == ECHO_C2P_MLP && !c->d_mlp_frag) return ECHO_ERR_ARG;  // no network loaded
   (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
   if (!c) return ECHO_ERR_ARG;
   enqueue_step(c);
@@ -471,6 +477,7 @@ int echo_gpu_step(EchoCtx* c, double* dt, int* errcode) {
 }
 
 int echo_gpu_run(EchoCtx* c, int nsteps) {
+  if (c && c->p.algo_solver == ECHO_C2P_MLP && !c->d_mlp_frag) return ECHO_ERR_ARG;  // no network loaded
   (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
   if (!c || nsteps < 0) return ECHO_ERR_ARG;
   for (int s = 0; s < nsteps; s++) {

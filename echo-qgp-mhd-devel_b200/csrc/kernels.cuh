@@ -411,28 +411,50 @@ struct UpdateArgs {
   double c1, c2;
   int irk, nrk, divclean, coordinates, algo, mode;
   double tol;
+  MlpDev mlp;  // learned seed (algo == ECHO_C2P_MLP)
 };
 
+// Learned con2prim seed of the calling lane's cell from its conserved
+// variables uu (times sqrt(-g)).  Called by all lanes of the warp together;
+// lanes without a cell pass active = false.
 template <int KIND>
+__device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, bool active, const double* uu,
+                                         float seed[2]) {
+  float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  if (active) {
+    double gm = M.gm, g3 = M.g3;
+    double D = gm * uu[KRH], sx = gm * uu[KVX], sy = gm * uu[KVY], sz = gm * uu[KVZ], U = gm * uu[KPR];
+    double bx = gm * uu[KBX], by = gm * uu[KBY], bz = gm * uu[KBZ];
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = sx * bx + sy * by + sz * bz;
+    double SS2 = sx * sx + sy * sy + sz * sz / g3;
+    if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, f);
+  }
+  mlp_warp(net, f, seed);
+}
+
+template <int KIND, bool SEED>
 __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const Grid& g = A.g;
   size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long my_iters = 0;
-  if (c < g.ncell) {
+  unsigned long long my_iters = 0, my_fallbacks = 0;
+  const bool active = c < g.ncell;
+  const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  double vv[NV], uu[NV];
+  if (active) {
     int ix = (int)(c % g.nx);
     size_t r = c / g.nx;
     int iy = (int)(r % g.ny);
     int iz = (int)(r / g.ny);
-    const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
     const size_t nfx = (size_t)(g.nx + 1) * g.ny * g.nz;
     const size_t nfy = (size_t)g.nx * (g.ny + 1) * g.nz;
     const size_t nfz = (size_t)g.nx * g.ny * (g.nz + 1);
     const size_t fx = ((size_t)iz * g.ny + iy) * (g.nx + 1) + ix;       // face ix-1/2 -> index ix
     const size_t fy = ((size_t)iz * (g.ny + 1) + iy) * g.nx + ix;
     const size_t fz = ((size_t)iz * g.ny + iy) * g.nx + ix;
-    double vv[NV], src[NV], du[NV];
+    double src[NV], du[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) vv[k] = A.vin[(size_t)k * g.ncell + c];
     // flux divergence in the reference's order: du = 0; += x; += y; += z
@@ -501,7 +523,6 @@ __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
     } else {
       // RK combination (evolve.f90:196-201)
       const double dt = A.sc->dt;
-      double uu[NV];
 #pragma unroll
       for (int k = 0; k < NV; k++) {
         double ui = A.uin[(size_t)k * g.ncell + c];
@@ -515,10 +536,22 @@ __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
       if (T::GLM && A.irk == A.nrk) uu[KGLM] = uu[KGLM] * A.sc->expfact;
 #pragma unroll
       for (int k = 0; k < NV; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
+    }
+  }
+  if (A.mode == MODE_RK) {
+    // learned seed, one warp at a time on the tensor cores
+    float seed[2] = {0.f, 0.f};
+    const float* sp = nullptr;
+    if (SEED) {
+      mlp_seed<KIND>(A.mlp, M, active, uu, seed);
+      sp = seed;
+    }
+    if (active) {
       // con2prim (evolve_u2v, evolve.f90:789-866)
-      int it = 0;
-      int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+      int it = 0, sfail = 0;
+      int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail);
       my_iters = (unsigned long long)it;
+      my_fallbacks = (unsigned long long)sfail;
       if (err) {
         A.fail[c] = 1;
         atomicAdd(&A.sc->nfail, 1);
@@ -528,12 +561,14 @@ __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
         for (int k = 0; k < NV; k++) A.vout[(size_t)k * g.ncell + c] = vv[k];
       }
     }
-  }
-  if (A.mode == MODE_RK) {
-    // per-block sum of iteration counts
+    // per-warp sums of iteration counts and seed fallbacks
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+    for (int o = 16; o > 0; o >>= 1) {
+      my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+      my_fallbacks += __shfl_xor_sync(0xffffffffu, my_fallbacks, o);
+    }
     if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
+    if ((threadIdx.x & 31) == 0 && my_fallbacks) atomicAdd(&A.sc->fallbacks, my_fallbacks);
   }
 }
 
@@ -558,9 +593,10 @@ struct SspArgs {
   int stage;  // 2, 3, 4: the combination that opens stage irk; 5: the final one
   int coordinates, algo, divclean;
   double tol;
+  MlpDev mlp;
 };
 
-template <int KIND>
+template <int KIND, bool SEED>
 __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
@@ -569,10 +605,11 @@ __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
   const Grid& g = A.g;
   size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long my_iters = 0;
-  if (c < g.ncell) {
-    const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  const bool active = c < g.ncell;
+  const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  double uu[NV], vv[NV];
+  if (active) {
     const double dt = A.sc->dt, ds = 0.0;
-    double uu[NV], vv[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) {
       size_t i = (size_t)k * g.ncell + c;
@@ -591,8 +628,16 @@ __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
     if (T::GLM && A.stage == 5) uu[KGLM] = uu[KGLM] * A.sc->expfact;
 #pragma unroll
     for (int k = 0; k < NV; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
+  }
+  float seed[2] = {0.f, 0.f};
+  const float* sp = nullptr;
+  if (SEED) {
+    mlp_seed<KIND>(A.mlp, M, active, uu, seed);
+    sp = seed;
+  }
+  if (active) {
     int it = 0;
-    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp);
     my_iters = (unsigned long long)it;
     if (err) {
       A.fail[c] = 1;

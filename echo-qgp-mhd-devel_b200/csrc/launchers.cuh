@@ -62,8 +62,14 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   A.algo = c->p.algo_solver;
   A.mode = mode;
   A.tol = c->p.c2p_tol;
+  A.mlp.frag = c->d_mlp_frag;
+  A.mlp.par = c->d_mlp_par;
+  if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;  // no network loaded
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  update_kernel<KIND><<<blocks, 128, 0, c->stream>>>(A);
+  if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP && mode == MODE_RK)
+    update_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
+  else
+    update_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
 }
 
 template <int KIND>
@@ -125,8 +131,14 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
   A.algo = c->p.algo_solver;
   A.divclean = c->p.divclean;
   A.tol = c->p.c2p_tol;
+  A.mlp.frag = c->d_mlp_frag;
+  A.mlp.par = c->d_mlp_par;
+  if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  ssp_combine_kernel<KIND><<<blocks, 128, 0, c->stream>>>(A);
+  if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP)
+    ssp_combine_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
+  else
+    ssp_combine_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
 }
 
 }  // namespace echo

@@ -1,0 +1,188 @@
+// mlp.cuh -- the learned con2prim seed for ideal RMHD.
+//
+// A 4x64 tanh MLP maps five normalised invariants of the conserved state
+//   f0 = log U, f1 = D/U, f2 = S^2/U^2, f3 = B^2/U, f4 = (S.B)^2/U^3
+// (U = energy, D = density, S = momentum, B = field, all already divided by
+// sqrt(-g); the same quantities BRENTM's system sist3 is written in) to the
+// two unknowns x = v^2 and q = p/U.  The third unknown y = (e+p)gamma^2
+// follows from the EoS (sist3's third equation).  The seed is finished by
+// the FP64 Newton solve on sist3; it is never used on its own.
+//
+// Inference runs per warp (32 cells) on the tensor cores: BF16 operands,
+// FP32 accumulation, mma.sync.m16n8k16.  The accumulator fragment of an
+// m16n8 tile holds, per thread, rows (g, g+8) and columns (2t, 2t+1) -- the
+// same elements the A fragment of an m16n8k16 operand holds for the k-tile
+// that covers those columns -- so one layer's output becomes the next
+// layer's input in registers, with no shuffles or shared memory.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "physics.cuh"
+
+namespace echo {
+
+enum { MLP_NIN = 5, MLP_H = 64, MLP_NOUT = 2, MLP_NHID = 4 };
+
+// Weight fragments (u32 = two bf16) in the order the mma B operand needs:
+// layer 0: [k-tile 0][n-tile 0..7][lane][2]; layers 1..3: [kt 0..3][nt 0..7]
+// [lane][2]; layer 4: [kt 0..3][nt 0][lane][2].
+enum {
+  MLP_FRAG_L0 = 0,
+  MLP_FRAG_L1 = MLP_FRAG_L0 + 1 * 8 * 64,
+  MLP_FRAG_L2 = MLP_FRAG_L1 + 4 * 8 * 64,
+  MLP_FRAG_L3 = MLP_FRAG_L2 + 4 * 8 * 64,
+  MLP_FRAG_L4 = MLP_FRAG_L3 + 4 * 8 * 64,
+  MLP_FRAG_N = MLP_FRAG_L4 + 4 * 1 * 64
+};
+// biases and normalisation, FP32: b0..b3 (64 each), b4 (8, two used),
+// feature mean/std (5+5), target mean/std (2+2)
+enum {
+  MLP_B0 = 0,
+  MLP_B4 = 4 * 64,
+  MLP_FMEAN = MLP_B4 + 8,
+  MLP_FSTD = MLP_FMEAN + 5,
+  MLP_TMEAN = MLP_FSTD + 5,
+  MLP_TSTD = MLP_TMEAN + 2,
+  MLP_PARAMS_N = MLP_TSTD + 2
+};
+
+struct MlpDev {
+  const unsigned* __restrict__ frag;  // MLP_FRAG_N u32
+  const float* __restrict__ par;      // MLP_PARAMS_N floats
+};
+
+// raw invariants of the cell (before standardisation)
+__device__ __forceinline__ void mlp_invariants(double D, double SS2, double U, double B2, double SB2, float f[5]) {
+  double iu = 1.0 / U;
+  f[0] = (float)log(U);
+  f[1] = (float)(D * iu);
+  f[2] = (float)(SS2 * iu * iu);
+  f[3] = (float)(B2 * iu);
+  f[4] = (float)(SB2 * iu * iu * iu);
+}
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<unsigned*>(&h);
+}
+
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Seed for the calling lane's cell.  Must be called by all 32 lanes of the
+// warp together (inactive lanes pass any finite features).  f: raw
+// invariants; out: (x, q) de-standardised.
+__device__ __forceinline__ void mlp_warp(const MlpDev& M, const float f[5], float out[2]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float fs[5];
+#pragma unroll
+  for (int j = 0; j < 5; j++) fs[j] = (f[j] - __ldg(M.par + MLP_FMEAN + j)) / __ldg(M.par + MLP_FSTD + j);
+  // layer-0 A fragments (16 input columns, 5 used) for both m-tiles
+  unsigned A[2][4][4];  // [m-tile][k-tile][reg]
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++) {
+    float lo[5], hi[5];
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      lo[j] = __shfl_sync(full, fs[j], mt * 16 + g);
+      hi[j] = __shfl_sync(full, fs[j], mt * 16 + g + 8);
+    }
+    // columns 2t and 2t+1
+    float l0 = t == 0 ? lo[0] : t == 1 ? lo[2] : t == 2 ? lo[4] : 0.f;
+    float l1 = t == 0 ? lo[1] : t == 1 ? lo[3] : 0.f;
+    float h0 = t == 0 ? hi[0] : t == 1 ? hi[2] : t == 2 ? hi[4] : 0.f;
+    float h1 = t == 0 ? hi[1] : t == 1 ? hi[3] : 0.f;
+    A[mt][0][0] = pack_bf16(l0, l1);
+    A[mt][0][1] = pack_bf16(h0, h1);
+    A[mt][0][2] = 0u;
+    A[mt][0][3] = 0u;
+  }
+  float C[2][8][4];
+  // hidden layers 0..3
+#pragma unroll
+  for (int layer = 0; layer < 4; layer++) {
+    const int nk = layer == 0 ? 1 : 4;
+    const unsigned* W = M.frag + (layer == 0 ? MLP_FRAG_L0 : MLP_FRAG_L1 + (layer - 1) * (4 * 8 * 64));
+    const float* b = M.par + MLP_B0 + layer * 64;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      float b0 = __ldg(b + nt * 8 + 2 * t), b1 = __ldg(b + nt * 8 + 2 * t + 1);
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++) {
+        C[mt][nt][0] = b0;
+        C[mt][nt][1] = b1;
+        C[mt][nt][2] = b0;
+        C[mt][nt][3] = b1;
+      }
+    }
+#pragma unroll
+    for (int kt = 0; kt < 4; kt++) {
+      if (kt >= nk) break;
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        const uint2 w = __ldg(reinterpret_cast<const uint2*>(W) + (kt * 8 + nt) * 32 + lane);
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) mma_bf16(C[mt][nt], A[mt][kt], w.x, w.y);
+      }
+    }
+    // tanh, then the accumulators become the next layer's A fragments
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        const float* c0 = C[mt][2 * kt];
+        const float* c1 = C[mt][2 * kt + 1];
+        A[mt][kt][0] = pack_bf16(tanh_fast(c0[0]), tanh_fast(c0[1]));
+        A[mt][kt][1] = pack_bf16(tanh_fast(c0[2]), tanh_fast(c0[3]));
+        A[mt][kt][2] = pack_bf16(tanh_fast(c1[0]), tanh_fast(c1[1]));
+        A[mt][kt][3] = pack_bf16(tanh_fast(c1[2]), tanh_fast(c1[3]));
+      }
+  }
+  // output layer: 64 -> 8 (two used), linear
+  float O[2][4];
+  {
+    float b0 = __ldg(M.par + MLP_B4 + 2 * t), b1 = __ldg(M.par + MLP_B4 + 2 * t + 1);
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+      O[mt][0] = b0;
+      O[mt][1] = b1;
+      O[mt][2] = b0;
+      O[mt][3] = b1;
+    }
+#pragma unroll
+    for (int kt = 0; kt < 4; kt++) {
+      const uint2 w = __ldg(reinterpret_cast<const uint2*>(M.frag + MLP_FRAG_L4) + kt * 32 + lane);
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++) mma_bf16(O[mt], A[mt][kt], w.x, w.y);
+    }
+  }
+  // row r = mt*16 + h*8 + g' of the output sits in lane g'*4 (t = 0), element 2h / 2h+1
+  const int mt_me = lane >> 4, h_me = (lane >> 3) & 1, src = (lane & 7) * 4;
+  float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++) {
+    float a0 = __shfl_sync(full, O[mt][0], src), a1 = __shfl_sync(full, O[mt][1], src);
+    float a2 = __shfl_sync(full, O[mt][2], src), a3 = __shfl_sync(full, O[mt][3], src);
+    if (mt == mt_me) {
+      y0 = h_me ? a2 : a0;
+      y1 = h_me ? a3 : a1;
+    }
+  }
+  out[0] = y0 * __ldg(M.par + MLP_TSTD + 0) + __ldg(M.par + MLP_TMEAN + 0);
+  out[1] = y1 * __ldg(M.par + MLP_TSTD + 1) + __ldg(M.par + MLP_TMEAN + 1);
+}
+
+}  // namespace echo

@@ -165,3 +165,126 @@ extern "C" int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, i
   cudaFree(dbk);
   return ECHO_OK;
 }
+
+// ---------------------------------------------------------------------------
+// con2prim of independent ideal-RMHD cells with the learned seed (weights !=
+// NULL) or with Newton from the guess in v (weights == NULL): the seed's
+// gain, cell by cell, at the same residual.
+// ---------------------------------------------------------------------------
+namespace echo {
+template <int KIND>
+__global__ void c2p_seed_kernel(DevPhys P, Metric M, MlpDev net, int use_seed, double tol, int ncells,
+                                const double* u, double* v, int* err, int* iters, int* seed_failed) {
+  typedef Traits<KIND> T;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = c < ncells;
+  double uu[T::NV], vv[T::NV];
+  for (int k = 0; k < T::NV; k++) {
+    uu[k] = active ? u[(size_t)c * T::NV + k] : 1.0;
+    vv[k] = active ? v[(size_t)c * T::NV + k] : 0.0;
+  }
+  float seed[2] = {0.f, 0.f};
+  if (use_seed) {
+    float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    if (active) {
+      double gm = M.gm, g3 = M.g3;
+      double D = gm * uu[KRH], sx = gm * uu[KVX], sy = gm * uu[KVY], sz = gm * uu[KVZ], U = gm * uu[KPR];
+      double bx = gm * uu[KBX], by = gm * uu[KBY], bz = gm * uu[KBZ];
+      double B2 = bx * bx + by * by + bz * bz * g3;
+      double SB = sx * bx + sy * by + sz * bz;
+      double SS2 = sx * sx + sy * sy + sz * sz / g3;
+      if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, f);
+    }
+    mlp_warp(net, f, seed);
+  }
+  if (!active) return;
+  int it = 0, sf = 0;
+  int e = cons2prim<KIND>(P, M, use_seed ? ECHO_C2P_MLP : ECHO_C2P_NEWTON, tol, uu, vv, &it,
+                          use_seed ? seed : nullptr, &sf);
+  for (int k = 0; k < T::NV; k++) v[(size_t)c * T::NV + k] = vv[k];
+  err[c] = e;
+  iters[c] = it;
+  seed_failed[c] = sf;
+}
+}  // namespace echo
+
+bool echo_mlp_pack(const float* W, const float* norm, std::vector<unsigned>& frag, std::vector<float>& par);
+
+extern "C" int echo_gpu_test_c2p_seeded(const EchoParams* p, const double* eos_table, int n_eos, int ncells,
+                                        double g3, double gp, const float* weights, const float* norm,
+                                        const double* u, double* v, int* err, int* iters, int* seed_failed) {
+  if (!p || !p->mhd || p->viscosity || ncells <= 0 || !u || !v || !err || !iters || !seed_failed)
+    return ECHO_ERR_ARG;
+  (void)cudaGetLastError();
+  int kind = echo_kind_of(p), nv = echo_nv_of(kind);
+  size_t nb = (size_t)ncells * nv * sizeof(double);
+  double *du, *dv, *dtab = nullptr;
+  int *derr, *dit, *dsf;
+  unsigned* dfrag = nullptr;
+  float* dpar = nullptr;
+  CK(cudaMalloc(&du, nb));
+  CK(cudaMalloc(&dv, nb));
+  CK(cudaMalloc(&derr, ncells * sizeof(int)));
+  CK(cudaMalloc(&dit, ncells * sizeof(int)));
+  CK(cudaMalloc(&dsf, ncells * sizeof(int)));
+  CK(cudaMemcpy(du, u, nb, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dv, v, nb, cudaMemcpyHostToDevice));
+  DevPhys P;
+  memset(&P, 0, sizeof(P));
+  std::vector<double> cols((size_t)4 * n_eos);
+  for (int i = 0; i < n_eos; i++)
+    for (int q = 0; q < 4; q++) cols[(size_t)q * n_eos + i] = eos_table[4 * i + q];
+  CK(cudaMalloc(&dtab, sizeof(double) * 4 * n_eos));
+  CK(cudaMemcpy(dtab, cols.data(), sizeof(double) * 4 * n_eos, cudaMemcpyHostToDevice));
+  P.nt = n_eos;
+  P.tT = dtab;
+  P.te = dtab + n_eos;
+  P.tp = dtab + 2 * n_eos;
+  P.tc = dtab + 3 * n_eos;
+  P.eqstate = p->eqstate;
+  P.coordinates = p->coordinates;
+  P.enezero = p->enezero;
+  P.przero = p->przero;
+  MlpDev net{nullptr, nullptr};
+  if (weights) {
+    std::vector<unsigned> frag;
+    std::vector<float> par;
+    echo_mlp_pack(weights, norm, frag, par);
+    CK(cudaMalloc(&dfrag, sizeof(unsigned) * frag.size()));
+    CK(cudaMalloc(&dpar, sizeof(float) * par.size()));
+    CK(cudaMemcpy(dfrag, frag.data(), sizeof(unsigned) * frag.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dpar, par.data(), sizeof(float) * par.size(), cudaMemcpyHostToDevice));
+    net.frag = dfrag;
+    net.par = dpar;
+  }
+  Metric M;
+  M.g0 = -1.;
+  M.g1 = 1.;
+  M.g2 = 1.;
+  M.g3 = g3;
+  M.gp = gp;
+  M.gm = 1. / gp;
+  M.t = gp;
+  M.t3 = pow(gp, 3.);
+  unsigned blocks = (unsigned)((ncells + 127) / 128);
+  if (kind == KIND_MHDGLM)
+    c2p_seed_kernel<KIND_MHDGLM><<<blocks, 128>>>(P, M, net, weights != nullptr, p->c2p_tol, ncells, du, dv, derr,
+                                                  dit, dsf);
+  else
+    c2p_seed_kernel<KIND_MHD><<<blocks, 128>>>(P, M, net, weights != nullptr, p->c2p_tol, ncells, du, dv, derr, dit,
+                                               dsf);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(v, dv, nb, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(err, derr, ncells * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(iters, dit, ncells * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(seed_failed, dsf, ncells * sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(du);
+  cudaFree(dv);
+  cudaFree(derr);
+  cudaFree(dit);
+  cudaFree(dsf);
+  cudaFree(dtab);
+  cudaFree(dfrag);
+  cudaFree(dpar);
+  return ECHO_OK;
+}

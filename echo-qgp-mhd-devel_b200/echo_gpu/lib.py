@@ -22,6 +22,7 @@ _libs: dict[str, ctypes.CDLL] = {}
 
 D = ctypes.POINTER(ctypes.c_double)
 I = ctypes.POINTER(ctypes.c_int)
+F = ctypes.POINTER(ctypes.c_float)
 P = ctypes.c_void_p
 
 
@@ -53,6 +54,13 @@ FUNCTIONS = {
     "echo_gpu_stream": (ctypes.c_int, [P, ctypes.POINTER(P)]),
     "echo_gpu_put_state": (ctypes.c_int, [P, P, P]),
     "echo_gpu_rhs_noalloc": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double, P, P, P, I]),
+    "echo_gpu_mlp_train": (ctypes.c_int, [F, F, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                          ctypes.c_uint, F, F, F, ctypes.c_int]),
+    "echo_gpu_mlp_grad": (ctypes.c_int, [F, F, F, ctypes.c_int, F, F]),
+    "echo_gpu_mlp_set": (ctypes.c_int, [P, F, F]),
+    "echo_gpu_mlp_infer": (ctypes.c_int, [F, F, F, ctypes.c_int, F]),
+    "echo_gpu_test_c2p_seeded": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                                F, F, D, D, I, I, I]),
     "echo_gpu_get_state": (ctypes.c_int, [P, P, P]),
     "echo_gpu_profile_step": (ctypes.c_int, [P, D, I]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
@@ -183,6 +191,11 @@ class Evolve:
         self._check(self.lib.echo_gpu_stats(self.h, ctypes.byref(st)), "stats")
         return st
 
+    def set_seed_network(self, weights, norm):
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        n = np.ascontiguousarray(norm, dtype=np.float32)
+        self._check(self.lib.echo_gpu_mlp_set(self.h, w.ctypes.data_as(F), n.ctypes.data_as(F)), "mlp_set")
+
     def stream_handle(self) -> int:
         s = P()
         self._check(self.lib.echo_gpu_stream(self.h, ctypes.byref(s)), "stream")
@@ -230,3 +243,25 @@ def unit_c2p(params, eos_table, g3, gp, u, vguess, exact: bool = True):
     if rc:
         raise RuntimeError(f"test_c2p status {rc}")
     return v, err, it
+
+
+def unit_c2p_seeded(params, eos_table, g3, gp, u, vguess, weights=None, norm=None):
+    """con2prim of independent RMHD cells from the learned seed (weights
+    given) or by Newton from vguess; returns v, err, iters, seed_failed."""
+    L = load(False)
+    tab = np.ascontiguousarray(eos_table, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    v = np.ascontiguousarray(vguess, dtype=np.float64).copy()
+    nc = u.shape[0]
+    err = np.zeros(nc, dtype=np.int32)
+    it = np.zeros(nc, dtype=np.int32)
+    sf = np.zeros(nc, dtype=np.int32)
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+    nm = None if norm is None else np.ascontiguousarray(norm, dtype=np.float32)
+    rc = L.echo_gpu_test_c2p_seeded(ctypes.byref(params), _dp(tab), len(tab), nc, g3, gp,
+                                    None if w is None else w.ctypes.data_as(F),
+                                    None if nm is None else nm.ctypes.data_as(F),
+                                    _dp(u), _dp(v), _ip(err), _ip(it), _ip(sf))
+    if rc:
+        raise RuntimeError(f"test_c2p_seeded status {rc}")
+    return v, err, it, sf

@@ -15,7 +15,7 @@ REC = {"TVD2": 0, "CENO3": 1, "WENO3": 2, "WENO5": 3, "PPM4": 4, "MPE3": 5, "MPE
 RK2, RK3, SSP = 2, 3, 4
 MINKOWSKI, BJORKEN = 1, 2
 EOS_CONFORMAL, EOS_IDEALGAS, EOS_TABLE = 1, 2, 3
-C2P_BRENT, C2P_NEWTON = 1, 100
+C2P_BRENT, C2P_NEWTON, C2P_MLP = 1, 100, 101
 
 
 class EchoParams(ctypes.Structure):

@@ -1,0 +1,138 @@
+"""The learned con2prim seed: training pairs from the solver, GPU training,
+loading into a run.
+
+Pairs are (conserved, primitive) states the GPU solver itself produces:
+ideal-RMHD runs of the 3+1D Milne workload at several energy scales and
+magnetisations, sampled every few steps.  The invariants and targets are
+computed here from u and v exactly as the device computes the invariants
+(csrc/kernels.cuh mlp_seed, csrc/mlp.cuh mlp_invariants):
+  U = u_E/tau, D = u_rho/tau, S_i = u_i/tau, B^i = u_B/tau (1/sqrt(-g) = 1/tau)
+  f = (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3), target = (v^2, p/U).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import initial as I
+from . import params as P
+from .lib import F, Evolve, load
+
+NW = 12994
+
+
+def invariants_targets(u: np.ndarray, v: np.ndarray, t: float, nv: int):
+    """Invariants X (n x 5) and targets T (n x 2) of every cell of a state."""
+    uu = u.reshape(nv, -1) / t
+    vv = v.reshape(nv, -1)
+    g3 = t * t
+    D, sx, sy, sz, E = uu[0], uu[1], uu[2], uu[3], uu[4]
+    bx, by, bz = uu[5], uu[6], uu[7]
+    B2 = bx * bx + by * by + bz * bz * g3
+    SB = sx * bx + sy * by + sz * bz
+    SS2 = sx * sx + sy * sy + sz * sz / g3
+    X = np.stack([np.log(E), D / E, SS2 / E**2, B2 / E, SB * SB / E**3], 1)
+    x2 = vv[1] ** 2 + vv[2] ** 2 + g3 * vv[3] ** 2
+    T = np.stack([x2, vv[4] / E], 1)
+    return X.astype(np.float32), T.astype(np.float32)
+
+
+def _magnetised(cfg, tab, peak_scale: float, mag: float, seed: int):
+    """Primitives of the workload with the energy density scaled and the
+    field set to magnetisation B^2/(2e) = mag at the centre."""
+    v = I.primitives(cfg, tab, seed=seed).reshape(cfg.nv, -1).copy()
+    e_floor = cfg.enezero
+    p = v[4]
+    # rescale pressure through e: e -> e_floor + s (e - e_floor)
+    e = np.interp(p, tab[:, 2], tab[:, 1])
+    e2 = e_floor + peak_scale * (e - e_floor)
+    v[4] = I.table_pressure(tab, e2)
+    v[5:8] *= math.sqrt(mag / 0.1 * peak_scale)
+    return v.reshape(-1)
+
+
+def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: int = 12, every: int = 3,
+                   rng_seed: int = 5, exact: bool = False):
+    """Run the GPU solver on the RMHD workload (the full 97x97x81 grid, or a
+    grid^3-sized version with the same spacing, EoS and scheme) at several
+    energy scales and magnetisations and collect (invariants, targets)
+    pairs.  The full grid covers the outer, dilute and strongly magnetised
+    region a central sub-grid never reaches."""
+    rng = np.random.default_rng(rng_seed)
+    tab = I.eos_table_loaded()
+    base = P.config1() if grid is None else P.small(P.config1(), grid, nz=max(8, int(grid * 0.84)))
+    base = base.replace(algo_solver=P.C2P_NEWTON)
+    przero = float(I.table_pressure(tab, np.array([base.enezero]))[0])
+    Xs, Ts = [], []
+    variants = [(s, m) for s in (0.3, 1.0, 3.0) for m in (0.03, 0.1, 0.3)]
+    per = max(1, n_target // (len(variants) * (steps // every)))
+    for k, (scale, mag) in enumerate(variants):
+        ev = Evolve(base.to_c(przero=przero), tab, exact=exact)
+        ev.upload(_magnetised(base, tab, scale, mag, seed=k), None, base.tstart)
+        for s in range(1, steps + 1):
+            ev.run(1)
+            if s % every == 0:
+                ev.sync()
+                st = ev.stats()
+                if st.errcode:
+                    break
+                v, u = ev.download()
+                # the step's last inversion used the metric of the step's start
+                X, T = invariants_targets(u, v, st.t - st.dt, base.nv)
+                ok = np.isfinite(X).all(1) & np.isfinite(T).all(1)
+                idx = np.nonzero(ok)[0]
+                take = rng.choice(idx, size=min(per, len(idx)), replace=False)
+                Xs.append(X[take])
+                Ts.append(T[take])
+        ev.close()
+    X = np.concatenate(Xs)
+    T = np.concatenate(Ts)
+    return X, T
+
+
+def train(X: np.ndarray, T: np.ndarray, steps: int = 3000, batch: int = 4096, lr: float = 3e-3,
+          seed: int = 1, report_every: int = 100):
+    """Train the seed network on the GPU; returns (weights, norm, losses)."""
+    L = load(False)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    w = np.zeros(NW, dtype=np.float32)
+    norm = np.zeros(14, dtype=np.float32)
+    losses = np.zeros(max(1, steps // report_every), dtype=np.float32)
+    rc = L.echo_gpu_mlp_train(X.ctypes.data_as(F), T.ctypes.data_as(F), len(X), steps, batch, lr, seed,
+                              w.ctypes.data_as(F), norm.ctypes.data_as(F), losses.ctypes.data_as(F),
+                              report_every)
+    if rc:
+        raise RuntimeError(f"echo_gpu_mlp_train status {rc}")
+    return w, norm, losses
+
+
+def infer(weights, norm, X):
+    """Tensor-core inference of the seed (BF16 operands, FP32 accumulation)."""
+    L = load(False)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    out = np.zeros((len(X), 2), dtype=np.float32)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    nm = np.ascontiguousarray(norm, dtype=np.float32)
+    rc = L.echo_gpu_mlp_infer(w.ctypes.data_as(F), nm.ctypes.data_as(F), X.ctypes.data_as(F), len(X),
+                              out.ctypes.data_as(F))
+    if rc:
+        raise RuntimeError(f"echo_gpu_mlp_infer status {rc}")
+    return out
+
+
+def gradient(weights, Xs, Ts):
+    """Loss and gradient from the GPU training kernels on standardised rows."""
+    L = load(False)
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    Xs = np.ascontiguousarray(Xs, dtype=np.float32)
+    Ts = np.ascontiguousarray(Ts, dtype=np.float32)
+    g = np.zeros(NW, dtype=np.float32)
+    loss = ctypes.c_float(0)
+    rc = L.echo_gpu_mlp_grad(w.ctypes.data_as(F), Xs.ctypes.data_as(F), Ts.ctypes.data_as(F), len(Xs),
+                             ctypes.pointer(loss), g.ctypes.data_as(F))
+    if rc:
+        raise RuntimeError(f"echo_gpu_mlp_grad status {rc}")
+    return float(loss.value), g

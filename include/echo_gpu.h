@@ -55,7 +55,10 @@ enum { ECHO_EOS_CONFORMAL = 1, ECHO_EOS_IDEALGAS = 2, ECHO_EOS_TABLE = 3 };
 /* con2prim solvers for ideal MHD (ALG_SOLV, common.f90:289) */
 enum {
   ECHO_C2P_BRENT = 1,   /* reference default: BRENTM on (v^2, w*gamma^2, p) */
-  ECHO_C2P_NEWTON = 100 /* this library: analytic-Jacobian Newton, same root */
+  ECHO_C2P_NEWTON = 100, /* this library: analytic-Jacobian Newton from the
+                            previous primitives, same root; BRENTM fallback */
+  ECHO_C2P_MLP = 101     /* Newton from the learned seed (<= 3 steps), then the
+                            ECHO_C2P_NEWTON path if it has not converged */
 };
 
 /* status codes */
@@ -195,6 +198,46 @@ int echo_gpu_test_recon(int recal, int m, int n, const double* f, double* gl,
 int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, int n_eos,
                       int ncells, double g3, double gp, const double* u,
                       double* v, int* err, int* iters);
+
+/* system_cons2prim of independent ideal-RMHD cells (u, v cell-major as in
+ * echo_gpu_test_c2p) at the residual p->c2p_tol: from the learned seed when
+ * weights != NULL (falling back to Newton from v, then BRENTM), else Newton
+ * from the guess in v.  seed_failed[c] = 1 where the seed did not converge
+ * within 3 Newton steps. */
+int echo_gpu_test_c2p_seeded(const EchoParams* p, const double* eos_table,
+                             int n_eos, int ncells, double g3, double gp,
+                             const float* weights, const float* norm,
+                             const double* u, double* v, int* err, int* iters,
+                             int* seed_failed);
+
+/* ---- learned con2prim seed (ECHO_C2P_MLP) -------------------------------- */
+
+/* The seed network is a 4x64 tanh MLP from five invariants of the conserved
+ * state (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3) to (v^2, p/U).  Weight
+ * vector: per layer W[K][N] row-major then b[N], (K,N) = (5,64), (64,64) x3,
+ * (64,2).  norm: feature mean[5], std[5], target mean[2], std[2]. */
+#define ECHO_MLP_NWEIGHTS 12994
+
+/* Trains the network with this library's own FP32 forward/backward kernels
+ * and Adam on n raw (invariants X[n][5], targets T[n][2]) pairs.  A set-up
+ * call: allocates device memory for the data and the optimiser.  loss_out
+ * receives one value every report_every steps (may be NULL). */
+int echo_gpu_mlp_train(const float* X, const float* T, int n, int steps,
+                       int batch, float lr, unsigned seed, float* weights_out,
+                       float* norm_out, float* loss_out, int report_every);
+
+/* Mean-squared loss and its gradient w.r.t. the weight vector on n
+ * standardised rows (gradient check against the CPU oracle). */
+int echo_gpu_mlp_grad(const float* weights, const float* Xs, const float* Ts,
+                      int n, float* loss, float* grad);
+
+/* Loads a trained network into a context (BF16 tensor-core fragments);
+ * required before stepping with algo_solver = ECHO_C2P_MLP.  Allocates. */
+int echo_gpu_mlp_set(EchoCtx* ctx, const float* weights, const float* norm);
+
+/* Tensor-core inference on n raw invariant rows -> out[n][2] = (v^2, p/U). */
+int echo_gpu_mlp_infer(const float* weights, const float* norm, const float* X,
+                       int n, float* out);
 
 /* ---- allocation-free stage right-hand side ------------------------------ */
 

@@ -2214,3 +2214,61 @@ int orc_flux(const EchoParams* p, const double* tab, int n_eos, double g3,
   for (int i = 0; i < 4; i++) free(bufs[i]);
   return r;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The learned con2prim seed network in FP64, for the gradient check of the */
+/* GPU training kernels: mean-squared loss over n standardised rows and its */
+/* gradient w.r.t. the weight vector (layout of ECHO_MLP_NWEIGHTS).         */
+/* ------------------------------------------------------------------------ */
+void orc_mlp_grad(const float* W, const float* Xs, const float* Ts, int n, double* loss, double* grad) {
+  static const int LK[5] = {5, 64, 64, 64, 64}, LN[5] = {64, 64, 64, 64, 2};
+  static const int WO[5] = {0, 384, 4544, 8704, 12864}, BO[5] = {320, 4480, 8640, 12800, 12992};
+  const int NW = 12994;
+  double* g = grad;
+  for (int i = 0; i < NW; i++) g[i] = 0.;
+  double L = 0.;
+  double act[6][64], dz[5][64];
+  for (int r = 0; r < n; r++) {
+    for (int j = 0; j < 5; j++) act[0][j] = Xs[r * 5 + j];
+    for (int l = 0; l < 5; l++)
+      for (int o = 0; o < LN[l]; o++) {
+        double z = W[BO[l] + o];
+        for (int k = 0; k < LK[l]; k++) z += act[l][k] * (double)W[WO[l] + k * LN[l] + o];
+        act[l + 1][o] = l < 4 ? tanh(z) : z;
+      }
+    for (int o = 0; o < 2; o++) {
+      double d = act[5][o] - Ts[r * 2 + o];
+      L += d * d / (2.0 * n);
+      dz[4][o] = 2.0 * d / (2.0 * n);
+    }
+    for (int l = 4; l >= 0; l--) {
+      for (int k = 0; k < LK[l]; k++)
+        for (int o = 0; o < LN[l]; o++) g[WO[l] + k * LN[l] + o] += act[l][k] * dz[l][o];
+      for (int o = 0; o < LN[l]; o++) g[BO[l] + o] += dz[l][o];
+      if (l > 0)
+        for (int k = 0; k < LK[l]; k++) {
+          double s = 0.;
+          for (int o = 0; o < LN[l]; o++) s += dz[l][o] * (double)W[WO[l] + k * LN[l] + o];
+          dz[l - 1][k] = s * (1. - act[l][k] * act[l][k]);
+        }
+    }
+  }
+  *loss = L;
+}
+
+/* FP64 forward pass on raw invariants with normalisation (seed accuracy) */
+void orc_mlp_forward(const float* W, const float* norm, const float* X, int n, double* out) {
+  static const int LK[5] = {5, 64, 64, 64, 64}, LN[5] = {64, 64, 64, 64, 2};
+  static const int WO[5] = {0, 384, 4544, 8704, 12864}, BO[5] = {320, 4480, 8640, 12800, 12992};
+  double act[6][64];
+  for (int r = 0; r < n; r++) {
+    for (int j = 0; j < 5; j++) act[0][j] = ((double)X[r * 5 + j] - norm[j]) / norm[5 + j];
+    for (int l = 0; l < 5; l++)
+      for (int o = 0; o < LN[l]; o++) {
+        double z = W[BO[l] + o];
+        for (int k = 0; k < LK[l]; k++) z += act[l][k] * (double)W[WO[l] + k * LN[l] + o];
+        act[l + 1][o] = l < 4 ? tanh(z) : z;
+      }
+    for (int o = 0; o < 2; o++) out[r * 2 + o] = act[5][o] * norm[12 + o] + norm[10 + o];
+  }
+}

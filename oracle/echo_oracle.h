@@ -62,6 +62,10 @@ int orc_flux(const EchoParams* p, const double* eos_table, int n_eos,
              double g3, double gp, int dir, double* v, double* u, double* f,
              double* vf);
 
+/* the learned con2prim seed network (gradient check, FP64) */
+void orc_mlp_grad(const float* W, const float* Xs, const float* Ts, int n, double* loss, double* grad);
+void orc_mlp_forward(const float* W, const float* norm, const float* X, int n, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,6 +56,9 @@ def lib():
                                     ctypes.c_double, D, D]
         L.orc_flux.argtypes = [P, D, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                ctypes.c_int, D, D, D, D]
+        Fp = ctypes.POINTER(ctypes.c_float)
+        L.orc_mlp_grad.argtypes = [Fp, Fp, Fp, ctypes.c_int, D, D]
+        L.orc_mlp_forward.argtypes = [Fp, Fp, Fp, ctypes.c_int, D]
         _lib = L
     return _lib
 
@@ -193,3 +196,27 @@ def flux(params, eos_table, g3, gp, direction, v):
     vf = np.zeros(2)
     err = lib().orc_flux(ctypes.byref(params), _dp(t), n, g3, gp, direction, _dp(v), _dp(u), _dp(f), _dp(vf))
     return err, u, f, vf
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mlp_grad(weights, Xs, Ts):
+    """FP64 loss and gradient of the seed network on standardised rows."""
+    W = np.ascontiguousarray(weights, dtype=np.float32)
+    X = np.ascontiguousarray(Xs, dtype=np.float32)
+    T = np.ascontiguousarray(Ts, dtype=np.float32)
+    g = np.zeros(W.size)
+    loss = ctypes.c_double(0)
+    lib().orc_mlp_grad(_fp(W), _fp(X), _fp(T), len(X), ctypes.byref(loss), _dp(g))
+    return loss.value, g
+
+
+def mlp_forward(weights, norm, X):
+    W = np.ascontiguousarray(weights, dtype=np.float32)
+    N = np.ascontiguousarray(norm, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    out = np.zeros((len(X), 2))
+    lib().orc_mlp_forward(_fp(W), _fp(N), _fp(X), len(X), _dp(out))
+    return out

@@ -1,0 +1,156 @@
+"""The learned con2prim seed: training kernels against the CPU oracle,
+tensor-core inference, and what the trained network gains.
+
+Tolerances:
+  gradients (FP32 GPU vs FP64 oracle): relative L2 1e-4;
+  inference (BF16 operands, FP32 accumulation vs FP64): 5 % of the
+      output's spread -- the precision of BF16 activations;
+  seeded steps vs the oracle's BRENTM step: 1e-12 relative L-inf, the
+      same bar as the plain path (the seed is always finished by Newton to
+      a 1e-10 residual plus one polishing correction).
+"""
+import numpy as np
+import pytest
+
+import pyoracle as O
+from echo_gpu import params as P
+from echo_gpu import seed as S
+from echo_gpu.lib import Evolve, unit_c2p_seeded
+from helpers import CASES, eos_table, rel_linf, setup
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_weights(rng):
+    w = np.zeros(S.NW, dtype=np.float32)
+    LK, LN = (5, 64, 64, 64, 64), (64, 64, 64, 64, 2)
+    WO, BO = (0, 384, 4544, 8704, 12864), (320, 4480, 8640, 12800, 12992)
+    for l in range(5):
+        a = np.sqrt(6.0 / (LK[l] + LN[l]))
+        w[WO[l]:WO[l] + LK[l] * LN[l]] = rng.uniform(-a, a, LK[l] * LN[l])
+        w[BO[l]:BO[l] + LN[l]] = rng.uniform(-0.1, 0.1, LN[l])
+    return w
+
+
+def test_training_gradient_matches_oracle():
+    rng = np.random.default_rng(11)
+    w = _random_weights(rng)
+    Xs = rng.standard_normal((256, 5)).astype(np.float32)
+    Ts = rng.standard_normal((256, 2)).astype(np.float32)
+    lg, gg = S.gradient(w, Xs, Ts)
+    lo, go = O.mlp_grad(w, Xs, Ts)
+    assert abs(lg - lo) <= 1e-5 * abs(lo)
+    assert np.linalg.norm(gg - go) <= 1e-4 * np.linalg.norm(go)
+
+
+def test_tensor_core_inference_matches_fp64():
+    rng = np.random.default_rng(12)
+    w = _random_weights(rng)
+    norm = np.array([0.5, 0.2, 0.1, 0.3, 0.05, 1.0, 0.3, 0.2, 0.4, 0.1, 0.2, 0.1, 0.3, 0.05], dtype=np.float32)
+    X = (rng.standard_normal((1000, 5)) * norm[5:10] + norm[:5]).astype(np.float32)
+    out = S.infer(w, norm, X)
+    ref = O.mlp_forward(w, norm, X)
+    spread = ref.std(0)
+    assert np.all(np.abs(out - ref).max(0) <= 0.05 * spread)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    X, T = S.generate_pairs(n_target=200_000, grid=24, steps=9, every=3)
+    w, norm, losses = S.train(X, T, steps=1500, batch=4096, lr=3e-3, report_every=100)
+    return X, T, w, norm, losses
+
+
+def test_training_reduces_loss(trained):
+    X, T, w, norm, losses = trained
+    assert losses[-1] < 0.1 * losses[0], losses
+    # seed accuracy on the training distribution (v^2 absolute, p/U relative)
+    idx = np.random.default_rng(3).choice(len(X), 4000, replace=False)
+    pred = S.infer(w, norm, X[idx])
+    assert np.median(np.abs(pred[:, 0] - T[idx, 0])) < 0.02
+    assert np.median(np.abs(pred[:, 1] / T[idx, 1] - 1)) < 0.1
+
+
+def _cells_from_run(cfg, steps=4):
+    pc, tab, v = setup(cfg)
+    ev = Evolve(pc.__class__.from_buffer_copy(pc), tab)
+    ev.upload(v, None, cfg.tstart)
+    ev.run(steps)
+    ev.sync()
+    st = ev.stats()
+    # the last inversion of the step used the metric of the step's start
+    # (the reference advances tau only after all stages, echo.f90:211-214)
+    t = st.t - st.dt
+    vv, uu = ev.download()
+    return pc, tab, vv.reshape(cfg.nv, -1).T.copy(), uu.reshape(cfg.nv, -1).T.copy(), t
+
+
+def test_seed_gain_over_cold_start(trained):
+    """Without previous primitives (a cold start: v = 0, p = U/3), Newton
+    needs more steps and more bracketed fallbacks than from the seed."""
+    _, _, w, norm, _ = trained
+    cfg = P.small(P.config1(), 16, nz=12).replace(algo_solver=P.C2P_NEWTON)
+    pc, tab, v, u, t = _cells_from_run(cfg)
+    cold = v.copy()
+    cold[:, 1:4] = 0.0
+    cold[:, 4] = u[:, 4] / t / 3.0
+    vs, es, its, sf = unit_c2p_seeded(pc, tab, t * t, t, u, cold, w, norm)
+    vc, ec, itc, _ = unit_c2p_seeded(pc, tab, t * t, t, u, cold)
+    assert (es == 0).all() and (ec == 0).all()
+    fb_seed = int((its >= 1000).sum())
+    fb_cold = int((itc >= 1000).sum())
+    it_seed = np.where(its >= 1000, its - 1000, its).mean()
+    it_cold = np.where(itc >= 1000, itc - 1000, itc).mean()
+    print(f"seeded: {it_seed:.2f} Newton steps/cell, {fb_seed} BRENTM fallbacks, {sf.mean():.3f} seed misses; "
+          f"cold: {it_cold:.2f} steps/cell, {fb_cold} fallbacks")
+    assert it_seed <= it_cold and fb_seed <= fb_cold and sf.mean() < 0.05
+    # both reach the root the run's own inversion found
+    assert rel_linf(vs.T.copy(), v.T.copy(), cfg.nv) < 1e-12
+    assert rel_linf(vc.T.copy(), v.T.copy(), cfg.nv) < 1e-12
+
+
+def test_seeded_steps_match_oracle(trained):
+    _, _, w, norm, _ = trained
+    cfg = CASES["rmhd3d"]().replace(algo_solver=P.C2P_MLP)
+    pc, tab, v = setup(cfg)
+    o = O.Oracle(cfg.replace(algo_solver=P.C2P_BRENT).to_c(przero=pc.przero), tab)
+    o.set_state(v, None, cfg.tstart)
+    v0, u0 = o.state()
+    g = Evolve(pc, tab)
+    g.set_seed_network(w, norm)
+    g.upload(v0, u0, cfg.tstart)
+    for _ in range(6):
+        o.step()
+    g.run(6)
+    g.sync()
+    st = g.stats()
+    assert st.errcode == 0
+    vg, ug = g.download()
+    vo, uo = o.state()
+    assert rel_linf(vg, vo, cfg.nv) <= 1e-12 and rel_linf(ug, uo, cfg.nv) <= 1e-12
+
+
+def test_newton_steps_match_oracle():
+    cfg = CASES["rmhd3d"]().replace(algo_solver=P.C2P_NEWTON)
+    pc, tab, v = setup(cfg)
+    o = O.Oracle(cfg.replace(algo_solver=P.C2P_BRENT).to_c(przero=pc.przero), tab)
+    o.set_state(v, None, cfg.tstart)
+    v0, u0 = o.state()
+    g = Evolve(pc, tab)
+    g.upload(v0, u0, cfg.tstart)
+    for _ in range(6):
+        o.step()
+    g.run(6)
+    g.sync()
+    vg, ug = g.download()
+    vo, uo = o.state()
+    assert rel_linf(vg, vo, cfg.nv) <= 1e-12 and rel_linf(ug, uo, cfg.nv) <= 1e-12
+
+
+def test_mlp_mode_requires_a_network():
+    cfg = CASES["rmhd3d"]().replace(algo_solver=P.C2P_MLP)
+    pc, tab, v = setup(cfg)
+    g = Evolve(pc, tab)
+    g.upload(v, None, cfg.tstart)
+    with pytest.raises(RuntimeError):
+        g.run(1)

@@ -92,3 +92,24 @@ def test_golden_vectors(name):
     vv, uu = o.state()
     assert np.array_equal(vv, g["v"]) and np.array_equal(uu, g["u"])
     assert o.t == meta["t"]
+
+
+def test_mlp_oracle_gradient_by_finite_differences():
+    # pins the FP64 network gradient the GPU training kernels are checked against
+    rng = np.random.default_rng(2)
+    w = (rng.standard_normal(12994) * 0.2).astype(np.float32)
+    X = rng.standard_normal((16, 5)).astype(np.float32)
+    T = rng.standard_normal((16, 2)).astype(np.float32)
+    _, g = O.mlp_grad(w, X, T)
+    for i in [0, 100, 330, 400, 5000, 9000, 12865, 12993]:
+        h = 2e-3 * max(1.0, abs(float(w[i])))
+        wp = w.astype(np.float64).copy()
+        wm = w.astype(np.float64).copy()
+        wp[i] += h
+        wm[i] -= h
+        # weights are float32 in the interface: use steps exactly representable
+        wp32, wm32 = wp.astype(np.float32), wm.astype(np.float32)
+        lp, _ = O.mlp_grad(wp32, X, T)
+        lm, _ = O.mlp_grad(wm32, X, T)
+        fd = (lp - lm) / (float(wp32[i]) - float(wm32[i]))
+        assert abs(fd - g[i]) <= 2e-3 * max(1e-3, abs(g[i])), (i, fd, g[i])
