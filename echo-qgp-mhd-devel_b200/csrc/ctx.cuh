@@ -56,6 +56,13 @@ inline void mark(EchoCtx* c, int cls) {
   c->marks->push_back({cls, e});
 }
 
+// shared by the single-grid and the batched contexts (echo_gpu.cu)
+int echo_kind_of(const EchoParams* p);
+int echo_nv_of(int kind);
+void echo_setup_bc(const EchoParams* p, int nv, BcDir bc[3], int uniform[3], int sign[3]);
+int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, DevPhys* P, double** d_tab,
+                    int** d_bk);
+
 // Bracket accelerator of tab_bracket: for every bucket of the bit pattern
 // (>> BK_SHIFT) between the first and last table value, the smallest
 // bracket index max(2, first i with arr(i) >= lowest value of the bucket).

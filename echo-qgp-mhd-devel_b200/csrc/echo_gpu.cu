@@ -60,6 +60,79 @@ int echo_nv_of(int kind) {
   }
 }
 
+// boundary codes of every variable and direction (ibc, init.f90:137-155)
+void echo_setup_bc(const EchoParams* p, int nv, BcDir bc[3], int uniform[3], int sign[3]) {
+  for (int d = 0; d < 3; d++)
+    for (int k = 0; k < ECHO_MAX_NV; k++)
+      for (int s = 0; s < 2; s++) bc[d].c[k][s] = (signed char)p->ibc[k][s][d];
+  for (int d = 0; d < 3; d++) {
+    int uni = 1, sgn = 0;
+    for (int k = 0; k < nv; k++)
+      for (int q = 0; q < 2; q++) {
+        int code = p->ibc[k][q][d];
+        if (code != p->ibc[0][q][d] || code == 3 || code < -1 || code > 3) uni = 0;
+        if (code == -1) sgn = 1;
+      }
+    uniform[d] = uni;
+    sign[d] = sgn;
+  }
+}
+
+// physics constants and the EoS table on the device (eos.f90:265-334)
+int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, DevPhys* P, double** d_tab,
+                    int** d_bk) {
+  *d_tab = nullptr;
+  int nt = 0;
+  if (eos_table && n_eos > 0) {
+    nt = n_eos;
+    std::vector<double> cols((size_t)4 * n_eos);
+    for (int i = 0; i < n_eos; i++)
+      for (int q = 0; q < 4; q++) cols[(size_t)q * n_eos + i] = eos_table[4 * i + q];
+    CK(cudaMalloc(d_tab, sizeof(double) * 4 * n_eos));
+    CK(cudaMemcpy(*d_tab, cols.data(), sizeof(double) * 4 * n_eos, cudaMemcpyHostToDevice));
+  }
+  P->eqstate = p->eqstate;
+  P->coordinates = p->coordinates;
+  P->recal = p->recal;
+  P->obtained_zz = p->obtained_zz;
+  P->init_type = p->init_type;
+  P->bulkvis = p->bulkvis;
+  P->nt = nt;
+  P->tT = *d_tab;
+  P->te = *d_tab ? *d_tab + nt : nullptr;
+  P->tp = *d_tab ? *d_tab + 2 * nt : nullptr;
+  P->tc = *d_tab ? *d_tab + 3 * nt : nullptr;
+  P->maxspeed = p->maxspeed;
+  P->eta_over_s = p->eta_over_s;
+  P->tau_pi_coeff = p->tau_pi_coeff;
+  P->enezero = p->enezero;
+  P->przero = p->przero;
+  P->glm_alpha = p->glm_alpha;
+  P->bke = P->bkp = nullptr;
+  *d_bk = nullptr;
+  if (nt > 0) {
+    std::vector<double> te(nt), tp(nt);
+    for (int i = 0; i < nt; i++) {
+      te[i] = eos_table[4 * i + 1];
+      tp[i] = eos_table[4 * i + 2];
+    }
+    std::vector<int> be, bp;
+    long long ke0 = 0, kp0 = 0;
+    if (echo_make_buckets(te.data(), nt, be, ke0) && echo_make_buckets(tp.data(), nt, bp, kp0)) {
+      CK(cudaMalloc(d_bk, sizeof(int) * (be.size() + bp.size())));
+      CK(cudaMemcpy(*d_bk, be.data(), sizeof(int) * be.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(*d_bk + be.size(), bp.data(), sizeof(int) * bp.size(), cudaMemcpyHostToDevice));
+      P->bke = *d_bk;
+      P->bkp = *d_bk + be.size();
+      P->bke0 = ke0;
+      P->bkp0 = kp0;
+      P->nbke = (int)be.size();
+      P->nbkp = (int)bp.size();
+    }
+  }
+  return ECHO_OK;
+}
+
 #define DISPATCH(c, fn, ...)                                      \
   do {                                                            \
     switch ((c)->kind) {                                          \
@@ -148,9 +221,11 @@ static void enqueue_stage(EchoCtx* c, int irk) {
   mark(c, PK_SCALARS);
   DISPATCH(c, launch_update, c, irk, MODE_RK, (double*)nullptr);
   mark(c, PK_UPDATE);
+  // stage 1 wrote the new u into the other buffer: it becomes current before
+  // the repair and the smoothing, which act on the new u
+  if (irk == 1) c->ucur = 1 - c->ucur;
   DISPATCH(c, launch_repair_smooth, c, 3);
   mark(c, PK_REPAIR);
-  if (irk == 1) c->ucur = 1 - c->ucur;
   c->vcur = 1 - c->vcur;
 }
 
@@ -210,20 +285,7 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->g.ddx = p->nx > 1 ? 1. / dx : 0.;
   c->g.ddy = p->ny > 1 ? 1. / dy : 0.;
   c->g.ddz = p->nz > 1 ? 1. / dz : 0.;
-  for (int d = 0; d < 3; d++)
-    for (int k = 0; k < ECHO_MAX_NV; k++)
-      for (int s = 0; s < 2; s++) c->bc[d].c[k][s] = (signed char)p->ibc[k][s][d];
-  for (int d = 0; d < 3; d++) {
-    int uni = 1, sgn = 0;
-    for (int k = 0; k < c->nv; k++)
-      for (int q = 0; q < 2; q++) {
-        int code = p->ibc[k][q][d];
-        if (code != p->ibc[0][q][d] || code == 3 || code < -1 || code > 3) uni = 0;
-        if (code == -1) sgn = 1;
-      }
-    c->bc_uniform[d] = uni;
-    c->bc_signed[d] = sgn;
-  }
+  echo_setup_bc(p, c->nv, c->bc, c->bc_uniform, c->bc_signed);
   c->nfaces[0] = (size_t)(p->nx + 1) * p->ny * p->nz;
   c->nfaces[1] = (size_t)p->nx * (p->ny + 1) * p->nz;
   c->nfaces[2] = (size_t)p->nx * p->ny * (p->nz + 1);
@@ -257,54 +319,9 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   CK(cudaMalloc(&c->d_sc, sizeof(DevScalars)));
   CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars)));
   memset(c->h_sc, 0, sizeof(DevScalars));
-  c->d_tab = nullptr;
-  int nt = 0;
-  if (eos_table && n_eos > 0) {
-    nt = n_eos;
-    std::vector<double> cols((size_t)4 * n_eos);
-    for (int i = 0; i < n_eos; i++)
-      for (int q = 0; q < 4; q++) cols[(size_t)q * n_eos + i] = eos_table[4 * i + q];
-    CK(cudaMalloc(&c->d_tab, sizeof(double) * 4 * n_eos));
-    CK(cudaMemcpy(c->d_tab, cols.data(), sizeof(double) * 4 * n_eos, cudaMemcpyHostToDevice));
-  }
-  c->P.eqstate = p->eqstate;
-  c->P.coordinates = p->coordinates;
-  c->P.recal = p->recal;
-  c->P.obtained_zz = p->obtained_zz;
-  c->P.init_type = p->init_type;
-  c->P.bulkvis = p->bulkvis;
-  c->P.nt = nt;
-  c->P.tT = c->d_tab;
-  c->P.te = c->d_tab ? c->d_tab + nt : nullptr;
-  c->P.tp = c->d_tab ? c->d_tab + 2 * nt : nullptr;
-  c->P.tc = c->d_tab ? c->d_tab + 3 * nt : nullptr;
-  c->P.maxspeed = p->maxspeed;
-  c->P.eta_over_s = p->eta_over_s;
-  c->P.tau_pi_coeff = p->tau_pi_coeff;
-  c->P.enezero = p->enezero;
-  c->P.przero = p->przero;
-  c->P.glm_alpha = p->glm_alpha;
-  c->P.bke = c->P.bkp = nullptr;
-  c->d_bk = nullptr;
-  if (nt > 0) {
-    std::vector<double> te(nt), tp(nt);
-    for (int i = 0; i < nt; i++) {
-      te[i] = eos_table[4 * i + 1];
-      tp[i] = eos_table[4 * i + 2];
-    }
-    std::vector<int> be, bp;
-    long long ke0 = 0, kp0 = 0;
-    if (echo_make_buckets(te.data(), nt, be, ke0) && echo_make_buckets(tp.data(), nt, bp, kp0)) {
-      CK(cudaMalloc(&c->d_bk, sizeof(int) * (be.size() + bp.size())));
-      CK(cudaMemcpy(c->d_bk, be.data(), sizeof(int) * be.size(), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(c->d_bk + be.size(), bp.data(), sizeof(int) * bp.size(), cudaMemcpyHostToDevice));
-      c->P.bke = c->d_bk;
-      c->P.bkp = c->d_bk + be.size();
-      c->P.bke0 = ke0;
-      c->P.bkp0 = kp0;
-      c->P.nbke = (int)be.size();
-      c->P.nbkp = (int)bp.size();
-    }
+  {
+    int r = echo_setup_phys(p, eos_table, n_eos, &c->P, &c->d_tab, &c->d_bk);
+    if (r) return r;
   }
   c->d_du = nullptr;
   c->marks = nullptr;

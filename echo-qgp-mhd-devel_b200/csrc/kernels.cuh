@@ -115,18 +115,24 @@ struct FaceArgs {
 //   DIR 0: F[k][iz][iy][i],  i = 0..nx
 //   DIR 1: F[k][iz][j][ix],  j = 0..ny
 //   DIR 2: F[k][kz][iy][ix], kz = 0..nz
+template <int DIR>
+__host__ __device__ __forceinline__ size_t faces_of(const Grid& g) {
+  return DIR == 0 ? (size_t)(g.nx + 1) * g.ny * g.nz
+         : DIR == 1 ? (size_t)g.nx * (g.ny + 1) * g.nz
+                    : (size_t)g.nx * g.ny * (g.nz + 1);
+}
+
+// The flux through face `fid` (< faces_of<DIR>(A.g)): writes A.F (and A.WD)
+// and returns the face's signal speed max(a+, a-) for the CFL reduction.
 template <int KIND, int DIR>
-__global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) faces_kernel(FaceArgs A) {
+__device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const Grid& g = A.g;
   const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
-  const size_t nfaces = DIR == 0 ? (size_t)(g.nx + 1) * g.ny * g.nz
-                        : DIR == 1 ? (size_t)g.nx * (g.ny + 1) * g.nz
-                                   : (size_t)g.nx * g.ny * (g.nz + 1);
-  size_t fid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nfaces = faces_of<DIR>(g);
   double amax_local = 0.0;
-  if (fid < nfaces) {
+  {
     int i, a, b;  // face index along DIR, transverse coordinates (1-based)
     size_t base;
     long long stride;
@@ -293,9 +299,14 @@ __global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) faces_kernel(F
       if (i == n && a == na && b == nb) A.sc->aflux[DIR] = amax_local;
     }
   }
-  // block max of the signal speed -> one atomic per block (CFL reduction, evolve.f90:723-764)
-  __shared__ double red[4];
-  double m = amax_local;
+  return amax_local;
+}
+
+// Block max of the signal speed -> one atomic per block (the CFL reduction of
+// evolve_dt, evolve.f90:723-764).  Positive doubles order like their bit
+// patterns, so the max is an integer atomicMax.  Called by every thread of
+// the block; `red` holds one entry per warp.
+__device__ __forceinline__ void block_max_atomic(double m, unsigned long long* dst, double* red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     double x = __shfl_xor_sync(0xffffffffu, m, o);
@@ -306,8 +317,16 @@ __global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) faces_kernel(F
   if (threadIdx.x == 0) {
     double mm = red[0];
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) mm = red[w] > mm ? red[w] : mm;
-    if (mm > 0.0) atomicMax(&A.sc->amax_bits[DIR], (unsigned long long)__double_as_longlong(mm));
+    if (mm > 0.0) atomicMax(dst, (unsigned long long)__double_as_longlong(mm));
   }
+}
+
+template <int KIND, int DIR>
+__global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) faces_kernel(FaceArgs A) {
+  __shared__ double red[4];
+  size_t fid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double amax_local = fid < faces_of<DIR>(A.g) ? face_flux<KIND, DIR>(A, fid) : 0.0;
+  block_max_atomic(amax_local, &A.sc->amax_bits[DIR], red);
 }
 
 // ---------------------------------------------------------------------------
@@ -322,7 +341,7 @@ struct ScalarArgs {
              // sweeps of stage 1, from the previous stage's speeds); 2: IMEX-SSP GLM
 };
 
-static __global__ void stage_scalars_kernel(ScalarArgs A) {
+__device__ __forceinline__ void stage_scalars(const ScalarArgs& A) {
   DevScalars* sc = A.sc;
   if (A.mode != 1) {
     // glm_ch = glm_ch_old (start of stage); glm_ch_old = maxval(aflux) (end of sweeps)
@@ -370,8 +389,10 @@ static __global__ void stage_scalars_kernel(ScalarArgs A) {
   if (A.divclean && A.mode != 1) sc->expfact = exp(-sc->glm_ch * sc->glm_ch * A.glm_alpha * (sc->dt / 2.));
 }
 
+static __global__ void stage_scalars_kernel(ScalarArgs A) { stage_scalars(A); }
+
 // end of step (echo.f90:211-241)
-static __global__ void end_step_kernel(DevScalars* sc, int coordinates) {
+__device__ __forceinline__ void end_step_scalars(DevScalars* sc, int coordinates) {
   sc->timeold = sc->t;
   sc->t = sc->t + sc->dt;
   double g3 = coordinates == ECHO_BJORKEN ? sc->timeold * sc->timeold : 1.;
@@ -383,6 +404,8 @@ static __global__ void end_step_kernel(DevScalars* sc, int coordinates) {
     if ((fabs(sc->tout - sc->tmax) < 1.e-10) || (sc->tout > sc->tmax)) sc->tout = sc->tmax;
   }
 }
+
+static __global__ void end_step_kernel(DevScalars* sc, int coordinates) { end_step_scalars(sc, coordinates); }
 
 // ---------------------------------------------------------------------------
 // per-cell update
@@ -412,6 +435,9 @@ struct UpdateArgs {
   int irk, nrk, divclean, coordinates, algo, mode;
   double tol;
   MlpDev mlp;  // learned seed (algo == ECHO_C2P_MLP)
+  // viscous, stage 1 of a batched step: vnewstep = v (echo.f90:192-202) is
+  // taken here, per cell, instead of by a separate copy; null otherwise
+  double* vsnap;
 };
 
 // Learned con2prim seed of the calling lane's cell from its conserved
@@ -433,14 +459,16 @@ __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, boo
   mlp_warp(net, f, seed);
 }
 
+// The update of cell c (flux divergence, sources, RK combination,
+// con2prim).  Called by every thread of a warp together (the learned seed
+// and the counters are warp-collective); threads without a cell pass
+// active = false.
 template <int KIND, bool SEED>
-__global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
+__device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool active) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const Grid& g = A.g;
-  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long my_iters = 0, my_fallbacks = 0;
-  const bool active = c < g.ncell;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
   double vv[NV], uu[NV];
   if (active) {
@@ -495,11 +523,24 @@ __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
                          (A.WDz[(size_t)q * nfz + fz + s] + A.WDz[(size_t)(4 + q) * nfz + fz + s] -
                           A.WDz[(size_t)q * nfz + fz] - A.WDz[(size_t)(4 + q) * nfz + fz]);
       }
+      if (A.vsnap) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) A.vsnap[(size_t)k * g.ncell + c] = vv[k];
+      }
       // dts (viscous.f90:56-97)
       double ti = A.sc->timeinterval;
       if (ti != 0) {
         double vxo = A.vold[1 * g.ncell + c], vyo = A.vold[2 * g.ncell + c], vzo = A.vold[3 * g.ncell + c];
-        double vx = A.vnew[1 * g.ncell + c], vy = A.vnew[2 * g.ncell + c], vz = A.vnew[3 * g.ncell + c];
+        double vx, vy, vz;
+        if (A.vsnap) {
+          vx = vv[KVX];
+          vy = vv[KVY];
+          vz = vv[KVZ];
+        } else {
+          vx = A.vnew[1 * g.ncell + c];
+          vy = A.vnew[2 * g.ncell + c];
+          vz = A.vnew[3 * g.ncell + c];
+        }
         double gamma1 = 1. / sqrt(1. - M.g1 * (vxo * vxo) - M.g2 * (vyo * vyo) - A.sc->g3old * (vzo * vzo));
         double gamma2 = 1. / sqrt(1. - M.g1 * (vx * vx) - M.g2 * (vy * vy) - M.g3 * (vz * vz));
         dv[DTT] = (gamma2 - gamma1) / (ti);
@@ -570,6 +611,12 @@ __global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
     if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
     if ((threadIdx.x & 31) == 0 && my_fallbacks) atomicAdd(&A.sc->fallbacks, my_fallbacks);
   }
+}
+
+template <int KIND, bool SEED>
+__global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  update_cell<KIND, SEED>(A, c, c < A.g.ncell);
 }
 
 // ---------------------------------------------------------------------------
@@ -681,13 +728,12 @@ __device__ __forceinline__ double flat_u(const double* u, size_t tot, long long 
   return u[off];
 }
 
+// Called by every thread of one block; s_any and s_stop are block-shared.
 template <int KIND>
-__global__ void __launch_bounds__(256) repair_kernel(RepairArgs A) {
+__device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int& s_stop) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
-  if (A.sc->nfail == 0) return;
   const Grid& g = A.g;
-  __shared__ int s_any, s_stop;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
   if (threadIdx.x == 0) s_stop = 0;
   for (size_t chunk = 0; chunk < g.ncell; chunk += blockDim.x) {
@@ -754,6 +800,13 @@ __global__ void __launch_bounds__(256) repair_kernel(RepairArgs A) {
   }
 }
 
+template <int KIND>
+__global__ void __launch_bounds__(256) repair_kernel(RepairArgs A) {
+  if (A.sc->nfail == 0) return;
+  __shared__ int s_any, s_stop;
+  repair_grid<KIND>(A, s_any, s_stop);
+}
+
 // evolve_smooth_viscosity (evolve.f90:1159-1207)
 struct SmoothArgs {
   DevPhys P;
@@ -766,10 +819,8 @@ struct SmoothArgs {
 };
 
 template <int KIND>
-__global__ void smooth_kernel(SmoothArgs A) {
+__device__ __forceinline__ void smooth_cell(const SmoothArgs& A, size_t c) {
   typedef Traits<KIND> T;
-  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= A.g.ncell) return;
   double pr = A.v[(size_t)KPR * A.g.ncell + c];
   if (!(pr < A.smooth_pressure)) return;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
@@ -792,6 +843,12 @@ __global__ void smooth_kernel(SmoothArgs A) {
     A.u[(size_t)k * A.g.ncell + c] = uu[k];
   }
   if (err) atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
+}
+
+template <int KIND>
+__global__ void smooth_kernel(SmoothArgs A) {
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < A.g.ncell) smooth_cell<KIND>(A, c);
 }
 
 // system_prim2cons over the grid (state upload without u)

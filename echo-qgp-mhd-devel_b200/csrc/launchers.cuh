@@ -2,7 +2,7 @@
 // included only by kind_*.cu, each of which instantiates one equation set.
 #pragma once
 
-#include "ctx.cuh"
+#include "batch.cuh"
 
 namespace echo {
 
@@ -64,6 +64,7 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   A.tol = c->p.c2p_tol;
   A.mlp.frag = c->d_mlp_frag;
   A.mlp.par = c->d_mlp_par;
+  A.vsnap = nullptr;
   if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;  // no network loaded
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
   if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP && mode == MODE_RK)
@@ -141,6 +142,113 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
     ssp_combine_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
 }
 
+// ---------------------------------------------------------------------------
+// batched launches (one launch per phase over all live events)
+// ---------------------------------------------------------------------------
+template <int KIND>
+void launch_batch_faces(EchoBatch* b, int dir) {
+  FaceArgs A;
+  A.P = b->P;
+  A.g = Grid{};
+  A.bc = b->bc[dir];
+  A.bc_uniform = b->bc_uniform[dir];
+  A.bc_signed = b->bc_signed[dir];
+  A.v = b->d_v[b->vcur];
+  A.F = b->d_F[dir];
+  A.WD = b->d_WD[dir];
+  A.sc = nullptr;
+  A.coordinates = b->p.coordinates;
+  BatchDev B = batch_dev(b);
+  unsigned grid = batch_grid(b, SL_FX + dir, PH_FX + dir);
+  if (dir == 0) batch_faces_kernel<KIND, 0><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+  if (dir == 1) batch_faces_kernel<KIND, 1><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+  if (dir == 2) batch_faces_kernel<KIND, 2><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+}
+
+template <int KIND>
+void launch_batch_update(EchoBatch* b, int irk) {
+  static const double crk[3][3][2] = {{{0., 1.}, {0., 0.}, {0., 0.}},
+                                      {{0., 1.}, {1. / 2., 1. / 2.}, {0., 0.}},
+                                      {{0., 1.}, {3. / 4., 1. / 4.}, {1. / 3., 2. / 3.}}};
+  UpdateArgs A;
+  A.P = b->P;
+  A.g = Grid{};
+  A.Fx = b->d_F[0];
+  A.Fy = b->d_F[1];
+  A.Fz = b->d_F[2];
+  A.WDx = b->d_WD[0];
+  A.WDy = b->d_WD[1];
+  A.WDz = b->d_WD[2];
+  A.vin = b->d_v[b->vcur];
+  A.vout = b->d_v[1 - b->vcur];
+  A.uin = b->d_u[b->ucur];
+  A.uout = irk == 1 ? b->d_u[1 - b->ucur] : b->d_u[b->ucur];
+  A.u0 = irk == 1 ? b->d_u[b->ucur] : b->d_u[1 - b->ucur];
+  A.vnew = b->d_vh[b->vn];
+  A.vold = b->d_vh[1 - b->vn];
+  A.vsnap = (Traits<KIND>::VISC && irk == 1) ? b->d_vh[b->vn] : nullptr;
+  A.du_out = nullptr;
+  A.fail = b->d_fail;
+  A.sc = nullptr;
+  int nrk = b->p.nrk;
+  A.c1 = crk[nrk - 1][irk - 1][0];
+  A.c2 = crk[nrk - 1][irk - 1][1];
+  A.irk = irk;
+  A.nrk = nrk;
+  A.divclean = b->p.divclean;
+  A.coordinates = b->p.coordinates;
+  A.algo = b->p.algo_solver;
+  A.mode = MODE_RK;
+  A.tol = b->p.c2p_tol;
+  A.mlp.frag = nullptr;
+  A.mlp.par = nullptr;
+  batch_update_kernel<KIND, false><<<batch_grid(b, SL_UPDATE, PH_CELL), 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+}
+
+template <int KIND>
+void launch_batch_repair_smooth(EchoBatch* b) {
+  RepairArgs R;
+  R.P = b->P;
+  R.g = Grid{};
+  R.vold = b->d_v[b->vcur];
+  R.vnew = b->d_v[1 - b->vcur];
+  R.u = b->d_u[b->ucur];
+  R.fail = b->d_fail;
+  R.sc = nullptr;
+  R.coordinates = b->p.coordinates;
+  R.algo = b->p.algo_solver;
+  R.maxspeed = b->p.maxspeed;
+  R.tol = b->p.c2p_tol;
+  batch_repair_kernel<KIND><<<(unsigned)b->nev, 256, 0, b->stream>>>(R, batch_dev(b), b->nv);
+  if (KIND == KIND_VISC && b->p.enable_smooth_viscosity) {
+    SmoothArgs S;
+    S.P = b->P;
+    S.g = Grid{};
+    S.v = b->d_v[1 - b->vcur];
+    S.u = b->d_u[b->ucur];
+    S.sc = nullptr;
+    S.coordinates = b->p.coordinates;
+    S.smooth_pressure = b->p.smooth_pressure;
+    batch_smooth_kernel<KIND><<<batch_grid(b, SL_SMOOTH, PH_CELL), 128, 0, b->stream>>>(S, batch_dev(b), b->nv);
+  }
+}
+
+template <int KIND>
+void launch_batch_p2c(EchoBatch* b) {
+  batch_p2c_kernel<KIND><<<(unsigned)(b->max_tiles[PH_CELL] > 0 ? b->max_tiles[PH_CELL] : 1), 128, 0, b->stream>>>(
+      b->P, batch_dev(b), b->nv, b->p.coordinates, b->d_v[b->vcur], b->d_u[b->ucur]);
+}
+
+template <int KIND>
+void batch_occupancy(const EchoBatch* b, int* per_sm) {
+  (void)b;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FX], batch_faces_kernel<KIND, 0>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FY], batch_faces_kernel<KIND, 1>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FZ], batch_faces_kernel<KIND, 2>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_UPDATE], batch_update_kernel<KIND, false>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_SMOOTH], batch_smooth_kernel<KIND>, 128, 0);
+}
+
 }  // namespace echo
 
 #define ECHO_INSTANTIATE(K)                                                   \
@@ -148,4 +256,9 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
   template void echo::launch_update<K>(EchoCtx*, int, int, double*);          \
   template void echo::launch_repair_smooth<K>(EchoCtx*, int);                      \
   template void echo::launch_p2c<K>(EchoCtx*);                                \
-  template void echo::launch_ssp_combine<K>(EchoCtx*, int);
+  template void echo::launch_ssp_combine<K>(EchoCtx*, int);                   \
+  template void echo::launch_batch_faces<K>(EchoBatch*, int);                 \
+  template void echo::launch_batch_update<K>(EchoBatch*, int);                \
+  template void echo::launch_batch_repair_smooth<K>(EchoBatch*);              \
+  template void echo::launch_batch_p2c<K>(EchoBatch*);                        \
+  template void echo::batch_occupancy<K>(const EchoBatch*, int*);

@@ -146,13 +146,13 @@ def optical_glauber(x: np.ndarray, y: np.ndarray, b: float, nucleus: str = "Au",
     return e * (peak / e.max())
 
 
-def mc_glauber(x: np.ndarray, y: np.ndarray, b: float, rng: np.random.Generator,
-               nucleus: str = "Pb", sigma_in_mb: float = 70.0,
-               smear: float = 0.5, ah: float = 0.15,
-               peak: float = 30.0) -> np.ndarray:
-    """One Monte Carlo Glauber event: Woods-Saxon nucleons, participants by
-    d^2 <= sigma/pi (glaubermc.f90:411), each participant and binary
-    collision smeared by a normalised 2D Gaussian of width ``smear``."""
+def glauber_sources(b: float, rng: np.random.Generator, nucleus: str = "Pb",
+                    sigma_in_mb: float = 70.0) -> tuple[np.ndarray, np.ndarray]:
+    """Participants and binary collisions of one Monte Carlo Glauber event:
+    Woods-Saxon nucleons of both nuclei (centres at x = -+b/2), a nucleon
+    pair collides when d^2 <= sigma/pi (glaubermc.f90:411).  Returns the
+    transverse positions (n, 2) of the participants and of the collision
+    midpoints."""
     A, R, a, rho0 = NUCLEI[nucleus]
     sig = sigma_in_mb / 10.0
     nA = int(A)
@@ -177,6 +177,14 @@ def mc_glauber(x: np.ndarray, y: np.ndarray, b: float, rng: np.random.Generator,
     parts = np.concatenate([pa[hit.any(1)], pb[hit.any(0)]])
     ia, ib = np.nonzero(hit)
     colls = 0.5 * (pa[ia] + pb[ib])
+    return parts, colls
+
+
+def smear_sources(x: np.ndarray, y: np.ndarray, parts: np.ndarray, colls: np.ndarray,
+                  smear: float = 0.5, ah: float = 0.15) -> np.ndarray:
+    """Unnormalised energy density (ny, nx): every participant (weight 1-ah)
+    and binary collision (weight ah) smeared by a normalised 2D Gaussian of
+    width ``smear`` (generate_energy_density_profile, glaubermc.f90:686-873)."""
     X, Y = np.meshgrid(x, y, indexing="xy")
     e = np.zeros_like(X)
     norm = 1.0 / (2 * np.pi * smear**2)
@@ -184,6 +192,17 @@ def mc_glauber(x: np.ndarray, y: np.ndarray, b: float, rng: np.random.Generator,
         e += (1 - ah) * norm * np.exp(-((X - px) ** 2 + (Y - py) ** 2) / (2 * smear**2))
     for (px, py) in colls:
         e += ah * norm * np.exp(-((X - px) ** 2 + (Y - py) ** 2) / (2 * smear**2))
+    return e
+
+
+def mc_glauber(x: np.ndarray, y: np.ndarray, b: float, rng: np.random.Generator,
+               nucleus: str = "Pb", sigma_in_mb: float = 70.0,
+               smear: float = 0.5, ah: float = 0.15,
+               peak: float = 30.0) -> np.ndarray:
+    """One Monte Carlo Glauber event on the grid x, y, normalised to
+    ``peak`` at its maximum."""
+    parts, colls = glauber_sources(b, rng, nucleus, sigma_in_mb)
+    e = smear_sources(x, y, parts, colls, smear, ah)
     if e.max() <= 0:
         return e
     return e * (peak / e.max())

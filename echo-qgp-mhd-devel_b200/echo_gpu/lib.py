@@ -35,6 +35,20 @@ class EchoStats(ctypes.Structure):
     ]
 
 
+class EchoEventGrid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("x1", ctypes.c_double), ("x2", ctypes.c_double), ("y1", ctypes.c_double),
+                ("y2", ctypes.c_double), ("z1", ctypes.c_double), ("z2", ctypes.c_double)]
+
+
+class EchoEventStatus(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_longlong),
+                ("state", ctypes.c_int), ("errcode", ctypes.c_int), ("err_cell", ctypes.c_int),
+                ("pad", ctypes.c_int), ("c2p_iters", ctypes.c_longlong), ("repairs", ctypes.c_longlong)]
+
+
+LL = ctypes.POINTER(ctypes.c_longlong)
+
 FUNCTIONS = {
     "echo_gpu_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.POINTER(P)]),
     "echo_gpu_free": (ctypes.c_int, [P]),
@@ -66,6 +80,25 @@ FUNCTIONS = {
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
+    "echo_batch_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(EchoEventGrid),
+                                       ctypes.POINTER(P)]),
+    "echo_batch_free": (ctypes.c_int, [P]),
+    "echo_batch_nv": (ctypes.c_int, [P]),
+    "echo_batch_offsets": (ctypes.c_int, [P, LL]),
+    "echo_batch_upload": (ctypes.c_int, [P, D, D, ctypes.c_double, ctypes.c_double]),
+    "echo_batch_upload_device": (ctypes.c_int, [P, P, P, ctypes.c_double, ctypes.c_double]),
+    "echo_batch_download": (ctypes.c_int, [P, D, D]),
+    "echo_batch_glauber": (ctypes.c_int, [P, D, LL, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double]),
+    "echo_batch_run": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_batch_live": (ctypes.c_int, [P, I]),
+    "echo_batch_status": (ctypes.c_int, [P, ctypes.POINTER(EchoEventStatus)]),
+    "echo_batch_sync": (ctypes.c_int, [P]),
+    "echo_batch_stream": (ctypes.c_int, [P, ctypes.POINTER(P)]),
+    "echo_batch_set_schedule": (ctypes.c_int, [P, I, I]),
+    "echo_batch_get_schedule": (ctypes.c_int, [P, I]),
+    "echo_batch_autotune": (ctypes.c_int, [P, ctypes.c_int, D]),
+    "echo_batch_profile_step": (ctypes.c_int, [P, D, I]),
 }
 
 

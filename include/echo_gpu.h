@@ -269,6 +269,95 @@ int echo_gpu_rhs_noalloc(const EchoParams* p, const double* d_eos_cols,
                          int n_eos, double t, const double* d_v, double* d_du,
                          void* stream, int* errcode);
 
+/* ---- batched event-by-event runs ----------------------------------------- */
+
+/* No single counterpart in the reference: a batch replaces the events loop
+ * of echo.f90:113-308 (Monte Carlo Glauber mode runs its events one after
+ * another, each through the whole time loop) by advancing many events at
+ * once.  Every event has its own grid size and extent, its own t, dt
+ * (evolve_dt per event), stop test (t >= tmax, echo.f90:187) and crash
+ * state (a crashed event is abandoned, the others go on: echo.f90:206-209,
+ * 283-307); the physics switches (EchoParams other than the grid fields) are
+ * shared.  Per event the arithmetic is the single-grid path's.
+ *
+ * Arrays cross as one arena: event e's primitives v(ix,iy,iz,k) (Fortran
+ * order, nv * ncell_e doubles) start at nv * cell_offset[e], where
+ * cell_offset is the running sum of the events' cell counts. */
+typedef struct EchoBatch EchoBatch;
+
+typedef struct EchoEventGrid {
+  int nx, ny, nz;
+  double x1, x2, y1, y2, z1, z2;
+} EchoEventGrid;
+
+/* event states */
+enum { ECHO_EVENT_LIVE = 0, ECHO_EVENT_DONE = 1, ECHO_EVENT_CRASHED = 2 };
+
+typedef struct EchoEventStatus {
+  double t, dt;
+  long long steps;      /* completed time steps */
+  int state;            /* ECHO_EVENT_* */
+  int errcode;          /* reference code of the crash, 0 = none */
+  int err_cell;
+  int pad;
+  long long c2p_iters;  /* con2prim iterations of the last stage */
+  long long repairs;    /* con2prim repairs so far */
+} EchoEventStatus;
+
+/* launch-shape slots (echo_batch_set_schedule) */
+enum { ECHO_SLOT_FACES_X = 0, ECHO_SLOT_FACES_Y = 1, ECHO_SLOT_FACES_Z = 2,
+       ECHO_SLOT_UPDATE = 3, ECHO_SLOT_SMOOTH = 4, ECHO_NSLOTS = 5 };
+
+/* Allocates the batch (RK2 or RK3; the plain con2prim solvers).  The grid
+ * fields of p are ignored; grids[e] gives event e's. */
+int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos,
+                     int nev, const EchoEventGrid* grids, EchoBatch** out);
+int echo_batch_free(EchoBatch* b);
+int echo_batch_nv(const EchoBatch* b);
+/* cell_offset[0..nev]: first cell of each event, [nev] = total cells */
+int echo_batch_offsets(const EchoBatch* b, long long* cell_offset);
+/* State of every event at time t (host arrays; u may be NULL: computed by
+ * system_prim2cons); events run until t >= tmax.  Resets every event to
+ * live, zero steps. */
+int echo_batch_upload(EchoBatch* b, const double* v, const double* u, double t,
+                      double tmax);
+int echo_batch_upload_device(EchoBatch* b, const double* d_v, const double* d_u,
+                             double t, double tmax);
+/* Monte Carlo Glauber initial state of every event, generated on the device
+ * (the energy-density part of generate_energy_density_profile,
+ * glaubermc.f90:686-873): the sources of event e -- participants and
+ * binary-collision points with their weights, src[3*i..3*i+2] = (x, y, w)
+ * for i in [src_offset[e], src_offset[e+1]) -- are smeared by a normalised
+ * 2D Gaussian of width sigma (fm) at the cell centres; per event
+ * e = peak * S / max(S) + ENEZERO, p = p(e) from the EoS, rho = 1, every
+ * other variable 0, u by system_prim2cons.  Then as echo_batch_upload.
+ * Sampling the nucleons stays on the host.  Allocates and frees device
+ * memory for the sources. */
+int echo_batch_glauber(EchoBatch* b, const double* src, const long long* src_offset,
+                       double sigma, double peak, double t, double tmax);
+int echo_batch_download(EchoBatch* b, double* v, double* u);
+/* nsteps time steps of every live event, asynchronous (one CUDA graph per
+ * step); finished and crashed events drop out on the device */
+int echo_batch_run(EchoBatch* b, int nsteps);
+/* synchronises; number of live events */
+int echo_batch_live(EchoBatch* b, int* nlive);
+/* synchronises; status of every event (nev entries) */
+int echo_batch_status(EchoBatch* b, EchoEventStatus* st);
+int echo_batch_sync(EchoBatch* b);
+int echo_batch_stream(EchoBatch* b, void** stream);
+/* Launch shape of each slot: the number of CTAs of its persistent launch
+ * (0 = one CTA per tile); order (nev entries, or NULL = 0..nev-1) is the
+ * order in which the tile lists visit the events. */
+int echo_batch_set_schedule(EchoBatch* b, const int* ctas, const int* order);
+int echo_batch_get_schedule(const EchoBatch* b, int* ctas);
+/* Times the candidate launch shapes of every slot on the current state
+ * (the face sweeps and the first-stage update are re-run `reps` times per
+ * candidate; the state and every event's scalars are restored) and keeps
+ * the fastest; ms[slot] = its time per launch.  Synchronises. */
+int echo_batch_autotune(EchoBatch* b, int reps, double* ms);
+/* one step with per-phase CUDA-event timing, like echo_gpu_profile_step */
+int echo_batch_profile_step(EchoBatch* b, double* ms, int* launches);
+
 #ifdef __cplusplus
 }
 #endif

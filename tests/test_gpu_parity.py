@@ -18,11 +18,23 @@ from helpers import CASES, rel_linf, setup
 pytestmark = pytest.mark.gpu
 
 
-def _pair(cfg, steps, exact=True, use_run=False):
+def _corrupt_centre(cfg, u0):
+    """|S^x| = 2 E in the centre cell: its inversion fails in the first stage
+    and the neighbour-average repair (evolve.f90:795-842) takes over."""
+    u = u0.reshape(cfg.nv, -1).copy()
+    c = (cfg.nz // 2) * cfg.nx * cfg.ny + (cfg.ny // 2) * cfg.nx + cfg.nx // 2
+    u[1, c] = 2.0 * u[4, c]
+    return u.reshape(-1)
+
+
+def _pair(cfg, steps, exact=True, use_run=False, prep=None):
     pc, tab, v = setup(cfg)
     o = O.Oracle(pc, tab)
     o.set_state(v, None, cfg.tstart)
     v0, u0 = o.state()
+    if prep is not None:
+        u0 = prep(cfg, u0)
+        o.set_state(v0, u0, cfg.tstart)
     g = Evolve(pc, tab, exact=exact)
     g.upload(v0, u0, cfg.tstart)
     for _ in range(steps):
@@ -81,6 +93,27 @@ def test_imex_ssp_parity(case, steps):
     ev, eu, _, _ = _pair(cfg, steps, exact=True)
     assert ev <= 1e-13 and eu <= 1e-13, (ev, eu)
     ev, eu, _, _ = _pair(cfg, steps, exact=False, use_run=True)
+    assert ev <= 1e-12 and eu <= 1e-12, (ev, eu)
+
+
+@pytest.mark.parametrize("case,nrk", [("hd2d", P.RK2), ("visc2d", P.RK2), ("hd2d", P.RK3), ("hd2d", P.SSP)])
+def test_repair_parity(case, nrk):
+    cfg = CASES[case]().replace(nrk=nrk)
+    ev, eu, o, g = _pair(cfg, 3, exact=True, prep=_corrupt_centre)
+    assert o.repairs > 0 and g.stats().repairs == o.repairs, (o.repairs, g.stats().repairs)
+    assert ev <= 1e-13 and eu <= 1e-13, (ev, eu)
+    ev, eu, o, g = _pair(cfg, 3, exact=False, use_run=True, prep=_corrupt_centre)
+    assert ev <= 1e-12 and eu <= 1e-12, (ev, eu)
+
+
+@pytest.mark.parametrize("nrk", [P.RK2, P.SSP])
+def test_smoothing_parity(nrk):
+    # T_cut = 0.35 GeV puts about three quarters of the cells under p_cut, so
+    # evolve_smooth_viscosity (evolve.f90:1159-1207) acts after every stage
+    cfg = CASES["visc2d"]().replace(smooth_temp=0.35, nrk=nrk)
+    ev, eu, o, g = _pair(cfg, 6, exact=True)
+    assert ev <= 1e-13 and eu <= 1e-13, (ev, eu)
+    ev, eu, o, g = _pair(cfg, 6, exact=False, use_run=True)
     assert ev <= 1e-12 and eu <= 1e-12, (ev, eu)
 
 
