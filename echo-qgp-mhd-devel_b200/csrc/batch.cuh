@@ -138,8 +138,8 @@ static __global__ void __launch_bounds__(BEGIN_THREADS) batch_stage_begin_kernel
 }
 
 // face sweep along DIR over the face tiles of all live events
-template <int KIND, int DIR>
-__global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) batch_faces_kernel(FaceArgs base, BatchDev B, int nv) {
+template <int KIND, int DIR, int REC>
+__global__ void ECHO_FACE_BOUNDS(KIND) batch_faces_kernel(FaceArgs base, BatchDev B, int nv) {
   __shared__ FaceArgs sA;
   __shared__ double red[4];
   __shared__ int s_tile;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) batch_faces_ke
     }
     __syncthreads();
     size_t fid = (size_t)s_tile * BATCH_TILE + threadIdx.x;
-    double am = fid < faces_of<DIR>(sA.g) ? face_flux<KIND, DIR>(sA, fid) : 0.0;
+    double am = fid < faces_of<DIR>(sA.g) ? face_flux<KIND, DIR, REC>(sA, fid) : 0.0;
     block_max_atomic(am, &sA.sc->amax_bits[DIR], red);
     __syncthreads();  // sA, red and s_tile are rewritten for the next tile
   }
@@ -178,7 +178,7 @@ static __global__ void batch_scalars_kernel(ScalarArgs base, BatchDev B) {
 
 // cell update over the cell tiles of all live events
 template <int KIND, bool SEED>
-__global__ void __launch_bounds__(128) batch_update_kernel(UpdateArgs base, BatchDev B, int nv) {
+__global__ void ECHO_UPDATE_BOUNDS(KIND, SEED) batch_update_kernel(UpdateArgs base, BatchDev B, int nv) {
   __shared__ UpdateArgs sA;
   __shared__ int s_tile;
   const int* pre = B.prefix + PH_CELL * (B.nev + 1);

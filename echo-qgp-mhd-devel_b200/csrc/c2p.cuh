@@ -190,6 +190,14 @@ __device__ __forceinline__ int eos_energy_slope(const DevPhys& P, double rh, dou
     if (pr < __ldg(P.tp)) return 125;
     if (pr > __ldg(P.tp + P.nt - 1)) return 126;
     int h = SEARCH_P(P, pr);
+#ifndef ECHO_EXACT
+    if (P.sl_ep) {
+      double sl = __ldg(P.sl_ep + h - 2);
+      *dedp = sl;
+      *en = __ldg(P.te + h - 2) + (pr - __ldg(P.tp + h - 2)) * sl;
+      return 0;
+    }
+#endif
     double p2 = __ldg(P.tp + h - 1), p1 = __ldg(P.tp + h - 2);
     double e2 = __ldg(P.te + h - 1), e1 = __ldg(P.te + h - 2);
     *dedp = (e2 - e1) / (p2 - p1);

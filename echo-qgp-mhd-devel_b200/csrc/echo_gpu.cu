@@ -84,12 +84,21 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
   *d_tab = nullptr;
   int nt = 0;
   if (eos_table && n_eos > 0) {
+    // columns T, e, p, c_s^2, then the interval slopes de/dp, d(c_s^2)/de
+    // and dp/de = (dp/dT)/(de/dT) (get_pressure's derivative, eos.f90:458-462)
     nt = n_eos;
-    std::vector<double> cols((size_t)4 * n_eos);
+    std::vector<double> cols((size_t)7 * n_eos, 0.0);
     for (int i = 0; i < n_eos; i++)
       for (int q = 0; q < 4; q++) cols[(size_t)q * n_eos + i] = eos_table[4 * i + q];
-    CK(cudaMalloc(d_tab, sizeof(double) * 4 * n_eos));
-    CK(cudaMemcpy(*d_tab, cols.data(), sizeof(double) * 4 * n_eos, cudaMemcpyHostToDevice));
+    for (int i = 0; i + 1 < n_eos; i++) {
+      const double* a = eos_table + 4 * i;
+      const double* b = a + 4;
+      cols[(size_t)4 * n_eos + i] = (b[1] - a[1]) / (b[2] - a[2]);
+      cols[(size_t)5 * n_eos + i] = (b[3] - a[3]) / (b[1] - a[1]);
+      cols[(size_t)6 * n_eos + i] = ((b[2] - a[2]) / (b[0] - a[0])) / ((b[1] - a[1]) / (b[0] - a[0]));
+    }
+    CK(cudaMalloc(d_tab, sizeof(double) * 7 * n_eos));
+    CK(cudaMemcpy(*d_tab, cols.data(), sizeof(double) * 7 * n_eos, cudaMemcpyHostToDevice));
   }
   P->eqstate = p->eqstate;
   P->coordinates = p->coordinates;
@@ -109,6 +118,7 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
   P->przero = p->przero;
   P->glm_alpha = p->glm_alpha;
   P->bke = P->bkp = nullptr;
+  P->sl_ep = P->sl_ce = P->sl_pe = nullptr;
   *d_bk = nullptr;
   if (nt > 0) {
     std::vector<double> te(nt), tp(nt);
@@ -128,6 +138,10 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
       P->bkp0 = kp0;
       P->nbke = (int)be.size();
       P->nbkp = (int)bp.size();
+      // strictly increasing e and p: every interval has a finite slope
+      P->sl_ep = *d_tab + 4 * nt;
+      P->sl_ce = *d_tab + 5 * nt;
+      P->sl_pe = *d_tab + 6 * nt;
     }
   }
   return ECHO_OK;

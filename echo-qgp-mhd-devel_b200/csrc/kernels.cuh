@@ -98,6 +98,33 @@ __device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, 
   }
 }
 
+// The face and update kernels are latency-bound (long-scoreboard and
+// dependent FP64 stalls): more resident warps win over the spills a lower
+// register cap costs.  Measured on B200 (blocks of 128 per SM): faces 7
+// (ideal RMHD; 5 is 10 % slower) and 5 (viscous; 3 is 15 % slower); update
+// 7 (ideal RMHD, from 4 uncapped), 5 (viscous, from 2) and 4 with the
+// learned seed (from 2: 0.83 vs 1.17 ms per step).
+#ifndef ECHO_FACE_MINB
+#define ECHO_FACE_MINB 7
+#endif
+#ifndef ECHO_FACE_MINB_VISC
+#define ECHO_FACE_MINB_VISC 5
+#endif
+#define ECHO_FACE_BOUNDS(KIND) __launch_bounds__(128, (KIND) == KIND_VISC ? ECHO_FACE_MINB_VISC : ECHO_FACE_MINB)
+#ifndef ECHO_UPDATE_MINB
+#define ECHO_UPDATE_MINB 7
+#endif
+#ifndef ECHO_UPDATE_MINB_VISC
+#define ECHO_UPDATE_MINB_VISC 5
+#endif
+#ifndef ECHO_UPDATE_MINB_SEED
+#define ECHO_UPDATE_MINB_SEED 4
+#endif
+#define ECHO_UPDATE_BOUNDS(KIND, SEED)                                       \
+  __launch_bounds__(128, (SEED)                 ? ECHO_UPDATE_MINB_SEED   \
+                         : (KIND) == KIND_VISC ? ECHO_UPDATE_MINB_VISC   \
+                                               : ECHO_UPDATE_MINB)
+
 struct FaceArgs {
   DevPhys P;
   Grid g;
@@ -124,7 +151,7 @@ __host__ __device__ __forceinline__ size_t faces_of(const Grid& g) {
 
 // The flux through face `fid` (< faces_of<DIR>(A.g)): writes A.F (and A.WD)
 // and returns the face's signal speed max(a+, a-) for the CFL reduction.
-template <int KIND, int DIR>
+template <int KIND, int DIR, int REC>
 __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
@@ -181,7 +208,7 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
           for (int q = 0; q < 6; q++) s[q] = sg[q] * s[q];
         }
         w0[k] = s[2];
-        recon_face(A.P.recal, s, wl[k], wr[k]);
+        recon_face<REC>(A.P.recal, s, wl[k], wr[k]);
       }
     } else {
 #pragma unroll
@@ -191,7 +218,7 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
 #pragma unroll
         for (int q = 0; q < 6; q++) s[q] = ghost_val(vk, base, stride, n, i - 2 + q, A.bc.c[k][0], A.bc.c[k][1]);
         w0[k] = s[2];
-        recon_face(A.P.recal, s, wl[k], wr[k]);
+        recon_face<REC>(A.P.recal, s, wl[k], wr[k]);
       }
     }
     // u^mu reconstruction for the viscous derivatives (work_rec(n,1,4,1))
@@ -212,7 +239,7 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
 #pragma unroll
       for (int c = 0; c < 4; c++) {
         double l, r;
-        recon_face(A.P.recal, s[c], l, r);
+        recon_face<REC>(A.P.recal, s[c], l, r);
         A.WD[(size_t)c * nfaces + fid] = l;
         A.WD[(size_t)(4 + c) * nfaces + fid] = r;
       }
@@ -321,11 +348,11 @@ __device__ __forceinline__ void block_max_atomic(double m, unsigned long long* d
   }
 }
 
-template <int KIND, int DIR>
-__global__ void __launch_bounds__(128, KIND == KIND_VISC ? 3 : 5) faces_kernel(FaceArgs A) {
+template <int KIND, int DIR, int REC>
+__global__ void ECHO_FACE_BOUNDS(KIND) faces_kernel(FaceArgs A) {
   __shared__ double red[4];
   size_t fid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  double amax_local = fid < faces_of<DIR>(A.g) ? face_flux<KIND, DIR>(A, fid) : 0.0;
+  double amax_local = fid < faces_of<DIR>(A.g) ? face_flux<KIND, DIR, REC>(A, fid) : 0.0;
   block_max_atomic(amax_local, &A.sc->amax_bits[DIR], red);
 }
 
@@ -614,7 +641,7 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
 }
 
 template <int KIND, bool SEED>
-__global__ void __launch_bounds__(128) update_kernel(UpdateArgs A) {
+__global__ void ECHO_UPDATE_BOUNDS(KIND, SEED) update_kernel(UpdateArgs A) {
   size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   update_cell<KIND, SEED>(A, c, c < A.g.ncell);
 }

@@ -23,9 +23,15 @@ void launch_faces(EchoCtx* c, int dir) {
   A.sc = c->d_sc;
   A.coordinates = c->p.coordinates;
   unsigned blocks = (unsigned)((c->nfaces[dir] + 127) / 128);
-  if (dir == 0) faces_kernel<KIND, 0><<<blocks, 128, 0, c->stream>>>(A);
-  if (dir == 1) faces_kernel<KIND, 1><<<blocks, 128, 0, c->stream>>>(A);
-  if (dir == 2) faces_kernel<KIND, 2><<<blocks, 128, 0, c->stream>>>(A);
+  if (c->p.recal == ECHO_REC_WENO5) {
+    if (dir == 0) faces_kernel<KIND, 0, ECHO_REC_WENO5><<<blocks, 128, 0, c->stream>>>(A);
+    if (dir == 1) faces_kernel<KIND, 1, ECHO_REC_WENO5><<<blocks, 128, 0, c->stream>>>(A);
+    if (dir == 2) faces_kernel<KIND, 2, ECHO_REC_WENO5><<<blocks, 128, 0, c->stream>>>(A);
+  } else {
+    if (dir == 0) faces_kernel<KIND, 0, REC_RUNTIME><<<blocks, 128, 0, c->stream>>>(A);
+    if (dir == 1) faces_kernel<KIND, 1, REC_RUNTIME><<<blocks, 128, 0, c->stream>>>(A);
+    if (dir == 2) faces_kernel<KIND, 2, REC_RUNTIME><<<blocks, 128, 0, c->stream>>>(A);
+  }
 }
 
 template <int KIND>
@@ -160,9 +166,15 @@ void launch_batch_faces(EchoBatch* b, int dir) {
   A.coordinates = b->p.coordinates;
   BatchDev B = batch_dev(b);
   unsigned grid = batch_grid(b, SL_FX + dir, PH_FX + dir);
-  if (dir == 0) batch_faces_kernel<KIND, 0><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
-  if (dir == 1) batch_faces_kernel<KIND, 1><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
-  if (dir == 2) batch_faces_kernel<KIND, 2><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+  if (b->p.recal == ECHO_REC_WENO5) {
+    if (dir == 0) batch_faces_kernel<KIND, 0, ECHO_REC_WENO5><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+    if (dir == 1) batch_faces_kernel<KIND, 1, ECHO_REC_WENO5><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+    if (dir == 2) batch_faces_kernel<KIND, 2, ECHO_REC_WENO5><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+  } else {
+    if (dir == 0) batch_faces_kernel<KIND, 0, REC_RUNTIME><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+    if (dir == 1) batch_faces_kernel<KIND, 1, REC_RUNTIME><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+    if (dir == 2) batch_faces_kernel<KIND, 2, REC_RUNTIME><<<grid, 128, 0, b->stream>>>(A, B, b->nv);
+  }
 }
 
 template <int KIND>
@@ -242,9 +254,15 @@ void launch_batch_p2c(EchoBatch* b) {
 template <int KIND>
 void batch_occupancy(const EchoBatch* b, int* per_sm) {
   (void)b;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FX], batch_faces_kernel<KIND, 0>, 128, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FY], batch_faces_kernel<KIND, 1>, 128, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FZ], batch_faces_kernel<KIND, 2>, 128, 0);
+  if (b->p.recal == ECHO_REC_WENO5) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FX], batch_faces_kernel<KIND, 0, ECHO_REC_WENO5>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FY], batch_faces_kernel<KIND, 1, ECHO_REC_WENO5>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FZ], batch_faces_kernel<KIND, 2, ECHO_REC_WENO5>, 128, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FX], batch_faces_kernel<KIND, 0, REC_RUNTIME>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FY], batch_faces_kernel<KIND, 1, REC_RUNTIME>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FZ], batch_faces_kernel<KIND, 2, REC_RUNTIME>, 128, 0);
+  }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_UPDATE], batch_update_kernel<KIND, false>, 128, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_SMOOTH], batch_smooth_kernel<KIND>, 128, 0);
 }

@@ -67,12 +67,6 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
   return *reinterpret_cast<unsigned*>(&h);
 }
 
-__device__ __forceinline__ float tanh_fast(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
 __device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
   asm volatile(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -81,101 +75,98 @@ __device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsign
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// tanh of two FP32 accumulators, packed as the BF16 pair the next layer's A
+// fragment takes: one conversion and one packed tanh
+__device__ __forceinline__ unsigned tanh_pack_bf16(float lo, float hi) {
+  unsigned p = pack_bf16(lo, hi), y;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(y) : "r"(p));
+  return y;
+}
+
 // Seed for the calling lane's cell.  Must be called by all 32 lanes of the
 // warp together (inactive lanes pass any finite features).  f: raw
-// invariants; out: (x, q) de-standardised.
+// invariants; out: (x, q) de-standardised.  The warp's 32 cells are two
+// m-tiles of 16 rows, run one after the other so that only one tile's
+// accumulators (32 registers) and A fragments (16) are live.
 __device__ __forceinline__ void mlp_warp(const MlpDev& M, const float f[5], float out[2]) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   float fs[5];
 #pragma unroll
   for (int j = 0; j < 5; j++) fs[j] = (f[j] - __ldg(M.par + MLP_FMEAN + j)) / __ldg(M.par + MLP_FSTD + j);
-  // layer-0 A fragments (16 input columns, 5 used) for both m-tiles
-  unsigned A[2][4][4];  // [m-tile][k-tile][reg]
-#pragma unroll
-  for (int mt = 0; mt < 2; mt++) {
-    float lo[5], hi[5];
-#pragma unroll
-    for (int j = 0; j < 5; j++) {
-      lo[j] = __shfl_sync(full, fs[j], mt * 16 + g);
-      hi[j] = __shfl_sync(full, fs[j], mt * 16 + g + 8);
-    }
-    // columns 2t and 2t+1
-    float l0 = t == 0 ? lo[0] : t == 1 ? lo[2] : t == 2 ? lo[4] : 0.f;
-    float l1 = t == 0 ? lo[1] : t == 1 ? lo[3] : 0.f;
-    float h0 = t == 0 ? hi[0] : t == 1 ? hi[2] : t == 2 ? hi[4] : 0.f;
-    float h1 = t == 0 ? hi[1] : t == 1 ? hi[3] : 0.f;
-    A[mt][0][0] = pack_bf16(l0, l1);
-    A[mt][0][1] = pack_bf16(h0, h1);
-    A[mt][0][2] = 0u;
-    A[mt][0][3] = 0u;
-  }
-  float C[2][8][4];
-  // hidden layers 0..3
-#pragma unroll
-  for (int layer = 0; layer < 4; layer++) {
-    const int nk = layer == 0 ? 1 : 4;
-    const unsigned* W = M.frag + (layer == 0 ? MLP_FRAG_L0 : MLP_FRAG_L1 + (layer - 1) * (4 * 8 * 64));
-    const float* b = M.par + MLP_B0 + layer * 64;
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      float b0 = __ldg(b + nt * 8 + 2 * t), b1 = __ldg(b + nt * 8 + 2 * t + 1);
-#pragma unroll
-      for (int mt = 0; mt < 2; mt++) {
-        C[mt][nt][0] = b0;
-        C[mt][nt][1] = b1;
-        C[mt][nt][2] = b0;
-        C[mt][nt][3] = b1;
-      }
-    }
-#pragma unroll
-    for (int kt = 0; kt < 4; kt++) {
-      if (kt >= nk) break;
-#pragma unroll
-      for (int nt = 0; nt < 8; nt++) {
-        const uint2 w = __ldg(reinterpret_cast<const uint2*>(W) + (kt * 8 + nt) * 32 + lane);
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++) mma_bf16(C[mt][nt], A[mt][kt], w.x, w.y);
-      }
-    }
-    // tanh, then the accumulators become the next layer's A fragments
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-      for (int kt = 0; kt < 4; kt++) {
-        const float* c0 = C[mt][2 * kt];
-        const float* c1 = C[mt][2 * kt + 1];
-        A[mt][kt][0] = pack_bf16(tanh_fast(c0[0]), tanh_fast(c0[1]));
-        A[mt][kt][1] = pack_bf16(tanh_fast(c0[2]), tanh_fast(c0[3]));
-        A[mt][kt][2] = pack_bf16(tanh_fast(c1[0]), tanh_fast(c1[1]));
-        A[mt][kt][3] = pack_bf16(tanh_fast(c1[2]), tanh_fast(c1[3]));
-      }
-  }
-  // output layer: 64 -> 8 (two used), linear
-  float O[2][4];
-  {
-    float b0 = __ldg(M.par + MLP_B4 + 2 * t), b1 = __ldg(M.par + MLP_B4 + 2 * t + 1);
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-      O[mt][0] = b0;
-      O[mt][1] = b1;
-      O[mt][2] = b0;
-      O[mt][3] = b1;
-    }
-#pragma unroll
-    for (int kt = 0; kt < 4; kt++) {
-      const uint2 w = __ldg(reinterpret_cast<const uint2*>(M.frag + MLP_FRAG_L4) + kt * 32 + lane);
-#pragma unroll
-      for (int mt = 0; mt < 2; mt++) mma_bf16(O[mt], A[mt][kt], w.x, w.y);
-    }
-  }
   // row r = mt*16 + h*8 + g' of the output sits in lane g'*4 (t = 0), element 2h / 2h+1
   const int mt_me = lane >> 4, h_me = (lane >> 3) & 1, src = (lane & 7) * 4;
   float y0 = 0.f, y1 = 0.f;
-#pragma unroll
+#pragma unroll 1
   for (int mt = 0; mt < 2; mt++) {
-    float a0 = __shfl_sync(full, O[mt][0], src), a1 = __shfl_sync(full, O[mt][1], src);
-    float a2 = __shfl_sync(full, O[mt][2], src), a3 = __shfl_sync(full, O[mt][3], src);
+    // layer-0 A fragment (16 input columns, 5 used): rows g and g + 8 of this tile
+    unsigned A[4][4];  // [k-tile][reg]
+    {
+      float lo[5], hi[5];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        lo[j] = __shfl_sync(full, fs[j], mt * 16 + g);
+        hi[j] = __shfl_sync(full, fs[j], mt * 16 + g + 8);
+      }
+      // columns 2t and 2t+1
+      float l0 = t == 0 ? lo[0] : t == 1 ? lo[2] : t == 2 ? lo[4] : 0.f;
+      float l1 = t == 0 ? lo[1] : t == 1 ? lo[3] : 0.f;
+      float h0 = t == 0 ? hi[0] : t == 1 ? hi[2] : t == 2 ? hi[4] : 0.f;
+      float h1 = t == 0 ? hi[1] : t == 1 ? hi[3] : 0.f;
+      A[0][0] = pack_bf16(l0, l1);
+      A[0][1] = pack_bf16(h0, h1);
+      A[0][2] = 0u;
+      A[0][3] = 0u;
+    }
+    // hidden layers 0..3
+#pragma unroll
+    for (int layer = 0; layer < 4; layer++) {
+      const int nk = layer == 0 ? 1 : 4;
+      const unsigned* W = M.frag + (layer == 0 ? MLP_FRAG_L0 : MLP_FRAG_L1 + (layer - 1) * (4 * 8 * 64));
+      const float* b = M.par + MLP_B0 + layer * 64;
+      float C[8][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        float b0 = __ldg(b + nt * 8 + 2 * t), b1 = __ldg(b + nt * 8 + 2 * t + 1);
+        C[nt][0] = b0;
+        C[nt][1] = b1;
+        C[nt][2] = b0;
+        C[nt][3] = b1;
+      }
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        if (kt >= nk) break;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+          const uint2 w = __ldg(reinterpret_cast<const uint2*>(W) + (kt * 8 + nt) * 32 + lane);
+          mma_bf16(C[nt], A[kt], w.x, w.y);
+        }
+      }
+      // tanh; the accumulators become the next layer's A fragments
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        A[kt][0] = tanh_pack_bf16(C[2 * kt][0], C[2 * kt][1]);
+        A[kt][1] = tanh_pack_bf16(C[2 * kt][2], C[2 * kt][3]);
+        A[kt][2] = tanh_pack_bf16(C[2 * kt + 1][0], C[2 * kt + 1][1]);
+        A[kt][3] = tanh_pack_bf16(C[2 * kt + 1][2], C[2 * kt + 1][3]);
+      }
+    }
+    // output layer: 64 -> 8 (two used), linear
+    float O[4];
+    {
+      float b0 = __ldg(M.par + MLP_B4 + 2 * t), b1 = __ldg(M.par + MLP_B4 + 2 * t + 1);
+      O[0] = b0;
+      O[1] = b1;
+      O[2] = b0;
+      O[3] = b1;
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        const uint2 w = __ldg(reinterpret_cast<const uint2*>(M.frag + MLP_FRAG_L4) + kt * 32 + lane);
+        mma_bf16(O, A[kt], w.x, w.y);
+      }
+    }
+    float a0 = __shfl_sync(full, O[0], src), a1 = __shfl_sync(full, O[1], src);
+    float a2 = __shfl_sync(full, O[2], src), a3 = __shfl_sync(full, O[3], src);
     if (mt == mt_me) {
       y0 = h_me ? a2 : a0;
       y1 = h_me ? a3 : a1;

@@ -147,6 +147,7 @@ extern "C" int echo_gpu_rhs_noalloc(const EchoParams* p, const double* d_eos_col
     c.P.tc = d_eos_cols + 3 * n_eos;
   }
   c.P.bke = c.P.bkp = nullptr;  // plain bracket search: same brackets, no accelerator table
+  c.P.sl_ep = c.P.sl_ce = c.P.sl_pe = nullptr;  // interpolation with divisions
   c.P.maxspeed = p->maxspeed;
   c.P.eta_over_s = p->eta_over_s;
   c.P.tau_pi_coeff = p->tau_pi_coeff;

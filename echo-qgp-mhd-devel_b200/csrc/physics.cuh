@@ -64,12 +64,17 @@ struct DevPhys {
   const int* __restrict__ bkp;
   long long bke0, bkp0;
   int nbke, nbkp;
+  // product build: slopes of every table interval, de/dp, d(c_s^2)/de and
+  // dp/de (null: interpolate with divisions, as the reference does)
+  const double* __restrict__ sl_ep;
+  const double* __restrict__ sl_ce;
+  const double* __restrict__ sl_pe;
   double maxspeed, eta_over_s, tau_pi_coeff, enezero, przero, glm_alpha;
 };
 
 // metric (system_metric_*, system.f90:132-160), derived from t on device
 struct Metric {
-  double g1, g2, g3, gp, gm, g0, t, t3;
+  double g1, g2, g3, gp, gm, g0, t, t3, ig3;
 };
 
 __device__ __forceinline__ Metric make_metric(int coordinates, double t, double t3) {
@@ -88,7 +93,25 @@ __device__ __forceinline__ Metric make_metric(int coordinates, double t, double 
     m.gp = 1.;
     m.gm = 1.;
   }
+  m.ig3 = 1. / m.g3;
   return m;
+}
+
+// x / g3 and x / gp as the reference writes them; the product build
+// multiplies by the reciprocals, computed once per thread
+__device__ __forceinline__ double over_g3(const Metric& M, double x) {
+#ifdef ECHO_EXACT
+  return x / M.g3;
+#else
+  return x * M.ig3;
+#endif
+}
+__device__ __forceinline__ double over_gp(const Metric& M, double x) {
+#ifdef ECHO_EXACT
+  return x / M.gp;
+#else
+  return x * M.gm;
+#endif
 }
 
 // ---------------------------------------------------------------------------
@@ -134,6 +157,12 @@ __device__ __forceinline__ int eos_energy(const DevPhys& P, double rh, double* e
     if (pr < __ldg(P.tp)) return 125;
     if (pr > __ldg(P.tp + P.nt - 1)) return 126;
     int h = SEARCH_P(P, pr);
+#ifndef ECHO_EXACT
+    if (P.sl_ep) {
+      *en = __ldg(P.te + h - 2) + (pr - __ldg(P.tp + h - 2)) * __ldg(P.sl_ep + h - 2);
+      return 0;
+    }
+#endif
     double p2 = __ldg(P.tp + h - 1), p1 = __ldg(P.tp + h - 2);
     double e2 = __ldg(P.te + h - 1), e1 = __ldg(P.te + h - 2);
     *en = e1 + (e2 - e1) * (pr - p1) / (p2 - p1);
@@ -157,6 +186,15 @@ __device__ __forceinline__ int eos_pressure(const DevPhys& P, double rh, double 
     if (en < __ldg(P.te)) return 123;
     if (en > __ldg(P.te + P.nt - 1)) return 124;
     int h = SEARCH_E(P, en);
+#ifndef ECHO_EXACT
+    if (P.sl_pe) {  // dp/de = (dp/dT)/(de/dT) of the interval, precomputed
+      double sl = __ldg(P.sl_pe + h - 2);
+      *pr = __ldg(P.tp + h - 2) + (en - __ldg(P.te + h - 2)) * sl;
+      *dprdrh = 0;
+      *dprden = sl;
+      return 0;
+    }
+#endif
     double p2 = __ldg(P.tp + h - 1), p1 = __ldg(P.tp + h - 2);
     double e2 = __ldg(P.te + h - 1), e1 = __ldg(P.te + h - 2);
     double t2 = __ldg(P.tT + h - 1), t1 = __ldg(P.tT + h - 2);
@@ -181,12 +219,43 @@ __device__ __forceinline__ int eos_pressure(const DevPhys& P, double rh, double 
   return 0;
 }
 
+#ifndef ECHO_EXACT
+// Product build, the face states of system_flux: e(p) interpolated in the p
+// interval of the bracket h (returned for eos_sound_at), with the interval's
+// precomputed slope instead of a division.  h = 0 when the EoS is not a
+// table with slopes (then eos_energy / eos_sound are used).
+__device__ __forceinline__ int eos_energy_h(const DevPhys& P, double rh, double* en, double pr, int* h) {
+  if (P.eqstate == ECHO_EOS_TABLE && P.sl_ep) {
+    if (pr < __ldg(P.tp)) return 125;
+    if (pr > __ldg(P.tp + P.nt - 1)) return 126;
+    int hh = SEARCH_P(P, pr);
+    *en = __ldg(P.te + hh - 2) + (pr - __ldg(P.tp + hh - 2)) * __ldg(P.sl_ep + hh - 2);
+    *h = hh;
+    return 0;
+  }
+  *h = 0;
+  return eos_energy(P, rh, en, pr);
+}
+// c_s^2(e) for the e just interpolated in bracket h: e lies in the same
+// interval of the e column (e(p) is monotonic; at a node both neighbouring
+// intervals give the node value), so get_sound's search is skipped
+__device__ __forceinline__ double eos_sound_at(const DevPhys& P, int h, double en) {
+  return __ldg(P.tc + h - 2) + (en - __ldg(P.te + h - 2)) * __ldg(P.sl_ce + h - 2);
+}
+#endif
+
 // eos_sound: get_sound (eos.f90:590-641) / eos_sound_ana (eos.f90:926-952)
 __device__ __forceinline__ int eos_sound(const DevPhys& P, double rh, double en, double pr, double* cs2) {
   if (P.eqstate == ECHO_EOS_TABLE) {
     if (en < __ldg(P.te)) return 131;
     if (en > __ldg(P.te + P.nt - 1)) return 132;
     int h = SEARCH_E(P, en);
+#ifndef ECHO_EXACT
+    if (P.sl_ce) {
+      *cs2 = __ldg(P.tc + h - 2) + (en - __ldg(P.te + h - 2)) * __ldg(P.sl_ce + h - 2);
+      return 0;
+    }
+#endif
     double s2 = __ldg(P.tc + h - 1), s1 = __ldg(P.tc + h - 2);
     double e2 = __ldg(P.te + h - 1), e1 = __ldg(P.te + h - 2);
     *cs2 = s1 + (s2 - s1) * (en - e1) / (e2 - e1);
@@ -307,9 +376,12 @@ __device__ __forceinline__ double mp5(double f, double f1, double f2, double f3,
 #ifndef ECHO_EXACT
 // Product build: the same weights with the common denominator multiplied
 // through, sum_k d_k p_k / q_k^2 / sum_k d_k / q_k^2 =
-// sum_k d_k p_k Q_j Q_l / sum_k d_k Q_j Q_l with Q = q^2: one division
-// instead of four.  Q >= 1e-12, so the products cannot underflow.
-__device__ __forceinline__ double weno5_side(double f1, double f2, double f3, double f4, double f5) {
+// sum_k d_k p_k Q_j Q_l / sum_k d_k Q_j Q_l with Q = q^2 (Q >= 1e-12, so
+// the products cannot underflow), and the two sides of a face sharing one
+// division: gl = nl/dl, gr = nr/dr = (nl dr, nr dl) / (dl dr), where
+// dl, dr >= 3e-24 and stay far below 1e150 for the values a run holds.
+__device__ __forceinline__ void weno5_nd(double f1, double f2, double f3, double f4, double f5, double& num,
+                                         double& den) {
   const double eps = 1.e-6, r12 = 1. / 12.;
   double t1, t2, q1, q2, q3;
   t1 = f3 - 2 * f2 + f1;
@@ -326,7 +398,16 @@ __device__ __forceinline__ double weno5_side(double f1, double f2, double f3, do
   double p1 = (3. * f1 - 10. * f2 + 15. * f3) * 0.125;
   double p2 = (-f2 + 6. * f3 + 3. * f4) * 0.125;
   double p3 = (3. * f3 + 6. * f4 - f5) * 0.125;
-  return (w1 * p1 + w2 * p2 + w3 * p3) / (w1 + w2 + w3);
+  num = w1 * p1 + w2 * p2 + w3 * p3;
+  den = w1 + w2 + w3;
+}
+__device__ __forceinline__ void weno5_face(const double s[6], double& gl, double& gr) {
+  double nl, dl, nr, dr;
+  weno5_nd(s[0], s[1], s[2], s[3], s[4], nl, dl);
+  weno5_nd(s[5], s[4], s[3], s[2], s[1], nr, dr);
+  double inv = 1. / (dl * dr);
+  gl = nl * dr * inv;
+  gr = nr * dl * inv;
 }
 #else
 __device__ __forceinline__ double weno5_side(double f1, double f2, double f3, double f4, double f5) {
@@ -386,7 +467,7 @@ __device__ __forceinline__ double ppm4_side(double f1, double f2, double f3, dou
 
 // Left and right states at face i+1/2 from the 6-point stencil
 // s[0..5] = f(i-2..i+3) (work_rec, work.f90:420-525).
-__device__ __forceinline__ void recon_face(int recal, const double s[6], double& gl, double& gr) {
+__device__ __forceinline__ void recon_any(int recal, const double s[6], double& gl, double& gr) {
   switch (recal) {
     case ECHO_REC_TVD2: {  // holib.f90:47-77, rewritten per face
       gl = s[2] + .5 * mm2(s[2] - s[1], s[3] - s[2]);
@@ -402,8 +483,12 @@ __device__ __forceinline__ void recon_face(int recal, const double s[6], double&
       gr = weno3_side(s[4], s[3], s[2]);
       break;
     case ECHO_REC_WENO5:
+#ifdef ECHO_EXACT
       gl = weno5_side(s[0], s[1], s[2], s[3], s[4]);
       gr = weno5_side(s[5], s[4], s[3], s[2], s[1]);
+#else
+      weno5_face(s, gl, gr);
+#endif
       break;
     case ECHO_REC_PPM4:
       gl = ppm4_side(s[1], s[2], s[3], s[4]);
@@ -426,6 +511,17 @@ __device__ __forceinline__ void recon_face(int recal, const double s[6], double&
       break;
     }
   }
+}
+
+// The reconstruction fixed at compile time (REC = ECHO_REC_*) or chosen at
+// run time (REC = REC_RUNTIME).  The face kernels reconstruct every
+// variable with an unrolled loop; a run-time switch inside it puts all seven
+// schemes into the kernel once per variable, so the common scheme gets a
+// kernel of its own.
+enum { REC_RUNTIME = -1 };
+template <int REC>
+__device__ __forceinline__ void recon_face(int recal, const double s[6], double& gl, double& gr) {
+  recon_any(REC >= 0 ? REC : recal, s, gl, gr);
 }
 
 // ---------------------------------------------------------------------------
@@ -511,7 +607,7 @@ __device__ __forceinline__ void e_ideal(const Metric& M, double vx, double vy, d
 }
 __device__ __forceinline__ void exb(const Metric& M, const double E[3], double bx, double by, double bz,
                                     double o[3]) {
-  double e0 = E[0], e1 = E[1], e2 = E[2] / M.g3, gp = M.gp;
+  double e0 = E[0], e1 = E[1], e2 = over_g3(M, E[2]), gp = M.gp;
   o[0] = gp * (e1 * bz - e2 * by);
   o[1] = gp * (e2 * bx - e0 * bz);
   o[2] = gp * (e0 * by - e1 * bx);
@@ -587,18 +683,27 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
   double g1 = M.g1, g2 = M.g2, g3 = M.g3, gp = M.gp, gm = M.gm;
   double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
   double en = 0;
+#ifdef ECHO_EXACT
   int err = eos_energy(P, rh, &en, pr);
+#else
+  int hb = 0;
+  int err = eos_energy_h(P, rh, &en, pr, &hb);
+#endif
   if (err) return err;
   double v2 = g1 * vx * vx + g2 * vy * vy + g3 * vz * vz;
   if (v2 > 1) return 333;
+#ifdef ECHO_EXACT
   double glf = 1. / sqrt(1. - v2);
+#else
+  double glf = rsqrt(1. - v2);
+#endif
   double w, E[3] = {0, 0, 0}, EXB[3] = {0, 0, 0}, E2 = 0, B2 = 0, EEM = 0;
   Pit pi = {0, 0, 0, 0, 0};
   if (!T::VISC) {
     w = en + pr;
     if (T::MHD) {
       e_ideal(M, vx, vy, vz, v[KBX], v[KBY], v[KBZ], E);
-      E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
+      E2 = E[0] * E[0] + E[1] * E[1] + over_g3(M, E[2] * E[2]);
       exb(M, E, v[KBX], v[KBY], v[KBZ], EXB);
       B2 = v[KBX] * v[KBX] + v[KBY] * v[KBY] + (v[KBZ] * v[KBZ]) * g3;
       EEM = 0.5 * (E2 + B2);
@@ -624,7 +729,7 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
     u[KBX] = v[KBX];
     u[KBY] = v[KBY];
     u[KBZ] = v[KBZ];
-    if (T::GLM) u[KGLM] = v[KGLM] / gp;
+    if (T::GLM) u[KGLM] = over_gp(M, v[KGLM]);
   } else {
     u[KVX] = ww * vx;
     u[KVY] = ww * vy;
@@ -654,7 +759,7 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
       f[KBZ] = +E[1] * gm;
       if (T::GLM) {
         f[KBX] = v[KGLM];
-        f[KGLM] = v[KBX] / gp;
+        f[KGLM] = over_gp(M, v[KBX]);
       }
     } else {
       f[KVX] = wwdir * vx * g1 + pr;
@@ -684,7 +789,7 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
       f[KBZ] = -E[0] * gm;
       if (T::GLM) {
         f[KBY] = v[KGLM];
-        f[KGLM] = v[KBY] / gp;
+        f[KGLM] = over_gp(M, v[KBY]);
       }
     } else {
       f[KVX] = wwdir * vx * g1;
@@ -705,16 +810,16 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
 #pragma unroll
       for (int k = 5; k < NV; k++) f[k] = u[k] * vz;
     } else if (T::MHD) {
-      f[KVX] = wwdir * vx - E[2] / g3 * E[0] - v[KBZ] * v[KBX];
-      f[KVY] = wwdir * vy - E[2] / g3 * E[1] - v[KBZ] * v[KBY];
-      f[KVZ] = wwdir * vz * g3 - (E[2] * E[2]) / g3 - (v[KBZ] * v[KBZ]) * g3 + pr + EEM;
-      f[KPR] = wwdir + EXB[2] / g3;
+      f[KVX] = wwdir * vx - over_g3(M, E[2]) * E[0] - v[KBZ] * v[KBX];
+      f[KVY] = wwdir * vy - over_g3(M, E[2]) * E[1] - v[KBZ] * v[KBY];
+      f[KVZ] = wwdir * vz * g3 - over_g3(M, E[2] * E[2]) - (v[KBZ] * v[KBZ]) * g3 + pr + EEM;
+      f[KPR] = wwdir + over_g3(M, EXB[2]);
       f[KBX] = -E[1] * gm;
       f[KBY] = E[0] * gm;
       f[KBZ] = 0.;
       if (T::GLM) {
-        f[KBZ] = v[KGLM] / g3;
-        f[KGLM] = v[KBZ] / gp;
+        f[KBZ] = over_g3(M, v[KGLM]);
+        f[KGLM] = over_gp(M, v[KBZ]);
       }
     } else {
       f[KVX] = wwdir * vx * g1;
@@ -735,12 +840,22 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
     ca2 = 0.;
   }
   double cs2 = 0;
+#ifdef ECHO_EXACT
   err = eos_sound(P, rh, en, pr, &cs2);
+#else
+  if (hb)
+    cs2 = eos_sound_at(P, hb, en);
+  else
+    err = eos_sound(P, rh, en, pr, &cs2);
+#endif
   if (err) return err;
   double a2 = cs2 + ca2 - cs2 * ca2;
   double den = 1. / (1. - v2 * a2);
   double vf1 = den * (1. - a2) * vdir;
-  double vf2 = den * sqrt(a2 * (1. - v2) * ((1. - v2 * a2) / gcov_dir - (1. - a2) * (vdir * vdir)));
+  // g_11 = g_22 = 1 in both metrics, so only the eta direction divides
+  double hdir = DIR == 3 ? over_g3(M, 1. - v2 * a2) : (1. - v2 * a2);
+  (void)gcov_dir;
+  double vf2 = den * sqrt(a2 * (1. - v2) * (hdir - (1. - a2) * (vdir * vdir)));
   vfp = vf1 + vf2;
   vfm = vf1 - vf2;
   return 0;

@@ -35,7 +35,7 @@ __global__ void recon_test_kernel(int recal, int m, int n, const double* f, doub
   double s[6];
   for (int q = 0; q < 6; q++) s[q] = fr[i - 2 + q];
   double l, r;
-  recon_face(recal, s, l, r);
+  recon_any(recal, s, l, r);
   gl[id] = l;
   gr[id] = r;
 }
