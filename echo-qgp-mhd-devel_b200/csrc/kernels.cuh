@@ -102,8 +102,8 @@ __device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, 
 // dependent FP64 stalls): more resident warps win over the spills a lower
 // register cap costs.  Measured on B200 (blocks of 128 per SM): faces 7
 // (ideal RMHD; 5 is 10 % slower) and 5 (viscous; 3 is 15 % slower); update
-// 7 (ideal RMHD, from 4 uncapped), 5 (viscous, from 2) and 4 with the
-// learned seed (from 2: 0.83 vs 1.17 ms per step).
+// 7 (ideal RMHD, from 4 uncapped), 5 (viscous, from 2) and 6 with the
+// learned seed (from 2: 0.74 vs 1.17 ms per step).
 #ifndef ECHO_FACE_MINB
 #define ECHO_FACE_MINB 7
 #endif
@@ -118,7 +118,7 @@ __device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, 
 #define ECHO_UPDATE_MINB_VISC 5
 #endif
 #ifndef ECHO_UPDATE_MINB_SEED
-#define ECHO_UPDATE_MINB_SEED 4
+#define ECHO_UPDATE_MINB_SEED 6
 #endif
 #define ECHO_UPDATE_BOUNDS(KIND, SEED)                                       \
   __launch_bounds__(128, (SEED)                 ? ECHO_UPDATE_MINB_SEED   \
@@ -137,6 +137,36 @@ struct FaceArgs {
   DevScalars* sc;
   int coordinates;
 };
+
+// The stencils and the reconstruction of every variable when the boundary
+// codes differ between variables or include extrapolation (code 3): a rare
+// configuration, kept out of line so that the common kernel body stays
+// small in the instruction cache.  Returns w0 (the cell left of the face),
+// the face states, and the velocity stencils sv for the viscous u^mu.
+template <int NV>
+struct ReconOut {
+  double w0[NV], wl[NV], wr[NV], sv[3][6];
+};
+template <int KIND, int REC>
+__device__ __noinline__ ReconOut<Traits<KIND>::NV> recon_general(const double* __restrict__ v, size_t ncell,
+                                                                  BcDir bc, int recal, size_t base,
+                                                                  long long stride, int n, int i) {
+  ReconOut<Traits<KIND>::NV> r;
+#pragma unroll 1
+  for (int k = 0; k < Traits<KIND>::NV; k++) {
+    const double* vk = v + (size_t)k * ncell;
+    double s[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) s[q] = ghost_val(vk, base, stride, n, i - 2 + q, bc.c[k][0], bc.c[k][1]);
+    r.w0[k] = s[2];
+    recon_face<REC>(recal, s, r.wl[k], r.wr[k]);
+    if (k >= KVX && k <= KVZ) {
+#pragma unroll
+      for (int q = 0; q < 6; q++) r.sv[k - KVX][q] = s[q];
+    }
+  }
+  return r;
+}
 
 // face index layout for DIR: (i fastest in x, then the other two)
 //   DIR 0: F[k][iz][iy][i],  i = 0..nx
@@ -187,6 +217,7 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
     }
     const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
     double wl[NV], wr[NV], w0[NV];
+    double sv[3][6];  // velocity stencils (ghosts filled), for the viscous u^mu
     // reconstruction of every variable (work_rec(n,1,nv,0))
     if (A.bc_uniform) {
       long long off[6];
@@ -209,27 +240,33 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
         }
         w0[k] = s[2];
         recon_face<REC>(A.P.recal, s, wl[k], wr[k]);
+        if (T::VISC && k >= KVX && k <= KVZ) {
+#pragma unroll
+          for (int q = 0; q < 6; q++) sv[k - KVX][q] = s[q];
+        }
       }
     } else {
+      ReconOut<NV> r = recon_general<KIND, REC>(A.v, g.ncell, A.bc, A.P.recal, base, stride, n, i);
 #pragma unroll
       for (int k = 0; k < NV; k++) {
-        const double* vk = A.v + (size_t)k * g.ncell;
-        double s[6];
+        w0[k] = r.w0[k];
+        wl[k] = r.wl[k];
+        wr[k] = r.wr[k];
+      }
+      if (T::VISC) {
 #pragma unroll
-        for (int q = 0; q < 6; q++) s[q] = ghost_val(vk, base, stride, n, i - 2 + q, A.bc.c[k][0], A.bc.c[k][1]);
-        w0[k] = s[2];
-        recon_face<REC>(A.P.recal, s, wl[k], wr[k]);
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int q = 0; q < 6; q++) sv[c][q] = r.sv[c][q];
       }
     }
-    // u^mu reconstruction for the viscous derivatives (work_rec(n,1,4,1))
+    // u^mu reconstruction for the viscous derivatives (work_rec(n,1,4,1)),
+    // from the same ghost-filled velocity stencils
     if (T::VISC) {
       double s[4][6];
 #pragma unroll
       for (int q = 0; q < 6; q++) {
-        int j = i - 2 + q;
-        double vx = ghost_val(A.v + (size_t)KVX * g.ncell, base, stride, n, j, A.bc.c[KVX][0], A.bc.c[KVX][1]);
-        double vy = ghost_val(A.v + (size_t)KVY * g.ncell, base, stride, n, j, A.bc.c[KVY][0], A.bc.c[KVY][1]);
-        double vz = ghost_val(A.v + (size_t)KVZ * g.ncell, base, stride, n, j, A.bc.c[KVZ][0], A.bc.c[KVZ][1]);
+        double vx = sv[0][q], vy = sv[1][q], vz = sv[2][q];
         double gg = 1. / sqrt(1. - vx * vx - vy * vy - M.g3 * (vz * vz));
         s[0][q] = gg;
         s[1][q] = gg * vx;
