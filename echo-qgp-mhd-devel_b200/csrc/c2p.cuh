@@ -13,6 +13,7 @@ namespace echo {
 // ---------------------------------------------------------------------------
 struct Sist3 {
   double B2, SB2, S2, U, D;
+  double iUB;  // 1 / (|U| + B2), the scale of the second residual
 };
 
 __device__ __forceinline__ double sist3_f(const DevPhys& P, const Sist3& s, const double* X, int K) {
@@ -230,11 +231,18 @@ static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, doubl
     double sq = sqrt(1. - xx);
     double rh = s.D * sq, en = 0, dedp = 0;
     if (eos_energy_slope(P, rh, pp, &en, &dedp)) return -1;
-    double ib = yy + s.B2, iy2 = 1.0 / (yy * yy), iy3 = iy2 / yy, i1x = 1.0 / (1. - xx);
+    double ib = yy + s.B2, iy2 = 1.0 / (yy * yy), i1x = 1.0 / (1. - xx);
     double F1 = ib * ib * xx - s.SB2 * iy2 * (2 * yy + s.B2) - s.S2;
     double F2 = yy - pp + 0.5 * (1. + xx) * s.B2 - 0.5 * s.SB2 * iy2 - s.U;
     double F3 = yy - (pp + en) * i1x;
+#ifdef ECHO_EXACT
+    double iy3 = iy2 / yy;
     double r = fmax(fabs(F1) / (ib * ib), fmax(fabs(F2) / (fabs(s.U) + s.B2), fabs(F3) / yy));
+#else
+    // 1/y = y * (1/y^2); the residual scales as reciprocals (one division)
+    double iy1 = yy * iy2, iy3 = iy2 * iy1;
+    double r = fmax(fabs(F1) / (ib * ib), fmax(fabs(F2) * s.iUB, fabs(F3) * iy1));
+#endif
     // d(en)/dx through rh is zero: the tabulated and conformal e(p) do not depend on rh
     double J11 = ib * ib, J12 = 2 * ib * xx + 2 * s.SB2 * (2 * yy + s.B2) * iy3 - 2 * s.SB2 * iy2, J13 = 0.;
     double J21 = 0.5 * s.B2, J22 = 1. + s.SB2 * iy3, J23 = -1.;
@@ -418,7 +426,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     X[0] = v2;
     X[1] = (en + pr) / (1 - v2);
     X[2] = pr;
-    Sist3 s = {B2, SB2, SS2, UU, DD};
+    Sist3 s = {B2, SB2, SS2, UU, DD, 1.0 / (fabs(UU) + B2)};
     int nfev = 0;
     if (algo == ECHO_C2P_NEWTON || algo == ECHO_C2P_MLP) {
       int it = -1, used = 0;
