@@ -81,6 +81,11 @@ static void enqueue_batch_stage(EchoBatch* b, int irk) {
 // one time step of every live event; vnewstep is taken by the first stage's
 // update (viscous), vold = vnewstep at the end is the role swap of vn
 static void enqueue_batch_step(EchoBatch* b) {
+  if (b->temp_end > 0.) {  // check_temp at the top of the time loop (echo.f90:189)
+    int g = b->max_tiles[PH_CELL] < 16 * b->nsm ? b->max_tiles[PH_CELL] : 16 * b->nsm;
+    batch_check_kernel<<<(unsigned)(g > 0 ? g : 1), 128, 0, b->stream>>>(b->P, batch_dev(b), b->nv,
+                                                                        b->d_v[b->vcur]);
+  }
   for (int irk = 1; irk <= b->p.nrk; irk++) enqueue_batch_stage(b, irk);
   batch_end_kernel<<<(unsigned)((b->nev + 127) / 128), 128, 0, b->stream>>>(batch_dev(b), b->p.coordinates,
                                                                              batch_roles(b));
@@ -223,6 +228,8 @@ int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos, int
   CK(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev));
   for (int s = 0; s < SL_N; s++) b->sched[s] = 0;
   b->tmax = 0.;
+  b->temp_end = 0.;
+  b->freeze_type = 1;
   b->vcur = b->ucur = b->vn = 0;
   b->marks = nullptr;
   *out = b;
@@ -306,10 +313,10 @@ static int batch_upload_impl(EchoBatch* b, const double* v, const double* u, dou
   if (r) return r;
   size_t bytes = sizeof(double) * b->nv * b->ncell;
   CK(cudaMemcpyAsync(b->d_v[0], v, bytes, kind, b->stream));
+  batch_begin(b, 0);  // tile lists of every event (the first check_temp uses them)
   if (u) {
     CK(cudaMemcpyAsync(b->d_u[0], u, bytes, kind, b->stream));
   } else {
-    batch_begin(b, 0);  // tile lists of every event
     BDISPATCH(b, launch_batch_p2c, b);
   }
   CK(cudaStreamSynchronize(b->stream));
@@ -476,6 +483,15 @@ int echo_batch_set_schedule(EchoBatch* b, const int* ctas, const int* order) {
     for (int s = 0; s < SL_N; s++) b->sched[s] = ctas[s];
   if (order) CK(cudaMemcpy(b->d_order, order, sizeof(int) * b->nev, cudaMemcpyHostToDevice));
   drop_graphs(b);
+  return ECHO_OK;
+}
+
+int echo_batch_set_stop(EchoBatch* b, int freeze_type, double temp_end) {
+  if (!b || (freeze_type != 0 && freeze_type != 1)) return ECHO_ERR_ARG;
+  CK(cudaStreamSynchronize(b->stream));
+  b->freeze_type = freeze_type;
+  b->temp_end = temp_end;
+  drop_graphs(b);  // the graphs hold both
   return ECHO_OK;
 }
 

@@ -27,7 +27,7 @@ enum { PH_FX = 0, PH_FY = 1, PH_FZ = 2, PH_CELL = 3, PH_N = 4 };
 // launch-shape slots of the schedule: the three face sweeps, update, smoothing
 enum { SL_FX = 0, SL_FY = 1, SL_FZ = 2, SL_UPDATE = 3, SL_SMOOTH = 4, SL_N = 5 };
 // event states
-enum { EV_LIVE = 0, EV_DONE = 1, EV_CRASHED = 2 };
+enum { EV_LIVE = 0, EV_DONE = 1, EV_CRASHED = 2, EV_COOLED = 3 };
 
 struct EvDesc {
   Grid g;
@@ -46,6 +46,8 @@ struct BatchDev {
   int* roles;        // buffer roles (ucur | vcur << 1) when the event stopped; -1 while live
   int nev;
   double tmax;
+  double temp_end;   // check_temp threshold (TEMP_END); <= 0: no check
+  int freeze_type;   // 0: temperature, 1: energy density
 };
 
 __host__ __device__ __forceinline__ int tiles_of(size_t n) { return (int)((n + BATCH_TILE - 1) / BATCH_TILE); }
@@ -93,6 +95,10 @@ static __global__ void __launch_bounds__(BEGIN_THREADS) batch_stage_begin_kernel
     DevScalars* sc = B.sc + e;
     int st = B.state[e];
     if (st == EV_LIVE && irk == 1 && sc->t >= B.tmax) st = EV_DONE;
+    // check_temp after the tmax test (echo.f90:187-190)
+    if (st == EV_LIVE && irk == 1 && B.temp_end > 0. &&
+        __longlong_as_double((long long)sc->check_bits) < B.temp_end)
+      st = EV_COOLED;
     if (st == EV_LIVE && sc->err_key != ~0ull) st = EV_CRASHED;
     if (st != EV_LIVE && B.state[e] == EV_LIVE) B.roles[e] = roles;
     B.state[e] = st;
@@ -373,6 +379,28 @@ static __global__ void __launch_bounds__(128) batch_glauber_fill_kernel(DevPhys 
   }
 }
 
+// check_temp of every live event at the top of its time loop (echo.f90:189):
+// the event's maximum of check_value over its cells, into its check_bits
+static __global__ void __launch_bounds__(128) batch_check_kernel(DevPhys P, BatchDev B, int nv,
+                                                                 const double* __restrict__ v) {
+  __shared__ double red[4];
+  const int* pre = B.prefix + PH_CELL * (B.nev + 1);
+  const int total = pre[B.nev];
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    const int i = tile_slot(pre, B.nev, t);
+    const int e = B.order[i];
+    const EvDesc& d = B.ev[e];
+    const size_t c = (size_t)(t - pre[i]) * BATCH_TILE + threadIdx.x;
+    double x = 0.;
+    if (c < d.g.ncell) {
+      const double* ve = v + (size_t)nv * d.cell;
+      x = check_value(P, B.freeze_type, ve[(size_t)KRH * d.g.ncell + c], ve[(size_t)KPR * d.g.ncell + c]);
+    }
+    block_max_atomic(x, &B.sc[e].check_bits, red);
+    __syncthreads();
+  }
+}
+
 // end of step per live event (echo.f90:206-241): a crash ends the event,
 // otherwise t advances and the step counts; `roles` are those after the step
 static __global__ void batch_end_kernel(BatchDev B, int coordinates, int roles) {
@@ -386,6 +414,7 @@ static __global__ void batch_end_kernel(BatchDev B, int coordinates, int roles) 
   }
   end_step_scalars(sc, coordinates);
   B.steps[e] += 1;
+  sc->check_bits = 0;  // the next step's check_temp maximum starts from 0
 }
 
 }  // namespace echo
@@ -427,6 +456,8 @@ struct EchoBatch {
   double* d_tab;
   int* d_bk;
   double tmax;
+  double temp_end;
+  int freeze_type;
   int nsm;
   int max_tiles[echo::PH_N];  // tiles with every event live
   int sched[echo::SL_N];      // CTAs per launch of each slot; 0 = one per tile
@@ -448,6 +479,8 @@ inline BatchDev batch_dev(const EchoBatch* b) {
   B.roles = b->d_roles;
   B.nev = b->nev;
   B.tmax = b->tmax;
+  B.temp_end = b->temp_end;
+  B.freeze_type = b->freeze_type;
   return B;
 }
 

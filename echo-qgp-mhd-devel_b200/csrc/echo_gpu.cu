@@ -532,6 +532,28 @@ int echo_gpu_run(EchoCtx* c, int nsteps) {
   return ECHO_OK;
 }
 
+int echo_gpu_check_temp(EchoCtx* c, int freeze_type, double temp_end, double* max_value, int* stop) {
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c || (freeze_type != 0 && freeze_type != 1)) return ECHO_ERR_ARG;
+  CK(cudaMemsetAsync(&c->d_sc->check_bits, 0, sizeof(unsigned long long), c->stream));
+  int dev = 0, nsm = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  size_t blocks = (c->g.ncell + 255) / 256;
+  if (blocks > (size_t)(8 * nsm)) blocks = (size_t)(8 * nsm);
+  check_temp_kernel<<<(unsigned)blocks, 256, 0, c->stream>>>(c->P, c->g, c->d_v[c->vcur], freeze_type,
+                                                              &c->d_sc->check_bits);
+  CK(cudaGetLastError());
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, &c->d_sc->check_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double m;
+  memcpy(&m, &bits, sizeof(m));
+  if (max_value) *max_value = m;
+  if (stop) *stop = m < temp_end ? 1 : 0;
+  return ECHO_OK;
+}
+
 int echo_gpu_stream(EchoCtx* c, void** stream) {
   if (!c || !stream) return ECHO_ERR_ARG;
   *stream = (void*)c->stream;

@@ -29,6 +29,7 @@ struct DevScalars {
   unsigned long long err_key;  // (cell << 20) | code, min over failures
   int nfail, pad;
   unsigned long long c2p_iters, c2p_cells, repairs, fallbacks;
+  unsigned long long check_bits;  // check_temp maximum (bit pattern of a double >= 0)
 };
 
 struct Grid {
@@ -470,6 +471,31 @@ __device__ __forceinline__ void end_step_scalars(DevScalars* sc, int coordinates
 }
 
 static __global__ void end_step_kernel(DevScalars* sc, int coordinates) { end_step_scalars(sc, coordinates); }
+
+// check_temp (out.f90:1487-1557): the quantity the stop criterion compares
+// with TEMP_END -- the temperature (freeze_type 0) or the energy density
+// (freeze_type 1) of a cell from its rho and p, as
+// get_derived_temp_for_check (eos.f90:706-759, 972-983) gives them (the
+// interpolation of get_derived_data).  A cell outside the table does not
+// count: the reference keeps the previous cell's value there.
+__device__ __forceinline__ double check_value(const DevPhys& P, int freeze_type, double rh, double pr) {
+  double en = 0., temp = 0., s = 0.;
+  if (get_derived_data(P, rh, pr, &en, &temp, &s)) return 0.;
+  return freeze_type == 0 ? temp : en;
+}
+
+// grid maximum of check_value into *out (zeroed by the caller); the
+// reference starts its maximum from 0
+static __global__ void __launch_bounds__(256) check_temp_kernel(DevPhys P, Grid g, const double* __restrict__ v,
+                                                                int freeze_type, unsigned long long* out) {
+  __shared__ double red[8];
+  double m = 0.;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < g.ncell; c += (size_t)gridDim.x * blockDim.x) {
+    double x = check_value(P, freeze_type, v[(size_t)KRH * g.ncell + c], v[(size_t)KPR * g.ncell + c]);
+    m = x > m ? x : m;
+  }
+  block_max_atomic(m, out, red);
+}
 
 // ---------------------------------------------------------------------------
 // per-cell update

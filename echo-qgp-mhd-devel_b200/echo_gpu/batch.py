@@ -16,7 +16,7 @@ import numpy as np
 from .lib import LL, EchoEventGrid, EchoEventStatus, I, P, _dp, load
 from .params import EchoParams
 
-LIVE, DONE, CRASHED = 0, 1, 2
+LIVE, DONE, CRASHED, COOLED = 0, 1, 2, 3
 SLOTS = ("faces_x", "faces_y", "faces_z", "update", "smooth")
 KERNEL_CLASSES = ("faces_x", "faces_y", "faces_z", "scalars", "update_c2p", "repair_smooth", "end_step")
 
@@ -144,6 +144,10 @@ class Batch:
         s = P()
         self._check(self.lib.echo_batch_stream(self.h, ctypes.byref(s)), "stream")
         return s.value or 0
+
+    def set_stop(self, freeze_type: int = 1, temp_end: float = 0.0) -> None:
+        """Per-event check_temp stop criterion (TEMP_END; 0 turns it off)."""
+        self._check(self.lib.echo_batch_set_stop(self.h, freeze_type, temp_end), "set_stop")
 
     # -- launch shapes ---------------------------------------------------------
     def set_schedule(self, ctas=None, order=None) -> None:

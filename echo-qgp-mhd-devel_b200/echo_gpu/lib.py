@@ -80,6 +80,8 @@ FUNCTIONS = {
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
+    "echo_gpu_check_temp": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, D, I]),
+    "echo_batch_set_stop": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
     "echo_batch_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(EchoEventGrid),
                                        ctypes.POINTER(P)]),
     "echo_batch_free": (ctypes.c_int, [P]),
@@ -241,6 +243,14 @@ class Evolve:
         n = np.zeros(7, dtype=np.int32)
         self._check(self.lib.echo_gpu_profile_step(self.h, _dp(ms), _ip(n)), "profile_step")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def check_temp(self, freeze_type: int = 1, temp_end: float = 0.0):
+        """check_temp (out.f90:1487-1557) on the device: (maximum, stop)."""
+        m = ctypes.c_double(0)
+        stop = ctypes.c_int(0)
+        self._check(self.lib.echo_gpu_check_temp(self.h, freeze_type, temp_end, ctypes.byref(m),
+                                                 ctypes.byref(stop)), "check_temp")
+        return m.value, bool(stop.value)
 
     def rhs(self):
         du = np.empty(self.ncell * self.nv)

@@ -173,6 +173,16 @@ int echo_gpu_sync(EchoCtx* ctx);
  * own work or timing events against the library's launches. */
 int echo_gpu_stream(EchoCtx* ctx, void** stream);
 
+/* check_temp (out.f90:1487-1557), the stop criterion the driver evaluates at
+ * the top of every step when TEMP_END > 0 (echo.f90:189-190): the maximum
+ * over the current primitives of the temperature (freeze_type 0) or the
+ * energy density (freeze_type 1) that get_derived_temp_for_check
+ * (eos.f90:706-759) gives from rho and p, reduced on the device; *stop =
+ * (max < temp_end), the reference's temp_check.  Cells outside the table do
+ * not count.  Synchronises the stream. */
+int echo_gpu_check_temp(EchoCtx* ctx, int freeze_type, double temp_end,
+                        double* max_value, int* stop);
+
 /* Runs one full step with a CUDA event after every launch group and returns
  * the device time per kernel class (ms[7]: faces x, faces y, faces z, stage
  * scalars, update+con2prim, repair(+smoothing), end of step) and the number
@@ -291,7 +301,8 @@ typedef struct EchoEventGrid {
 } EchoEventGrid;
 
 /* event states */
-enum { ECHO_EVENT_LIVE = 0, ECHO_EVENT_DONE = 1, ECHO_EVENT_CRASHED = 2 };
+enum { ECHO_EVENT_LIVE = 0, ECHO_EVENT_DONE = 1, ECHO_EVENT_CRASHED = 2,
+       ECHO_EVENT_COOLED = 3 /* stopped by check_temp (echo_batch_set_stop) */ };
 
 typedef struct EchoEventStatus {
   double t, dt;
@@ -345,6 +356,12 @@ int echo_batch_live(EchoBatch* b, int* nlive);
 int echo_batch_status(EchoBatch* b, EchoEventStatus* st);
 int echo_batch_sync(EchoBatch* b);
 int echo_batch_stream(EchoBatch* b, void** stream);
+/* The per-event check_temp stop criterion (echo_gpu_check_temp): before each
+ * step every live event whose maximum temperature (freeze_type 0) or energy
+ * density (1) is below temp_end stops (ECHO_EVENT_COOLED), after the
+ * t >= tmax test, as the reference's time loop does (echo.f90:187-190).
+ * temp_end <= 0 (the default) turns it off. */
+int echo_batch_set_stop(EchoBatch* b, int freeze_type, double temp_end);
 /* Launch shape of each slot: the number of CTAs of its persistent launch
  * (0 = one CTA per tile); order (nev entries, or NULL = 0..nev-1) is the
  * order in which the tile lists visit the events. */

@@ -1380,6 +1380,25 @@ double orc_glm_ch(const Orc* e) { return e->glm_ch; }
 long long orc_repairs(const Orc* e) { return e->repairs; }
 long long orc_c2p_iters(const Orc* e) { return e->c2p_iters; }
 
+/* check_temp (out.f90:1487-1557): the maximum over the grid, in the
+ * Fortran loop order, of the temperature (freeze_type 0) or the energy
+ * density (1) that get_derived_temp_for_check (eos.f90:706-759, 972-983)
+ * gives from rho and p -- the interpolation of get_derived_data.  Where the
+ * call fails (p outside the table) the reference keeps the previous cell's
+ * value, which leaves the maximum unchanged: the cell is skipped. */
+double orc_check_temp(const Orc* e, int freeze_type) {
+  const Phys* ph = &e->ph;
+  size_t nc = e->ncell;
+  double mx = 0.;
+  for (size_t c = 0; c < nc; c++) {
+    double en = 0., temp = 0., s = 0.;
+    if (get_derived_data(ph, e->v[(size_t)KRH * nc + c], e->v[(size_t)KPR * nc + c], &en, &temp, &s)) continue;
+    double x = freeze_type == 0 ? temp : en;
+    if (x > mx) mx = x;
+  }
+  return mx;
+}
+
 static void table_attach(Phys* ph, double** tT, double** te, double** tp,
                          double** tc, int* nt, const double* tab, int n) {
   *nt = n;

@@ -48,6 +48,8 @@ double orc_dt(const Orc* e);
 double orc_glm_ch(const Orc* e);
 long long orc_repairs(const Orc* e);
 long long orc_c2p_iters(const Orc* e);
+/* check_temp (out.f90:1487-1557) over the current primitives */
+double orc_check_temp(const Orc* e, int freeze_type);
 
 /* kernels on their own, for unit parity tests */
 void orc_recon(int recal, int m, int n, const double* f, double* gl,

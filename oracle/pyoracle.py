@@ -49,6 +49,8 @@ def lib():
         for f in ("orc_repairs", "orc_c2p_iters"):
             getattr(L, f).restype = ctypes.c_longlong
             getattr(L, f).argtypes = [P]
+        L.orc_check_temp.restype = ctypes.c_double
+        L.orc_check_temp.argtypes = [P, ctypes.c_int]
         L.orc_recon.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]
         L.orc_c2p.argtypes = [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                               ctypes.c_double, D, D, I, I]
@@ -149,6 +151,10 @@ class Oracle:
     @property
     def glm_ch(self) -> float:
         return lib().orc_glm_ch(self.h)
+
+    def check_temp(self, freeze_type: int = 1) -> float:
+        """check_temp (out.f90:1487-1557): maximum T (0) or e (1) over the grid."""
+        return lib().orc_check_temp(self.h, freeze_type)
 
     @property
     def repairs(self) -> int:

@@ -14,7 +14,7 @@ import pyoracle as O
 from echo_gpu import events as EV
 from echo_gpu import initial as I
 from echo_gpu import params as P
-from echo_gpu.batch import CRASHED, DONE, SLOTS, Batch, event_grid
+from echo_gpu.batch import COOLED, CRASHED, DONE, SLOTS, Batch, event_grid
 from helpers import eos_table, przero_of, rel_linf, smooth_pressure_of
 
 pytestmark = pytest.mark.gpu
@@ -167,3 +167,49 @@ def test_glauber_initial_state_matches_numpy(small):
         o.set_state(v[e], None, es.cfg.tstart)
         vo, uo = o.state()
         assert rel_linf(vs, vo, b.nv) <= 1e-12 and rel_linf(us, uo, b.nv) <= 1e-12, e
+
+
+def _oracle_event_stop(es, e, v, freeze_type, temp_end):
+    """Event e alone on the oracle with the check_temp stop at the top of its
+    time loop (echo.f90:187-190); returns (v, steps, cooled)."""
+    cfg = es.event_config(e)
+    o = O.Oracle(_params(cfg), eos_table())
+    o.set_state(v, None, cfg.tstart)
+    o.set_tout(es.tmax, es.tmax - cfg.tstart, es.tmax)
+    steps = 0
+    while o.t < es.tmax:
+        if o.check_temp(freeze_type) < temp_end:
+            return o.state()[0], steps, True
+        o.step()
+        steps += 1
+    return o.state()[0], steps, False
+
+
+def test_batch_check_temp_stop(small):
+    """Per-event check_temp: events whose maximum energy density falls below
+    TEMP_END stop there (ECHO_EVENT_COOLED), the others run to tmax; every
+    event matches the oracle running it with the same stop criterion."""
+    es, v, _ = small
+    # scale each event's pressure so the events cool below the threshold at
+    # different steps
+    tab = eos_table()
+    vs = []
+    for e, fac in enumerate((0.35, 0.5, 0.7, 1.0, 0.25)):
+        x = v[e].reshape(12, -1).copy()
+        en = np.interp(x[4], tab[:, 2], tab[:, 1])
+        x[4] = I.table_pressure(tab, fac * en)
+        vs.append(x.reshape(-1))
+    temp_end = 7.0
+    ref = [_oracle_event_stop(es, e, vs[e], 1, temp_end) for e in range(es.nev)]
+    cooled = [r[2] for r in ref]
+    assert any(cooled) and not all(cooled), [r[1:] for r in ref]
+    for exact, tol in ((True, 1e-13), (False, 1e-12)):
+        b = _batch(es, vs, exact=exact)
+        b.set_stop(1, temp_end)
+        b.run_to_end(chunk=3)
+        st = b.status()
+        vg, _ = b.download()
+        for e, vv in enumerate(b.split(vg)):
+            vo, n, c = ref[e]
+            assert st[e]["state"] == (COOLED if c else DONE) and st[e]["steps"] == n, (e, st[e], n, c)
+            assert rel_linf(vv, vo, b.nv) <= tol, e

@@ -117,6 +117,20 @@ def test_smoothing_parity(nrk):
     assert ev <= 1e-12 and eu <= 1e-12, (ev, eu)
 
 
+@pytest.mark.parametrize("case", ["hd2d", "rmhd3d", "visc2d"])
+@pytest.mark.parametrize("exact,tol", [(True, 0.0), (False, 1e-13)])
+def test_check_temp_matches_oracle(case, exact, tol):
+    """check_temp (out.f90:1487-1557) on the device: the maximum temperature
+    and energy density of the state after a few steps, and the stop flag."""
+    ev, eu, o, g = _pair(CASES[case](), 3, exact=exact)
+    for ft in (0, 1):
+        mo = o.check_temp(ft)
+        mg, stop = g.check_temp(ft, mo * 1.01)
+        assert abs(mg - mo) <= tol * mo, (ft, mg, mo)
+        assert stop
+        assert not g.check_temp(ft, mo * 0.99)[1]
+
+
 def test_graph_run_matches_steps():
     ev, eu, _, _ = _pair(CASES["rmhd3d"](), 4, exact=True, use_run=True)
     assert ev <= 1e-13 and eu <= 1e-13

@@ -113,3 +113,24 @@ def test_mlp_oracle_gradient_by_finite_differences():
         lm, _ = O.mlp_grad(wm32, X, T)
         fd = (lp - lm) / (float(wp32[i]) - float(wm32[i]))
         assert abs(fd - g[i]) <= 2e-3 * max(1e-3, abs(g[i])), (i, fd, g[i])
+
+
+def test_check_temp_known_answers():
+    """check_temp (out.f90:1487-1557): on a uniform state the maximum energy
+    density is the state's e, and with p = e/3 the temperature is
+    0.148909 e^(1/4) (temperature.def); on the table the maximum is that of
+    the hottest cell."""
+    cfg = P.small(P.config0(), 6)
+    o = O.Oracle(cfg.to_c(przero=cfg.enezero / 3))
+    o.set_state(I.bjorken_uniform(cfg, 12.0), None, 0.4)
+    assert abs(o.check_temp(1) - 12.0) <= 1e-14 * 12.0
+    assert abs(o.check_temp(0) - 0.148909 * 12.0 ** 0.25) <= 1e-14
+    cfg = CASES["visc2d"]()
+    pc, tab, v = setup(cfg)
+    o = O.Oracle(pc, tab)
+    o.set_state(v, None, cfg.tstart)
+    p = v.reshape(cfg.nv, -1)[4]
+    e_of_p = np.interp(p, tab[:, 2], tab[:, 1])
+    T_of_p = np.interp(p, tab[:, 2], tab[:, 0])
+    assert abs(o.check_temp(1) / e_of_p.max() - 1) < 1e-12
+    assert abs(o.check_temp(0) / T_of_p.max() - 1) < 1e-12
