@@ -190,23 +190,29 @@ def algorithmic_bytes(kclass: str, cfg) -> float:
     return 0.0
 
 
-def run_batched(args, torch, barrier, world):
+def run_batched(args, torch, barrier, world, rank):
     """The batched event-by-event workload: 512 Monte Carlo Glauber Pb+Pb
     events (viscous 2+1D, grids 61^2..161^2) from tau = 0.4 to 10 fm/c in
     one batch, beside the same events run one after another through the
-    single-grid path."""
+    single-grid path.  With N ranks the events are split across the GPUs by
+    cell count (no collective on the data path): the whole job's
+    cell-updates over the slowest rank's time."""
     from echo_gpu import events as EV
     from echo_gpu import initial as I
+    from echo_gpu import shard as SH
     from echo_gpu.batch import Batch, event_grid
     from echo_gpu.lib import Evolve
 
-    es = EV.batched_viscous()
+    full = EV.batched_viscous()
+    mine = SH.partition_by_cells(full.cells, world)[rank]
+    es = EV.EventSet(cfg=full.cfg, b=full.b[mine], n=full.n[mine], dx=full.dx, tmax=full.tmax)
     tab = EV.batched_eos_table()
     przero = float(I.table_pressure(tab, np.array([es.cfg.enezero]))[0])
     pcut = I.table_temperature_to_pressure(tab, es.cfg.smooth_temp)
     pc = es.cfg.to_c(przero=przero, smooth_pressure=pcut)
     t0 = time.perf_counter()
-    srcs = EV.event_sources(es)
+    srcs_all = EV.event_sources(full)
+    srcs = [srcs_all[int(e)] for e in mine]
     sampling_s = time.perf_counter() - t0
     b = Batch(pc, tab, [event_grid(*es.grid(e)) for e in range(es.nev)])
     t0 = time.perf_counter()
@@ -224,10 +230,11 @@ def run_batched(args, torch, barrier, world):
     nsteps = b.run_to_end(chunk=16)
     e1.record(stream)
     b.sync()
-    ms = e0.elapsed_time(e1)
-    st = b.status()
-    cu = b.cell_updates()
-    states = np.bincount([s["state"] for s in st], minlength=3)
+    barrier()
+    ms = SH.reduce_max(e0.elapsed_time(e1), device="cuda")
+    st_local = b.status()
+    cu = SH.reduce_sum(b.cell_updates(), device="cuda")
+    st = SH.gather_status(mine, st_local, full.nev)
     # the same events one at a time through the single-grid path (a sample)
     b.glauber(srcs, es.cfg.tstart, es.tmax)
     v0 = b.split(b.download()[0])
@@ -251,17 +258,24 @@ def run_batched(args, torch, barrier, world):
         seq_ms += f0.elapsed_time(f1)
         seq_cu += 20 * cfg.ncell
         g.close()
-    value = cu * world / (ms / 1e3)
     seq = seq_cu / (seq_ms / 1e3)
+    if rank != 0:
+        return None
+    value = cu / (ms / 1e3)
+    states = np.bincount([s["state"] for s in st], minlength=4)
     return {
-        "workload": f"{es.nev} MC-Glauber Pb+Pb events (b in [0,12] fm), viscous 2+1D IS, grids "
-                    f"{int(es.n.min())}^2..{int(es.n.max())}^2 at dx={es.dx}, tau {es.cfg.tstart} -> {es.tmax} fm/c, "
-                    f"CFL dt per event, RK2, WENO5+HLL, crossover EoS to 1e-7 GeV/fm^3, ENEZERO {es.cfg.enezero}",
-        "cells": int(es.cells.sum()),
+        "workload": f"{full.nev} MC-Glauber Pb+Pb events (b in [0,12] fm), viscous 2+1D IS, grids "
+                    f"{int(full.n.min())}^2..{int(full.n.max())}^2 at dx={full.dx}, tau {full.cfg.tstart} -> "
+                    f"{full.tmax} fm/c, CFL dt per event, RK2, WENO5+HLL, crossover EoS to 1e-7 GeV/fm^3, "
+                    f"ENEZERO {full.cfg.enezero}",
+        "cells": int(full.cells.sum()),
         "value": value, "unit": UNIT, "ms": ms, "batched_steps": nsteps,
-        "cell_updates": cu, "events_done": int(states[1]), "events_crashed": int(states[2]),
+        "scaling": "strong" if world > 1 else None,
+        "sharding": f"events split over {world} GPU(s) by cell count, no data-path collective",
+        "cell_updates": int(cu), "events_done": int(states[1]), "events_crashed": int(states[2]),
         "event_steps_min_max": [int(min(s["steps"] for s in st)), int(max(s["steps"] for s in st))],
-        "sequential_single_grid": {"value": seq, "unit": UNIT, "sample": f"every 16th event, 20 steps each"},
+        "sequential_single_grid": {"value": seq, "unit": UNIT,
+                                   "sample": "every 16th event of rank 0's share, 20 steps each, one GPU"},
         "speedup_vs_sequential": value / world / seq,
         "kernels_ms_per_step_at_start": {k: round(x, 4) for k, x in prof.items()},
         "autotuned_ms_per_launch": {k: round(x, 4) for k, x in tune_ms.items()},
@@ -382,7 +396,7 @@ def run_b200(args):
         dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
     e2e_value = cfg0.ncell * e2e_steps * world / (float(e2e_ms.item()) / 1e3)
     st2 = ev.stats()
-    batched = run_batched(args, torch, barrier, world) if args.batched else None
+    batched = run_batched(args, torch, barrier, world, rank) if args.batched else None
 
     if world > 1:
         dist.barrier()
