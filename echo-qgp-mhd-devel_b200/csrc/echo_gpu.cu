@@ -554,6 +554,73 @@ int echo_gpu_check_temp(EchoCtx* c, int freeze_type, double temp_end, double* ma
   return ECHO_OK;
 }
 
+// Checkpoint of the run state at a step boundary (the role of out_dump /
+// out_restart, out.f90:1313-1483): the current v and u, vold (the snapshot
+// the next step's lagged time derivatives read) and every run scalar.
+struct EchoCheckpointHeader {
+  char magic[8];
+  int kind, nv, nx, ny, nz, nrk;
+  int scalars_bytes;
+  int pad;
+  DevScalars sc;
+};
+static const char kCkptMagic[8] = {'E', 'C', 'H', 'O', 'C', 'K', 'P', '1'};
+
+int echo_gpu_checkpoint_size(const EchoCtx* c, size_t* bytes) {
+  if (!c || !bytes) return ECHO_ERR_ARG;
+  *bytes = sizeof(EchoCheckpointHeader) + sizeof(double) * c->g.ncell * (2 * (size_t)c->nv + 4);
+  return ECHO_OK;
+}
+
+int echo_gpu_checkpoint(EchoCtx* c, void* blob) {
+  (void)cudaGetLastError();
+  if (!c || !blob) return ECHO_ERR_ARG;
+  EchoCheckpointHeader h;
+  memset(&h, 0, sizeof(h));
+  memcpy(h.magic, kCkptMagic, 8);
+  h.kind = c->kind;
+  h.nv = c->nv;
+  h.nx = c->g.nx;
+  h.ny = c->g.ny;
+  h.nz = c->g.nz;
+  h.nrk = c->p.nrk;
+  h.scalars_bytes = (int)sizeof(DevScalars);
+  size_t nvc = (size_t)c->nv * c->g.ncell;
+  char* p = (char*)blob + sizeof(h);
+  CK(cudaMemcpyAsync(&h.sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(p, c->d_v[c->vcur], sizeof(double) * nvc, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(p + sizeof(double) * nvc, c->d_u[c->ucur], sizeof(double) * nvc, cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaMemcpyAsync(p + sizeof(double) * 2 * nvc, c->d_vh[1 - c->vn], sizeof(double) * 4 * c->g.ncell,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  memcpy(blob, &h, sizeof(h));
+  return ECHO_OK;
+}
+
+int echo_gpu_restart(EchoCtx* c, const void* blob) {
+  (void)cudaGetLastError();
+  if (!c || !blob) return ECHO_ERR_ARG;
+  EchoCheckpointHeader h;
+  memcpy(&h, blob, sizeof(h));
+  if (memcmp(h.magic, kCkptMagic, 8) != 0 || h.scalars_bytes != (int)sizeof(DevScalars) || h.kind != c->kind ||
+      h.nv != c->nv || h.nx != c->g.nx || h.ny != c->g.ny || h.nz != c->g.nz || h.nrk != c->p.nrk) {
+    fprintf(stderr, "echo_gpu_restart: the checkpoint does not belong to a run of this shape\n");
+    return ECHO_ERR_ARG;
+  }
+  size_t nvc = (size_t)c->nv * c->g.ncell;
+  const char* p = (const char*)blob + sizeof(h);
+  c->vcur = c->ucur = c->vn = 0;
+  CK(cudaMemcpyAsync(c->d_sc, &h.sc, sizeof(DevScalars), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_v[0], p, sizeof(double) * nvc, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_u[0], p + sizeof(double) * nvc, sizeof(double) * nvc, cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(c->d_vh[1], p + sizeof(double) * 2 * nvc, sizeof(double) * 4 * c->g.ncell,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ECHO_OK;
+}
+
 int echo_gpu_stream(EchoCtx* c, void** stream) {
   if (!c || !stream) return ECHO_ERR_ARG;
   *stream = (void*)c->stream;

@@ -80,6 +80,9 @@ FUNCTIONS = {
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
+    "echo_gpu_checkpoint_size": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
+    "echo_gpu_checkpoint": (ctypes.c_int, [P, P]),
+    "echo_gpu_restart": (ctypes.c_int, [P, P]),
     "echo_gpu_check_temp": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, D, I]),
     "echo_batch_set_stop": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
     "echo_batch_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(EchoEventGrid),
@@ -243,6 +246,19 @@ class Evolve:
         n = np.zeros(7, dtype=np.int32)
         self._check(self.lib.echo_gpu_profile_step(self.h, _dp(ms), _ip(n)), "profile_step")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def checkpoint(self) -> bytes:
+        """The run state at this step boundary (out_dump's role)."""
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.echo_gpu_checkpoint_size(self.h, ctypes.byref(n)), "checkpoint_size")
+        buf = ctypes.create_string_buffer(n.value)
+        self._check(self.lib.echo_gpu_checkpoint(self.h, buf), "checkpoint")
+        return buf.raw
+
+    def restart(self, blob: bytes) -> None:
+        """Continue from a checkpoint of a run of the same shape (out_restart)."""
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        self._check(self.lib.echo_gpu_restart(self.h, buf), "restart")
 
     def check_temp(self, freeze_type: int = 1, temp_end: float = 0.0):
         """check_temp (out.f90:1487-1557) on the device: (maximum, stop)."""

@@ -183,6 +183,18 @@ int echo_gpu_stream(EchoCtx* ctx, void** stream);
 int echo_gpu_check_temp(EchoCtx* ctx, int freeze_type, double temp_end,
                         double* max_value, int* stop);
 
+/* Checkpoint / restart of a run at a step boundary (the role of out_dump and
+ * out_restart, out.f90:1313-1483, which the reference turns off for MHD and
+ * Monte Carlo runs; here every equation set).  The blob (checkpoint_size
+ * bytes, host memory) holds the current v and u, vold and every run scalar
+ * (t, dt, timeold, timeinterval, tout, GLM speed, ...); a context of the same
+ * shape restarted from it continues bit for bit as the original would have.
+ * Both synchronise the stream; restart rejects a blob of another shape with
+ * ECHO_ERR_ARG. */
+int echo_gpu_checkpoint_size(const EchoCtx* ctx, size_t* bytes);
+int echo_gpu_checkpoint(EchoCtx* ctx, void* blob);
+int echo_gpu_restart(EchoCtx* ctx, const void* blob);
+
 /* Runs one full step with a CUDA event after every launch group and returns
  * the device time per kernel class (ms[7]: faces x, faces y, faces z, stage
  * scalars, update+con2prim, repair(+smoothing), end of step) and the number
