@@ -13,6 +13,9 @@
 
 using namespace echo;
 
+struct EchoHyp;  // freeze-out hypersurface state (hyper.cu)
+void echo_hyp_free(EchoHyp* h);
+
 struct EchoCtx {
   EchoParams p;
   int kind, nv, nvold;
@@ -42,6 +45,7 @@ struct EchoCtx {
   bool graph_ok[8];
   // per-kernel timing (echo_gpu_profile_step): events recorded after each launch group
   std::vector<std::pair<int, cudaEvent_t>>* marks;
+  EchoHyp* hyp;             // set up by echo_gpu_hyp_init
 };
 
 // kernel classes reported by echo_gpu_profile_step

@@ -341,6 +341,7 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->marks = nullptr;
   c->d_mlp_frag = nullptr;
   c->d_mlp_par = nullptr;
+  c->hyp = nullptr;
   *out = c;
   return ECHO_OK;
 }
@@ -368,6 +369,7 @@ int echo_gpu_free(EchoCtx* c) {
   cudaFree(c->d_mlp_frag);
   cudaFree(c->d_mlp_par);
   cudaFreeHost(c->h_sc);
+  echo_hyp_free(c->hyp);
   cudaStreamDestroy(c->stream);
   free(c);
   return ECHO_OK;

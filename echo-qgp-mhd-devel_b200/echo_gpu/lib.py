@@ -80,6 +80,9 @@ FUNCTIONS = {
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
+    "echo_gpu_hyp_init": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
+    "echo_gpu_hyp_step": (ctypes.c_int, [P, I, I]),
+    "echo_gpu_hyp_get": (ctypes.c_int, [P, D]),
     "echo_gpu_checkpoint_size": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
     "echo_gpu_checkpoint": (ctypes.c_int, [P, P]),
     "echo_gpu_restart": (ctypes.c_int, [P, P]),
@@ -246,6 +249,22 @@ class Evolve:
         n = np.zeros(7, dtype=np.int32)
         self._check(self.lib.echo_gpu_profile_step(self.h, _dp(ms), _ip(n)), "profile_step")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def hyp_init(self, freeze_type: int, freeze_value: float) -> None:
+        """Freeze-out hypersurface on T (0) or e (1) = freeze_value."""
+        self._check(self.lib.echo_gpu_hyp_init(self.h, freeze_type, freeze_value), "hyp_init")
+
+    def hyp_step(self) -> np.ndarray:
+        """One out_hyp call: the elements found now, shape (n, 8 + nv)."""
+        n = ctypes.c_int(0)
+        err = ctypes.c_int(0)
+        self._check(self.lib.echo_gpu_hyp_step(self.h, ctypes.byref(n), ctypes.byref(err)), "hyp_step")
+        if err.value:
+            raise CrashError(err.value)
+        out = np.empty((n.value, 8 + self.nv))
+        if n.value:
+            self._check(self.lib.echo_gpu_hyp_get(self.h, _dp(out)), "hyp_get")
+        return out
 
     def checkpoint(self) -> bytes:
         """The run state at this step boundary (out_dump's role)."""

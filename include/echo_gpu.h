@@ -26,6 +26,8 @@
 #ifndef ECHO_GPU_H
 #define ECHO_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -194,6 +196,25 @@ int echo_gpu_check_temp(EchoCtx* ctx, int freeze_type, double temp_end,
 int echo_gpu_checkpoint_size(const EchoCtx* ctx, size_t* bytes);
 int echo_gpu_checkpoint(EchoCtx* ctx, void* blob);
 int echo_gpu_restart(EchoCtx* ctx, const void* blob);
+
+/* Freeze-out hypersurface (out_hyp, out.f90:1569-1650, with
+ * find_hypersurface_ideal/_visco/_mhd and set_fo_ide/_vis,
+ * hypersurface.f90:172-460, 775-1117), on the device.  hyp_init sets the
+ * freeze criterion -- temperature (freeze_type 0) or energy density (1) equal
+ * to freeze_value -- and allocates the two time slices.  Each hyp_step is one
+ * out_hyp call at the current t: the field of the current primitives
+ * becomes the new slice; from the second call on, the surface elements
+ * between the two slices are collected, in the reference's order (ix outer,
+ * eta inner; per cell tau, x, y, eta).  Every element is 8 + nv doubles:
+ * tau, x, y, eta; the nv primitives interpolated to the crossing; dV_tau,
+ * dV_x, dV_y, dV_eta times the crossing's sign (hy_ide's columns, then
+ * hy_vis's for viscous runs).  *errcode: a get_derived_data code (the
+ * reference crashes the run) or 1 for a superluminal element (the reference
+ * exits).  hyp_step synchronises and may grow its output buffer; hyp_get
+ * copies the last call's n_elements records to the host. */
+int echo_gpu_hyp_init(EchoCtx* ctx, int freeze_type, double freeze_value);
+int echo_gpu_hyp_step(EchoCtx* ctx, int* n_elements, int* errcode);
+int echo_gpu_hyp_get(EchoCtx* ctx, double* out);
 
 /* Runs one full step with a CUDA event after every launch group and returns
  * the device time per kernel class (ms[7]: faces x, faces y, faces z, stage

@@ -1364,6 +1364,10 @@ struct Orc {
   double glm_ch, glm_ch_old, aflux[3];
   int run_crashed, errcode, nthreads;
   long long repairs, c2p_iters;
+  /* freeze-out hypersurface (hypersurface.f90, out_hyp out.f90:1569-1650) */
+  int hyp_on, hyp_first, hyp_type, hyp_n;
+  double hyp_value, hyp_time[2];
+  double *hyp_field1, *hyp_field2, *hyp_prim, *hyp_back, *hyp_out;
 };
 
 #define IDX(e, k, ix, iy, iz) \
@@ -1476,7 +1480,138 @@ void orc_free(Orc* e) {
   free(e->w); free(e->ax); free(e->ay); free(e->az); free(e->deriv);
   free(e->vold); free(e->vnewstep); free(e->vtmp); free(e->fail);
   free(e->tT); free(e->te); free(e->tp); free(e->tc);
+  free(e->hyp_field1); free(e->hyp_field2); free(e->hyp_prim); free(e->hyp_back); free(e->hyp_out);
   free(e);
+}
+
+/* ------------------------------------------------------------------------ */
+/* freeze-out hypersurface                                                  */
+/* ------------------------------------------------------------------------ */
+/* Record of one surface element, HYP_REC(nv) doubles: tau, x, y, eta; the nv
+ * primitives interpolated to the crossing; dV_tau, dV_x, dV_y, dV_eta with
+ * the crossing's sign.  For ideal and viscous runs these are the columns of
+ * hy_ide (tau..prex, dV) and hy_vis (Pi, pi^xy..pi^zz) of the reference. */
+#define HYP_REC(nv) (8 + (nv))
+
+int orc_hyp_init(Orc* e, int freeze_type, double freeze_value) {
+  size_t nc = e->ncell;
+  if (freeze_type != 0 && freeze_type != 1) return -1;
+  if (!e->hyp_on) {
+    e->hyp_field1 = (double*)calloc(nc, sizeof(double));
+    e->hyp_field2 = (double*)calloc(nc, sizeof(double));
+    e->hyp_prim = (double*)calloc(nc * e->nv, sizeof(double));
+    e->hyp_back = (double*)calloc(nc * e->nv, sizeof(double));
+    e->hyp_out = (double*)calloc(4 * nc * HYP_REC(e->nv), sizeof(double));
+  }
+  e->hyp_on = 1;
+  e->hyp_first = 1;
+  e->hyp_type = freeze_type;
+  e->hyp_value = freeze_value;
+  e->hyp_n = 0;
+  e->hyp_time[0] = e->hyp_time[1] = 0.;
+  return 0;
+}
+
+/* one crossing between cell (it; ix,iy,iz) and (iit; iix,iiy,iiz):
+ * set_fo_ide / set_fo_vis (hypersurface.f90:354-460, 984-1117) and the
+ * sign of save_hypersurface_* (:280-350) */
+static int hyp_element(Orc* e, int it, int ix, int iy, int iz, int iit, int iix, int iiy, int iiz, int tau_dir,
+                       double* rec) {
+  int nv = e->nv;
+  const double* f_it = it == 1 ? e->hyp_field1 : e->hyp_field2;
+  const double* f_iit = iit == 1 ? e->hyp_field1 : e->hyp_field2;
+  size_t c = IDX(e, 0, ix, iy, iz), cc = IDX(e, 0, iix, iiy, iiz);
+  double fv = e->hyp_value;
+  double weight = (f_it[c] - fv) / (f_it[c] - f_iit[cc]);
+  double sign_ = f_it[c] - f_iit[cc] >= 0. ? 1.0 : -1.0; /* sign(1.0d0, .) */
+  double xc = e->p.x1 + ((double)ix - 0.5) * e->dx, xcc = e->p.x1 + ((double)iix - 0.5) * e->dx;
+  double yc = e->p.y1 + ((double)iy - 0.5) * e->dy, ycc = e->p.y1 + ((double)iiy - 0.5) * e->dy;
+  double zc = e->p.z1 + ((double)iz - 0.5) * e->dz, zcc = e->p.z1 + ((double)iiz - 0.5) * e->dz;
+  rec[0] = e->hyp_time[it - 1] + weight * (e->hyp_time[iit - 1] - e->hyp_time[it - 1]);
+  rec[1] = xc + weight * (xcc - xc);
+  rec[2] = yc + weight * (ycc - yc);
+  rec[3] = zc + weight * (zcc - zc);
+  const double* far = tau_dir ? e->hyp_prim : e->hyp_back;
+  for (int k = 0; k < nv; k++) {
+    double a = e->hyp_back[(size_t)k * e->ncell + c];
+    rec[4 + k] = a + weight * (far[(size_t)k * e->ncell + cc] - a);
+  }
+  double g3 = e->p.coordinates == ECHO_BJORKEN ? e->hyp_time[1] * e->hyp_time[1] : 1.;
+  double betasq = rec[4 + KVX] * rec[4 + KVX] + rec[4 + KVY] * rec[4 + KVY] + rec[4 + KVZ] * rec[4 + KVZ] * g3;
+  if (betasq > 1.0) return 1; /* the reference stops here ("you have to fix this") */
+  double dt = fabs(e->hyp_time[1] - e->hyp_time[0]);
+  double dx = e->dx, dy = e->dy, dz = e->nz > 1 ? e->dz : 1.0; /* d_val, common.f90:472-478 */
+  rec[4 + nv] = sign_ * ((double)(iit - it) * dx * dy * dz * rec[0]);
+  rec[5 + nv] = sign_ * ((double)(iix - ix) * dt * dy * dz * rec[0]);
+  rec[6 + nv] = sign_ * ((double)(iiy - iy) * dx * dt * dz * rec[0]);
+  rec[7 + nv] = sign_ * ((double)(iiz - iz) * dx * dy * dt * rec[0]);
+  return 0;
+}
+
+/* out_hyp (out.f90:1569-1650) with find_hypersurface_* (hypersurface.f90:
+ * 172-229 and its viscous and MHD twins): the freeze field of the current
+ * primitives becomes slice 2, and from the second call on the crossings
+ * between the slices (tau) and inside slice 1 (x, y, eta) are collected in
+ * the reference's loop order: ix outer, iz inner; per cell tau, x, y, eta */
+int orc_hyp_step(Orc* e, int* nout) {
+  size_t nc = e->ncell;
+  int nv = e->nv;
+  if (!e->hyp_on) return -1;
+  *nout = 0;
+  if (e->hyp_first) e->hyp_time[1] = e->t;
+  for (size_t c = 0; c < nc; c++) {
+    double en = 0., temp = 0., s = 0.;
+    int err = get_derived_data(&e->ph, e->v[(size_t)KRH * nc + c], e->v[(size_t)KPR * nc + c], &en, &temp, &s);
+    if (err > 0) return err; /* out_hyp sets run_crashed */
+    e->hyp_field1[c] = e->hyp_field2[c];
+    e->hyp_field2[c] = e->hyp_type == 0 ? temp : en;
+  }
+  if (e->hyp_first) {
+    e->hyp_first = 0;
+    memcpy(e->hyp_prim, e->v, sizeof(double) * nc * nv);
+    e->hyp_n = 0;
+    return 0;
+  }
+  memcpy(e->hyp_back, e->hyp_prim, sizeof(double) * nc * nv);
+  memcpy(e->hyp_prim, e->v, sizeof(double) * nc * nv);
+  e->hyp_time[0] = e->hyp_time[1];
+  e->hyp_time[1] = e->t;
+  const double fv = e->hyp_value;
+  const double *f1 = e->hyp_field1, *f2 = e->hyp_field2;
+  int n = 0;
+  for (int ix = 1; ix <= e->nx; ix++)
+    for (int iy = 1; iy <= e->ny; iy++)
+      for (int iz = 1; iz <= e->nz; iz++) {
+        size_t c = IDX(e, 0, ix, iy, iz);
+        double* rec;
+        if ((f2[c] - fv) * (fv - f1[c]) > 0.0) {
+          rec = e->hyp_out + (size_t)n * HYP_REC(nv);
+          if (hyp_element(e, 1, ix, iy, iz, 2, ix, iy, iz, 1, rec)) return 1;
+          n++;
+        }
+        if (ix < e->nx && (f1[IDX(e, 0, ix + 1, iy, iz)] - fv) * (fv - f1[c]) > 0.0) {
+          rec = e->hyp_out + (size_t)n * HYP_REC(nv);
+          if (hyp_element(e, 1, ix, iy, iz, 1, ix + 1, iy, iz, 0, rec)) return 1;
+          n++;
+        }
+        if (iy < e->ny && (f1[IDX(e, 0, ix, iy + 1, iz)] - fv) * (fv - f1[c]) > 0.0) {
+          rec = e->hyp_out + (size_t)n * HYP_REC(nv);
+          if (hyp_element(e, 1, ix, iy, iz, 1, ix, iy + 1, iz, 0, rec)) return 1;
+          n++;
+        }
+        if (iz < e->nz && (f1[IDX(e, 0, ix, iy, iz + 1)] - fv) * (fv - f1[c]) > 0.0) {
+          rec = e->hyp_out + (size_t)n * HYP_REC(nv);
+          if (hyp_element(e, 1, ix, iy, iz, 1, ix, iy, iz + 1, 0, rec)) return 1;
+          n++;
+        }
+      }
+  e->hyp_n = n;
+  *nout = n;
+  return 0;
+}
+
+void orc_hyp_get(const Orc* e, double* out) {
+  memcpy(out, e->hyp_out, sizeof(double) * (size_t)e->hyp_n * HYP_REC(e->nv));
 }
 
 int orc_set_state(Orc* e, const double* v, const double* u, double t) {

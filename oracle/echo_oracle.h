@@ -50,6 +50,11 @@ long long orc_repairs(const Orc* e);
 long long orc_c2p_iters(const Orc* e);
 /* check_temp (out.f90:1487-1557) over the current primitives */
 double orc_check_temp(const Orc* e, int freeze_type);
+/* freeze-out hypersurface (out_hyp / find_hypersurface_*): records of
+ * 8 + nv doubles (tau, x, y, eta, primitives, dV with sign) */
+int orc_hyp_init(Orc* e, int freeze_type, double freeze_value);
+int orc_hyp_step(Orc* e, int* n);
+void orc_hyp_get(const Orc* e, double* out);
 
 /* kernels on their own, for unit parity tests */
 void orc_recon(int recal, int m, int n, const double* f, double* gl,

@@ -49,6 +49,9 @@ def lib():
         for f in ("orc_repairs", "orc_c2p_iters"):
             getattr(L, f).restype = ctypes.c_longlong
             getattr(L, f).argtypes = [P]
+        L.orc_hyp_init.argtypes = [P, ctypes.c_int, ctypes.c_double]
+        L.orc_hyp_step.argtypes = [P, I]
+        L.orc_hyp_get.argtypes = [P, D]
         L.orc_check_temp.restype = ctypes.c_double
         L.orc_check_temp.argtypes = [P, ctypes.c_int]
         L.orc_recon.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]
@@ -155,6 +158,21 @@ class Oracle:
     def check_temp(self, freeze_type: int = 1) -> float:
         """check_temp (out.f90:1487-1557): maximum T (0) or e (1) over the grid."""
         return lib().orc_check_temp(self.h, freeze_type)
+
+    def hyp_init(self, freeze_type: int, freeze_value: float) -> None:
+        if lib().orc_hyp_init(self.h, freeze_type, freeze_value):
+            raise ValueError("freeze_type must be 0 or 1")
+
+    def hyp_step(self) -> np.ndarray:
+        """out_hyp: the surface elements found now, shape (n, 8 + nv)."""
+        n = ctypes.c_int(0)
+        err = lib().orc_hyp_step(self.h, ctypes.byref(n))
+        if err:
+            raise RuntimeError(f"oracle hypersurface error {err}")
+        out = np.empty((n.value, 8 + self.nv))
+        if n.value:
+            lib().orc_hyp_get(self.h, _dp(out))
+        return out
 
     @property
     def repairs(self) -> int:
