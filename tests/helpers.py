@@ -69,3 +69,31 @@ CASES = {
     "rmhd3d": lambda: P.small(P.config1(), 10, nz=8),
     "visc2d": lambda: P.small(P.config2(), 14),
 }
+
+
+def gubser(tau, X, Y, q=1.0, T0=0.4):
+    """Ideal Gubser flow (the reference's GUBSER_IDEAL initial state,
+    init.f90:2901-2961, and the analytic solution it follows): temperature
+    (GeV) and radial velocity at Milne time tau."""
+    r2 = X * X + Y * Y
+    T = T0 / tau * (4 * q * q * tau * tau) ** (1 / 3) / (
+        1 + 2 * q * q * (tau * tau + r2) + q**4 * (tau * tau - r2) ** 2) ** (1 / 3)
+    vr = 2 * q * q * tau * np.sqrt(r2) / (1 + q * q * tau * tau + q * q * r2)
+    return T, vr
+
+
+def gubser_case(n=81, dx=0.1, dt=0.01, tau0=1.0):
+    """Conformal 2+1D Milne run of the Gubser state: config, primitives and
+    the cell centres.  e from T by temperature.def (T = 0.148909 e^(1/4))."""
+    h = 0.5 * n * dx
+    cfg = P.Config("gubser-ideal", n, n, 1, -h, h, -h, h, tstart=tau0, maxdt=dt, cfl=0.4, enezero=1e-6,
+                   recal="WENO5", nrk=P.RK2)
+    x = I.cell_centres(n, -h, h)
+    X, Y = np.meshgrid(x, x, indexing="xy")
+    T, vr = gubser(tau0, X, Y)
+    r = np.sqrt(X * X + Y * Y)
+    rs = np.where(r > 0, r, 1.0)
+    p = (T / 0.148909) ** 4 / 3.0
+    z = np.zeros_like(X)
+    v = np.stack([np.ones_like(X), vr * X / rs, vr * Y / rs, z, p]).reshape(-1)
+    return cfg, v, X, Y

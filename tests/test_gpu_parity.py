@@ -13,7 +13,7 @@ import pytest
 import pyoracle as O
 from echo_gpu import params as P
 from echo_gpu.lib import Evolve, unit_c2p, unit_recon
-from helpers import CASES, rel_linf, setup
+from helpers import CASES, gubser_case, rel_linf, setup
 
 pytestmark = pytest.mark.gpu
 
@@ -129,6 +129,28 @@ def test_check_temp_matches_oracle(case, exact, tol):
         assert abs(mg - mo) <= tol * mo, (ft, mg, mo)
         assert stop
         assert not g.check_temp(ft, mo * 0.99)[1]
+
+
+def test_gubser_flow_matches_oracle():
+    """The reference's ideal Gubser test problem on the device: 50 steps of
+    the 81x81 conformal run equal the oracle's (which converges to the
+    analytic flow, tests/test_oracle.py)."""
+    cfg, v, _, _ = gubser_case()
+    pc = cfg.to_c(przero=cfg.enezero / 3)
+    o = O.Oracle(pc, None)
+    o.set_state(v, None, cfg.tstart)
+    v0, u0 = o.state()
+    for exact, tol in ((True, 1e-13), (False, 1e-12)):
+        g = Evolve(pc.__class__.from_buffer_copy(pc), None, exact=exact)
+        g.upload(v0, u0, cfg.tstart)
+        g.run(50)
+        g.sync()
+        vg, ug = g.download()
+        if exact:
+            for _ in range(50):
+                o.step()
+            vo, uo = o.state()
+        assert rel_linf(vg, vo, 5) <= tol and rel_linf(ug, uo, 5) <= tol, exact
 
 
 def test_graph_run_matches_steps():

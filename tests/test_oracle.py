@@ -10,7 +10,7 @@ import pytest
 import pyoracle as O
 from echo_gpu import initial as I
 from echo_gpu import params as P
-from helpers import CASES, eos_table, rel_linf, setup
+from helpers import CASES, eos_table, gubser, gubser_case, rel_linf, setup
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -134,3 +134,29 @@ def test_check_temp_known_answers():
     T_of_p = np.interp(p, tab[:, 2], tab[:, 0])
     assert abs(o.check_temp(1) / e_of_p.max() - 1) < 1e-12
     assert abs(o.check_temp(0) / T_of_p.max() - 1) < 1e-12
+
+
+def _gubser_error(dt, tau1=1.5):
+    cfg, v, X, Y = gubser_case(dt=dt)
+    o = O.Oracle(cfg.to_c(przero=cfg.enezero / 3), None, threads=4)
+    o.set_state(v, None, cfg.tstart)
+    o.set_tout(tau1, 1e300, 1e300)
+    while o.t < tau1 - 1e-12:
+        o.step()
+    p = o.state()[0].reshape(5, cfg.ny, cfg.nx)[4]
+    T = 0.148909 * (3.0 * p) ** 0.25
+    Ta, _ = gubser(o.t, X, Y)
+    inner = np.sqrt(X * X + Y * Y) < 2.0  # away from the outflow boundaries
+    return float(np.max(np.abs(T[inner] / Ta[inner] - 1)))
+
+
+def test_gubser_flow_converges_first_order_in_dt():
+    """Ideal Gubser flow, the reference's own analytic test (init.f90:
+    2901-2961): the temperature at tau = 1.5 approaches the analytic one at
+    first order in dt, the order of the reference's step (the metric is
+    frozen over a step, echo.f90:211-214)."""
+    e1 = _gubser_error(0.02)
+    e2 = _gubser_error(0.01)
+    e3 = _gubser_error(0.005)
+    assert e3 < 1e-3
+    assert 1.7 < e1 / e2 < 2.4 and 1.7 < e2 / e3 < 2.4, (e1, e2, e3)
