@@ -160,3 +160,29 @@ def test_gubser_flow_converges_first_order_in_dt():
     e3 = _gubser_error(0.005)
     assert e3 < 1e-3
     assert 1.7 < e1 / e2 < 2.4 and 1.7 < e2 / e3 < 2.4, (e1, e2, e3)
+
+
+def _bjorken_mhd_error(dt, steps):
+    cfg = P.small(P.config1(), 6, nz=6).replace(maxdt=dt, cfl=10.0, eqstate=P.EOS_CONFORMAL,
+                                                algo_solver=P.C2P_BRENT, enezero=1e-6)
+    o = O.Oracle(cfg.to_c(przero=cfg.enezero / 3))
+    v = np.zeros((cfg.nv, cfg.ncell))
+    v[0], v[4], v[6] = 1.0, 10.0 / 3.0, 1.0  # rho, p = e/3 with e = 10, B^y = 1
+    o.set_state(v.reshape(-1), None, 0.4)
+    for _ in range(steps):
+        o.step()
+    vv = o.state()[0].reshape(cfg.nv, -1)
+    assert np.ptp(vv[4]) == 0.0 and np.abs(vv[1:4]).max() == 0.0  # uniform and at rest
+    e_err = vv[4, 0] * 3 / (10.0 * (0.4 / o.t) ** (4.0 / 3.0)) - 1
+    b_err = vv[6, 0] * o.t / 0.4 - 1
+    return abs(e_err), abs(b_err)
+
+
+def test_bjorken_mhd_flow_first_order_in_dt():
+    """1-D Bjorken MHD flow (the reference's Bjorken-MHD test, init.f90:
+    2454-2499): with a transverse field, e ~ tau^(-4/3) and B ~ 1/tau, both
+    reached at first order in dt by the frozen-metric step."""
+    e1, b1 = _bjorken_mhd_error(0.02, 25)
+    e2, b2 = _bjorken_mhd_error(0.01, 50)
+    assert 1.8 < e1 / e2 < 2.2 and 1.8 < b1 / b2 < 2.2, (e1, e2, b1, b2)
+    assert e2 < 1e-2 and b2 < 1.5e-2
