@@ -412,12 +412,15 @@ def run_b200(args):
     per_launch_s = dom_ms / dom_n / 1e3
     alg = algorithmic_bytes(dom, cfg0)
     achieved = alg / per_launch_s / 1e9
-    traffic = None
+    traffic, pipes = None, None
     tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get(dom)
+                rec = json.load(f).get(dom)
+            if isinstance(rec, dict):
+                traffic = rec.get("dram_bytes")
+                pipes = {k: rec[k] for k in ("fp64_pipe_pct", "tensor_pipe_pct") if k in rec}
         except Exception:
             traffic = None
     launches_per_step = sum(n for (_, n) in prof.values())
@@ -445,7 +448,7 @@ def run_b200(args):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg, "launch_ms": dom_ms / dom_n,
-                     "peak_src": pk["src"] + " (hbm_gbs)"},
+                     "peak_src": pk["src"] + " (hbm_gbs)", "ncu_pipes": pipes},
         "step_roofline": {"bytes_per_cell_update": B_ALG_STEP,
                           "achieved_gbs": value / world * B_ALG_STEP / 1e9,
                           "frac": value / world * B_ALG_STEP / 1e9 / pk["hbm_gbs"]},
