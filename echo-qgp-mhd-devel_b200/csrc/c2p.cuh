@@ -548,9 +548,15 @@ __device__ __forceinline__ void get_sigma(const DevPhys& P, const Metric& M, con
 // ---------------------------------------------------------------------------
 // system_source (system.f90:1587-1842) without the resistive terms.
 // v: primitives of the cell (modified copy), dv: its 16 derivatives.
+// kap, when not null on a viscous run, receives the Israel-Stewart
+// relaxation rates on the conserved stresses: the source of
+// u[k] = sqrt(-g) rho gamma v[k] holds -kap u[k], with kap[0] = 1/(gamma
+// tau_Pi) for the bulk pressure and kap[1] = 1/(gamma tau_pi) for the shear
+// components (the -1/tau (v[k] + ...) terms times rho sqrt(-g)).
 // ---------------------------------------------------------------------------
 template <int KIND>
-__device__ int system_source(const DevPhys& P, const Metric& M, double* v, const double* dv, double* src) {
+__device__ int system_source(const DevPhys& P, const Metric& M, double* v, const double* dv, double* src,
+                             double* kap = nullptr) {
   typedef Traits<KIND> T;
   double g1 = M.g1, g2 = M.g2, g3 = M.g3, gp = M.gp, g0 = M.g0, t = M.t;
 #pragma unroll
@@ -685,6 +691,10 @@ __device__ int system_source(const DevPhys& P, const Metric& M, double* v, const
     }
 #pragma unroll
     for (int k = KPIBU; k < T::NV; k++) src[k] = src[k] * v[KRH];
+    if (kap) {
+      kap[0] = 1. / (glf * tau_pi_big);
+      kap[1] = 1. / (glf * tau_pi);
+    }
   }
 #pragma unroll
   for (int k = 0; k < T::NV; k++) src[k] = src[k] * gp;

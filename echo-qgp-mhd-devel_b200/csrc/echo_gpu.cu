@@ -282,6 +282,8 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   *out = nullptr;
   if (p->mhd > 1 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
   if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3 && p->nrk != ECHO_SSP) return ECHO_ERR_UNSUPPORTED;
+  if (p->imex != 0 && p->imex != 1) return ECHO_ERR_ARG;
+  if (p->imex && p->nrk == ECHO_SSP) return ECHO_ERR_UNSUPPORTED;  // IMEX RK2/RK3 only
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return ECHO_ERR_ARG;
   if ((p->nx > 1 && p->nx < 3) || (p->ny > 1 && p->ny < 3) || (p->nz > 1 && p->nz < 3)) return ECHO_ERR_ARG;
   if (p->eqstate == ECHO_EOS_TABLE && (!eos_table || n_eos < 2)) return ECHO_ERR_ARG;

@@ -523,6 +523,7 @@ struct UpdateArgs {
   DevScalars* sc;
   double c1, c2;
   int irk, nrk, divclean, coordinates, algo, mode;
+  int imex;  // viscous: relaxation of the stresses linearly implicit per stage
   double tol;
   MlpDev mlp;  // learned seed (algo == ECHO_C2P_MLP)
   // viscous, stage 1 of a batched step: vnewstep = v (echo.f90:192-202) is
@@ -572,7 +573,7 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
     const size_t fx = ((size_t)iz * g.ny + iy) * (g.nx + 1) + ix;       // face ix-1/2 -> index ix
     const size_t fy = ((size_t)iz * (g.ny + 1) + iy) * g.nx + ix;
     const size_t fz = ((size_t)iz * g.ny + iy) * g.nx + ix;
-    double src[NV], du[NV];
+    double src[NV], du[NV], kap[2] = {0., 0.};
 #pragma unroll
     for (int k = 0; k < NV; k++) vv[k] = A.vin[(size_t)k * g.ncell + c];
     // flux divergence in the reference's order: du = 0; += x; += y; += z
@@ -643,7 +644,7 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
       double vs[NV];
 #pragma unroll
       for (int k = 0; k < NV; k++) vs[k] = vv[k];
-      int err = system_source<KIND>(A.P, M, vs, dv, src);
+      int err = system_source<KIND>(A.P, M, vs, dv, src, T::VISC ? kap : nullptr);
       if (err) atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
     }
 #pragma unroll
@@ -662,7 +663,14 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
           A.uin[(size_t)k * g.ncell + c] = ui;  // u0 = u after the GLM half step
         }
         double u0 = A.irk == 1 ? ui : A.u0[(size_t)k * g.ncell + c];
-        uu[k] = A.c1 * u0 + A.c2 * (ui - dt * du[k]);
+        if (T::VISC && k >= KPIBU && A.imex) {
+          // IMEX RK2/RK3: the relaxation -kap u of the stresses at the new
+          // stage value, u_new = u_expl + c2 dt kap (u - u_new)
+          double ck = A.c2 * dt * (k == KPIBU ? kap[0] : kap[1]);
+          uu[k] = (A.c1 * u0 + A.c2 * (ui - dt * du[k]) + ck * ui) / (1. + ck);
+        } else {
+          uu[k] = A.c1 * u0 + A.c2 * (ui - dt * du[k]);
+        }
       }
       if (T::GLM && A.irk == A.nrk) uu[KGLM] = uu[KGLM] * A.sc->expfact;
 #pragma unroll

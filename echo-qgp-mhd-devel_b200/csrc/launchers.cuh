@@ -67,6 +67,7 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   A.coordinates = c->p.coordinates;
   A.algo = c->p.algo_solver;
   A.mode = mode;
+  A.imex = c->p.imex;
   A.tol = c->p.c2p_tol;
   A.mlp.frag = c->d_mlp_frag;
   A.mlp.par = c->d_mlp_par;
@@ -211,6 +212,7 @@ void launch_batch_update(EchoBatch* b, int irk) {
   A.coordinates = b->p.coordinates;
   A.algo = b->p.algo_solver;
   A.mode = MODE_RK;
+  A.imex = b->p.imex;
   A.tol = b->p.c2p_tol;
   A.mlp.frag = nullptr;
   A.mlp.par = nullptr;

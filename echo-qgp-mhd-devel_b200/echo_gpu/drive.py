@@ -1,6 +1,6 @@
 """Run a named workload for a number of steps through the C-ABI.
 
-    python -m echo_gpu.drive --config rmhd --steps 3 [--c2p newton|mlp] [--exact] [--n N]
+    python -m echo_gpu.drive --config rmhd --steps 3 [--c2p newton|mlp] [--exact] [--imex] [--n N]
     python -m echo_gpu.drive --config batch --events 64 --steps 3
 
 Used for profiling runs: it does exactly the product path (upload, the
@@ -51,6 +51,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--c2p", default="brent", choices=["brent", "newton", "mlp"])
     ap.add_argument("--exact", action="store_true")
+    ap.add_argument("--imex", action="store_true", help="viscous: Israel-Stewart relaxation implicit per stage")
     ap.add_argument("--n", type=int, default=0, help="cells per side of a smaller grid (0 = full size)")
     ap.add_argument("--events", type=int, default=64, help="events of the batched workload")
     ap.add_argument("--pairs", type=int, default=100_000, help="training pairs for --c2p mlp")
@@ -66,6 +67,8 @@ def main():
         cfg = cfg.replace(algo_solver=P.C2P_NEWTON)
     if a.c2p == "mlp":
         cfg = cfg.replace(algo_solver=P.C2P_MLP)
+    if a.imex:
+        cfg = cfg.replace(imex=1)
     tab = I.eos_table_loaded() if cfg.eqstate == P.EOS_TABLE else None
     przero = float(I.table_pressure(tab, np.array([cfg.enezero]))[0]) if tab is not None else cfg.enezero / 3
     sp = I.table_temperature_to_pressure(tab, cfg.smooth_temp) if (tab is not None and cfg.viscosity) else 0.0

@@ -47,6 +47,7 @@ class EchoParams(ctypes.Structure):
         ("enezero", ctypes.c_double),
         ("przero", ctypes.c_double),
         ("c2p_tol", ctypes.c_double),
+        ("imex", ctypes.c_int),
     ]
 
 
@@ -91,6 +92,7 @@ class Config:
     tstart: float = 0.4
     steps: int = 10
     c2p_tol: float = 1e-10
+    imex: int = 0              # viscous: Israel-Stewart relaxation linearly implicit per stage
 
     @property
     def nv(self) -> int:
@@ -136,6 +138,7 @@ class Config:
         p.enezero = self.enezero
         p.przero = przero
         p.c2p_tol = self.c2p_tol
+        p.imex = self.imex
         return p
 
 

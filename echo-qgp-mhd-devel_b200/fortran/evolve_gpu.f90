@@ -22,6 +22,7 @@ module evolve_gpu
     integer(c_int) :: ibc(3, 2, ECHO_MAX_NV)   ! C int ibc[16][2][3]
     real(c_double) :: cfl, maxdt, maxspeed, glm_alpha, eta_over_s
     real(c_double) :: tau_pi_coeff, smooth_pressure, enezero, przero, c2p_tol
+    integer(c_int) :: imex   ! this library's implicit Israel-Stewart relaxation; set 0 for the reference's explicit
   end type echo_params
 
   type(c_ptr), save :: echo_ctx = c_null_ptr

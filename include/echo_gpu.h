@@ -100,6 +100,11 @@ typedef struct EchoParams {
   double enezero;                 /* ENEZERO */
   double przero;                  /* p(ENEZERO) (eos.f90:131) */
   double c2p_tol;                 /* Newton residual target (ECHO_C2P_NEWTON) */
+  int imex;                       /* this library (no param.dat key): 1 = viscous
+                                     runs treat the Israel-Stewart relaxation
+                                     linearly implicitly in every RK2/RK3 stage
+                                     (the "IMEX RK2" of the batched workload);
+                                     0 = explicit, as the reference */
 } EchoParams;
 
 typedef struct EchoCtx EchoCtx;

@@ -1193,8 +1193,13 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
 /* system_source (system.f90:1587-1842), non-resistive                      */
 /* v: cell primitives (copy), d: deriv of the cell                          */
 /* ------------------------------------------------------------------------ */
+/* kap, when not NULL and the run is viscous, receives the relaxation rates
+   of the Israel-Stewart equations on the conserved stresses: the source of
+   u[k] = sqrt(-g) rho gamma v[k] holds -kap u[k] with kap[0] = 1/(gamma tau_Pi)
+   for the bulk pressure and kap[1] = 1/(gamma tau_pi) for the shear
+   components (the -1/tau (v[k] + ...) terms times rho sqrt(-g)). */
 static int system_source(const Phys* ph, double* v, const double* dv,
-                         double* src) {
+                         double* src, double* kap) {
   const EchoParams* p = ph->p;
   double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gp = ph->gp, g0 = ph->g0;
   double t = ph->t;
@@ -1260,6 +1265,10 @@ static int system_source(const Phys* ph, double* v, const double* dv,
       double IVxz = v[KPIXX] * wzx + v[KPIZZ] * wxz + v[KPIXY] * wzy + v[KPIYZ] * wxy + pitx * wz0 + pitz * wx0;
       double IVyz = v[KPIYY] * wzy + v[KPIZZ] * wyz + v[KPIXY] * wzx + v[KPIXZ] * wyx + pity * wz0 + pitz * wy0;
       (void)pitt;
+      if (kap) {
+        kap[0] = 1. / (glf * tau_pi_big);
+        kap[1] = 1. / (glf * tau_pi);
+      }
       src[KPIZZ] = -1. / tau_pi * (v[KPIZZ] + 2. * eta * sigma[SZZ]) - 2. * glf * v[KPIZZ] / t -
                    2. * (glf * vz) * pitz / t - lambda0 * 4. / 3. * v[KPIZZ] * sum_der_t +
                    lambda1 * glf * (2. * v[KVZ] * (pitz * sum_der_0 + v[KPIXZ] * sum_der_x + v[KPIYZ] * sum_der_y + v[KPIZZ] * sum_der_z)) -
@@ -1304,6 +1313,10 @@ static int system_source(const Phys* ph, double* v, const double* dv,
       double sum_der_y = g2 * (glf * duydt + v[KVX] * duydx + v[KVY] * duydy + v[KVZ] * duydz);
       double sum_der_z = g3 * (glf * duzdt + v[KVX] * duzdx + v[KVY] * duzdy + v[KVZ] * duzdz);
       src[KPIBU] = -1. / tau_pi_big * (v[KPIBU] + zeta * sum_der) + lambda0 * (-1. / 3. * v[KPIBU] * sum_der);
+      if (kap) {
+        kap[0] = 1. / (glf * tau_pi_big);
+        kap[1] = 1. / (glf * tau_pi);
+      }
       double w0x = -0.5 * (dutdx + duxdt) + 0.5 * glf * (sum_der_x - v[KVX] * g1 * sum_der_0);
       double w0y = -0.5 * (dutdy + duydt) + 0.5 * glf * (sum_der_y - v[KVY] * g2 * sum_der_0);
       double w0z = -0.5 * (dutdz + duzdt) + 0.5 * glf * (sum_der_z - v[KVZ] * g3 * sum_der_0);
@@ -1359,6 +1372,7 @@ struct Orc {
   double *tT, *te, *tp, *tc;
   double *v, *u, *u0, *du[4], *dus[4], *w, *ax, *ay, *az, *deriv;
   double *vold, *vnewstep, *vtmp;
+  double* kap; /* imex: 2 relaxation rates per cell, from the last RHS */
   unsigned char* fail;
   double t, tout, dtout, tmax, timeold, timeinterval, dt, g3old;
   double glm_ch, glm_ch_old, aflux[3];
@@ -1428,6 +1442,7 @@ static void table_attach(Phys* ph, double** tT, double** te, double** tp,
 Orc* orc_create(const EchoParams* p, const double* eos_table, int n_eos) {
   if (p->mhd && p->viscosity) return NULL;
   if (p->mhd > 1) return NULL;
+  if (p->imex && p->nrk == ECHO_SSP) return NULL;
   Orc* e = (Orc*)calloc(1, sizeof(Orc));
   e->p = *p;
   phys_setup(&e->ph, &e->p);
@@ -1466,6 +1481,7 @@ Orc* orc_create(const EchoParams* p, const double* eos_table, int n_eos) {
   e->vnewstep = (double*)calloc(nc * e->nvold, sizeof(double));
   e->vtmp = (double*)calloc(nc * nv, sizeof(double));
   e->fail = (unsigned char*)calloc(nc, 1);
+  if (p->viscosity && p->imex) e->kap = (double*)calloc(nc * 2, sizeof(double));
   e->glm_ch_old = 0.5; /* common.f90:283 */
   e->tout = 1e300;
   e->dtout = 1e300;
@@ -1478,7 +1494,7 @@ void orc_free(Orc* e) {
   free(e->v); free(e->u); free(e->u0);
   for (int s = 0; s < 4; s++) { free(e->du[s]); free(e->dus[s]); }
   free(e->w); free(e->ax); free(e->ay); free(e->az); free(e->deriv);
-  free(e->vold); free(e->vnewstep); free(e->vtmp); free(e->fail);
+  free(e->vold); free(e->vnewstep); free(e->vtmp); free(e->fail); free(e->kap);
   free(e->tT); free(e->te); free(e->tp); free(e->tc);
   free(e->hyp_field1); free(e->hyp_field2); free(e->hyp_prim); free(e->hyp_back); free(e->hyp_out);
   free(e);
@@ -1979,7 +1995,8 @@ static int evolve_src(Orc* e, int iteration) {
     for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
     if (e->p.viscosity)
       for (int d = 0; d < NDERIV; d++) dv[d] = e->deriv[(size_t)d * nc + c];
-    int ec = system_source(&e->ph, vv, dv, src);
+    double* kap = e->kap ? e->kap + 2 * c : NULL;
+    int ec = system_source(&e->ph, vv, dv, src, kap);
     if (ec) {
       err = ec;
       break;
@@ -2228,7 +2245,18 @@ int orc_evolve_main(Orc* e, int irk, double* dt_out) {
       memcpy(e->u0, e->u, sizeof(double) * n);
     }
     double dt = e->dt, *du = e->du[0];
-    for (size_t i = 0; i < n; i++) e->u[i] = c1 * e->u0[i] + c2 * (e->u[i] - dt * du[i]);
+    size_t nimex = e->kap ? (size_t)KPIBU * e->ncell : n;
+    for (size_t i = 0; i < nimex; i++) e->u[i] = c1 * e->u0[i] + c2 * (e->u[i] - dt * du[i]);
+    /* IMEX RK2/RK3 (no reference counterpart): the relaxation -kap u of the
+       stresses taken at the new stage value, linearly implicit; the rest of
+       du stays explicit.  u_new = u_expl + c2 dt kap (u - u_new), i.e.
+       u_new = (c1 u0 + c2 (u - dt du) + c2 dt kap u) / (1 + c2 dt kap). */
+    for (size_t i = nimex; i < n; i++) {
+      size_t c = (i - nimex) % e->ncell;
+      int k = (int)((i - nimex) / e->ncell) + KPIBU;
+      double ck = c2 * dt * e->kap[2 * c + (k == KPIBU ? 0 : 1)];
+      e->u[i] = (c1 * e->u0[i] + c2 * (e->u[i] - dt * du[i]) + ck * e->u[i]) / (1. + ck);
+    }
     if (e->p.divclean && irk == e->p.nrk) glm_source(e, dt / 2.);
     if (evolve_u2v(e)) return e->errcode;
   } else {

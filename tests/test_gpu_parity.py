@@ -153,6 +153,29 @@ def test_gubser_flow_matches_oracle():
         assert rel_linf(vg, vo, 5) <= tol and rel_linf(ug, uo, 5) <= tol, exact
 
 
+@pytest.mark.parametrize("case", ["visc2d", "rmhd3d"])
+def test_eos_range_error_is_reported(case):
+    """A pressure above the EoS table in one cell: the face states around it
+    fall outside the table and the step fails with the reference's code
+    (126, get_energy, eos.f90:468-523), on the device as on the oracle."""
+    cfg = CASES[case]()
+    pc, tab, v = setup(cfg)
+    o = O.Oracle(pc, tab)
+    o.set_state(v, None, cfg.tstart)
+    v0, u0 = o.state()
+    vv = v0.reshape(cfg.nv, -1).copy()
+    vv[4, cfg.ncell // 2 + cfg.nx // 2] = 1.5 * tab[-1, 2]
+    o.set_state(vv.reshape(-1), u0, cfg.tstart)
+    with pytest.raises(RuntimeError, match="126"):
+        o.step()
+    g = Evolve(pc, tab)
+    g.upload(vv.reshape(-1), u0, cfg.tstart)
+    g.run(1)
+    g.sync()
+    st = g.stats()
+    assert st.errcode == 126 and st.err_cell >= 0
+
+
 def test_graph_run_matches_steps():
     ev, eu, _, _ = _pair(CASES["rmhd3d"](), 4, exact=True, use_run=True)
     assert ev <= 1e-13 and eu <= 1e-13
