@@ -183,7 +183,7 @@ static __global__ void batch_scalars_kernel(ScalarArgs base, BatchDev B) {
 }
 
 // cell update over the cell tiles of all live events
-template <int KIND, bool SEED>
+template <int KIND, bool SEED, bool IMEX = false>
 __global__ void ECHO_UPDATE_BOUNDS(KIND, SEED) batch_update_kernel(UpdateArgs base, BatchDev B, int nv) {
   __shared__ UpdateArgs sA;
   __shared__ int s_tile;
@@ -218,7 +218,7 @@ __global__ void ECHO_UPDATE_BOUNDS(KIND, SEED) batch_update_kernel(UpdateArgs ba
     }
     __syncthreads();
     size_t c = (size_t)s_tile * BATCH_TILE + threadIdx.x;
-    update_cell<KIND, SEED>(sA, c, c < sA.g.ncell);
+    update_cell<KIND, SEED, IMEX>(sA, c, c < sA.g.ncell);
     __syncthreads();
   }
 }

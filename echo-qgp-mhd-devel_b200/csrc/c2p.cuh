@@ -281,14 +281,165 @@ static __device__ int newton3(const DevPhys& P, const Sist3& s, double* X, doubl
 }
 
 // ---------------------------------------------------------------------------
+// Resistive MHD (MHD = 2): Ohm's law and the implicit E solve.
+// ---------------------------------------------------------------------------
+// contravariant (a x b)^i = sqrt(gamma)/g_ii [ijk] a^j b^k of contravariant a,
+// b (system_crossprod, system.f90:1867-1880, as the reference uses it in
+// Minkowski coordinates)
+__device__ __forceinline__ void cross_contra(const Metric& M, const double* a, const double* b, double* o) {
+  double gp = M.gp;
+  o[0] = gp * (a[1] * b[2] - a[2] * b[1]);
+  o[1] = gp * (a[2] * b[0] - a[0] * b[2]);
+  o[2] = gp / M.g3 * (a[0] * b[1] - a[1] * b[0]);
+}
+
+// stiff E source before the sqrt(-g) factor (system.f90:1656-1660):
+// S = -gamma [sigma (E - (E.v) v + v x B) + sigma_chi (B - (B.v) v - v x E)]
+// (B.v where the reference's Minkowski branch leaves it unset, :1750-1751)
+__device__ __forceinline__ void ohm_stiff(const DevPhys& P, const Metric& M, const double* vel, const double* B,
+                                          const double* E, double glf, double* S) {
+  double g3 = M.g3, sig = P.sigma_el, chi = P.sigma_chiral;
+  double vxb[3], vxe[3];
+  cross_contra(M, vel, B, vxb);
+  cross_contra(M, vel, E, vxe);
+  double vdotb = vel[0] * B[0] + vel[1] * B[1] + vel[2] * B[2] * g3;
+  double vdote = vel[0] * E[0] + vel[1] * E[1] + vel[2] * E[2] * g3;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+    S[i] = -glf * (sig * (E[i] - vdote * vel[i] + vxb[i]) + chi * (B[i] - vdotb * vel[i] - vxe[i]));
+}
+
+// E = Es + h S(E) for fixed v and B, linear in E:
+// [(1 + lam) I - lam v v_cov - mu (v x .)] E = Es - lam v x B - mu (B - (B.v) v),
+// lam = h gamma sigma, mu = h gamma sigma_chi; solved by cofactors
+__device__ __forceinline__ void ohm_solve(const DevPhys& P, const Metric& M, const double* Es, const double* vel,
+                                          const double* B, double h, double* E) {
+  double g3 = M.g3, gp = M.gp, gq = M.gp / M.g3;
+  double v2 = vel[0] * vel[0] + vel[1] * vel[1] + g3 * (vel[2] * vel[2]);
+  double glf = 1. / sqrt(1. - v2);
+  double lam = h * glf * P.sigma_el, mu = h * glf * P.sigma_chiral;
+  double vxb[3];
+  cross_contra(M, vel, B, vxb);
+  double vdotb = vel[0] * B[0] + vel[1] * B[1] + vel[2] * B[2] * g3;
+  double vc[3] = {vel[0], vel[1], g3 * vel[2]};
+  double C[3][3] = {{0., -gp * vel[2], gp * vel[1]}, {gp * vel[2], 0., -gp * vel[0]}, {-gq * vel[1], gq * vel[0], 0.}};
+  double r[3], Mx[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    r[i] = Es[i] - lam * vxb[i] - mu * (B[i] - vdotb * vel[i]);
+#pragma unroll
+    for (int j = 0; j < 3; j++) Mx[i][j] = (i == j ? 1. + lam : 0.) - lam * vel[i] * vc[j] - mu * C[i][j];
+  }
+  double c00 = Mx[1][1] * Mx[2][2] - Mx[1][2] * Mx[2][1];
+  double c01 = Mx[1][2] * Mx[2][0] - Mx[1][0] * Mx[2][2];
+  double c02 = Mx[1][0] * Mx[2][1] - Mx[1][1] * Mx[2][0];
+  double c10 = Mx[0][2] * Mx[2][1] - Mx[0][1] * Mx[2][2];
+  double c11 = Mx[0][0] * Mx[2][2] - Mx[0][2] * Mx[2][0];
+  double c12 = Mx[0][1] * Mx[2][0] - Mx[0][0] * Mx[2][1];
+  double c20 = Mx[0][1] * Mx[1][2] - Mx[0][2] * Mx[1][1];
+  double c21 = Mx[0][2] * Mx[1][0] - Mx[0][0] * Mx[1][2];
+  double c22 = Mx[0][0] * Mx[1][1] - Mx[0][1] * Mx[1][0];
+  double det = Mx[0][0] * c00 + Mx[0][1] * c01 + Mx[0][2] * c02;
+  E[0] = (c00 * r[0] + c10 * r[1] + c20 * r[2]) / det;
+  E[1] = (c01 * r[0] + c11 * r[1] + c21 * r[2]) / det;
+  E[2] = (c02 * r[0] + c12 * r[1] + c22 * r[2]) / det;
+}
+
+// Resistive con2prim with the implicit Ohm's law of an IMEX stage (the
+// algo_solver 7 the reference names, common.f90:292-293, 2109-2113, but has
+// no branch for, system.f90:1160-1162).  h = a_ii dt of the stage (0: plain
+// inversion).  Fixed point on v: E(v) from ohm_solve; the fluid's share
+// S - E x B, U - (E^2 + B^2)/2; the ideal-HD Newton on p (system.f90:511-561)
+// for p and the new v; until max |dv| <= 1e-14 (one pass for h = 0), 779
+// after 200 passes.  v[KEX..KEZ] receives E and, when h > 0, u[KEX..KEZ]
+// sqrt(-g) E: the implicit solve changes the conserved E.
+inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u, double* v, int* iters,
+                                    double h) {
+  const double ntol = 1.e-12, vtol = 1.e-14;
+  double g1 = M.g1, g2 = M.g2, g3 = M.g3, gm = M.gm, gp = M.gp;
+  double d = gm * u[KRH], U = gm * u[KPR];
+  double S[3] = {gm * u[KVX], gm * u[KVY], gm * u[KVZ]};
+  double B[3] = {gm * u[KBX], gm * u[KBY], gm * u[KBZ]};
+  double Es[3] = {gm * u[KEX], gm * u[KEY], gm * u[KEZ]};
+  double vel[3] = {v[KVX], v[KVY], v[KVZ]}, E[3];
+  double pr = v[KPR], rh = v[KRH];
+  double B2 = B[0] * B[0] + B[1] * B[1] + (B[2] * B[2]) * g3;
+  int errcode = 0, outer, total = 0;
+  for (outer = 1; outer <= 200; outer++) {
+    if (h > 0.) {
+      ohm_solve(P, M, Es, vel, B, h, E);
+    } else {
+      E[0] = Es[0];
+      E[1] = Es[1];
+      E[2] = Es[2];
+    }
+    double Ec[3] = {E[0], E[1], E[2] * g3}, EXB[3];
+    exb(M, Ec, B[0], B[1], B[2], EXB);
+    double E2 = Ec[0] * Ec[0] + Ec[1] * Ec[1] + (Ec[2] * Ec[2]) / g3;
+    double sx = S[0] - EXB[0], sy = S[1] - EXB[1], sz = (S[2] - EXB[2]) / g3;
+    double et = U - 0.5 * (E2 + B2);
+    double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
+    double w = 0, v2, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    int iter;
+    for (iter = 1; iter <= 100; iter++) {
+      w = et + pr;
+      v2 = s2 / (w * w);
+      if (v2 >= 1.) {
+        *iters = total + iter;
+        return 777;
+      }
+      glf = 1. / sqrt(1. - v2);
+      rh = d / glf;
+      en = w * (1. - v2) - pr;
+      drhdpr = rh * v2 * glf / (en + pr);
+      dendpr = v2;
+      errcode = eos_pressure(P, rh, en, &pr_eos, &dprdrh, &dprden);
+      f = pr_eos - pr;
+      df = dprdrh * drhdpr + dprden * dendpr - 1.;
+      dpr = -f / df;
+      if (fabs(dpr) < ntol * pr) break;
+      pr = pr + dpr;
+    }
+    total += iter;
+    double vn0 = sx / w, vn1 = sy / w, vn2 = sz / w;
+    double dv = fmax3(fabs(vn0 - vel[0]), fabs(vn1 - vel[1]), fabs(vn2 - vel[2]) * gp);
+    vel[0] = vn0;
+    vel[1] = vn1;
+    vel[2] = vn2;
+    if (!(h > 0.) || dv <= vtol) break;
+  }
+  *iters = total;
+  if (outer > 200) return 779;
+  v[KRH] = rh;
+  v[KVX] = vel[0];
+  v[KVY] = vel[1];
+  v[KVZ] = vel[2];
+  v[KPR] = pr;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    v[KBX + i] = B[i];
+    v[KEX + i] = E[i];
+    if (h > 0.) u[KEX + i] = E[i] * gp;
+  }
+  v[Traits<KIND_RES>::KG] = u[Traits<KIND_RES>::KG];
+  if (pr <= 0) errcode = 777;
+  return errcode;
+}
+
+// ---------------------------------------------------------------------------
 // system_cons2prim (system.f90:423-1166).  u, v of length NV; v holds the
 // initial guess.  Returns the reference errcode; *iters gets the iteration
-// count (Newton steps, or BRENTM function evaluations).
+// count (Newton steps, or BRENTM function evaluations).  h: the implicit
+// coefficient of a resistive IMEX stage (cons2prim_res).
 // ---------------------------------------------------------------------------
 template <int KIND>
 __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol, const double* u,
-                         double* v, int* iters, const float* seed = nullptr, int* seed_failed = nullptr) {
+                         double* v, int* iters, const float* seed = nullptr, int* seed_failed = nullptr,
+                         double h = 0.) {
   typedef Traits<KIND> T;
+  // every resistive caller passes its own copy of u, which the implicit
+  // solve updates (the reference's con2prim may modify u, evolve.f90:848)
+  if (T::RES) return cons2prim_res(P, M, const_cast<double*>(u), v, iters, h);
   const double eps = 1.e-12;
   const double ntol = 1.e-12;
   double g1 = M.g1, g2 = M.g2, g3 = M.g3, gm = M.gm;
@@ -479,7 +630,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     v[KVY] = vy;
     v[KVZ] = vz;
     v[KPR] = pr;
-    if (T::GLM) v[KGLM] = u[KGLM];
+    if (T::GLM) v[T::KG] = u[T::KG];
     return errcode;
   }
 }
@@ -556,7 +707,7 @@ __device__ __forceinline__ void get_sigma(const DevPhys& P, const Metric& M, con
 // ---------------------------------------------------------------------------
 template <int KIND>
 __device__ int system_source(const DevPhys& P, const Metric& M, double* v, const double* dv, double* src,
-                             double* kap = nullptr) {
+                             double* kap = nullptr, double rhoC = 0., double* stiff = nullptr) {
   typedef Traits<KIND> T;
   double g1 = M.g1, g2 = M.g2, g3 = M.g3, gp = M.gp, g0 = M.g0, t = M.t;
 #pragma unroll
@@ -575,7 +726,8 @@ __device__ int system_source(const DevPhys& P, const Metric& M, double* v, const
       double ww = w * (glf * glf);
       if (T::MHD) {
         double E[3];
-        e_ideal(M, vx, vy, vz, v[KBX], v[KBY], v[KBZ], E);
+        e_field<KIND>(M, v, E);  // the reference takes -v x B here also for
+                                 // resistive runs (system.f90:1641)
         double bx = v[KBX], by = v[KBY], bz = v[KBZ];
         double B2 = bx * bx + by * by + (bz * bz) * g3;
         double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
@@ -694,6 +846,17 @@ __device__ int system_source(const DevPhys& P, const Metric& M, double* v, const
     if (kap) {
       kap[0] = 1. / (glf * tau_pi_big);
       kap[1] = 1. / (glf * tau_pi);
+    }
+  }
+  if (T::RES) {
+    // charge current and Ohm's law (system.f90:1650-1661, 1747-1756);
+    // stiff: the three E components, times sqrt(-g)
+    double vel[3] = {vx, vy, vz}, S[3];
+    ohm_stiff(P, M, vel, v + KBX, v + KEX, glf, S);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      src[KEX + i] = -rhoC * vel[i];
+      if (stiff) stiff[i] = S[i] * gp;
     }
   }
 #pragma unroll

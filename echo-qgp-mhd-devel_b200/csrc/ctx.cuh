@@ -36,6 +36,7 @@ struct EchoCtx {
   int* d_bk;                // EoS bracket accelerators
   double* d_du;             // scratch for echo_gpu_rhs
   double* d_dussp[4];       // IMEX-SSP stage right-hand sides du(:,:,:,:,1..4)
+  double* d_dss[4];         // resistive IMEX-SSP: stiff E right-hand sides, 3 x ncell
   unsigned* d_mlp_frag;     // learned con2prim seed: BF16 weight fragments
   float* d_mlp_par;         //   biases and normalisation
   unsigned char* d_fail;
@@ -84,5 +85,7 @@ template <int KIND>
 void launch_p2c(EchoCtx* c);
 template <int KIND>
 void launch_ssp_combine(EchoCtx* c, int stage);
+template <int KIND>
+void launch_ssp_stage1(EchoCtx* c);
 
 }  // namespace echo

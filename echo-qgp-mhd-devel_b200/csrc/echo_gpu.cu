@@ -48,12 +48,14 @@ bool echo_make_buckets(const double* arr, int n, std::vector<int>& bk, long long
 
 int echo_kind_of(const EchoParams* p) {
   if (p->viscosity) return KIND_VISC;
+  if (p->mhd == 2) return KIND_RES;
   if (p->mhd) return p->divclean ? KIND_MHDGLM : KIND_MHD;
   return KIND_HD;
 }
 int echo_nv_of(int kind) {
   switch (kind) {
     case KIND_VISC: return 12;
+    case KIND_RES: return 12;
     case KIND_MHD: return 8;
     case KIND_MHDGLM: return 9;
     default: return 5;
@@ -117,6 +119,8 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
   P->enezero = p->enezero;
   P->przero = p->przero;
   P->glm_alpha = p->glm_alpha;
+  P->sigma_el = p->sigma_el;
+  P->sigma_chiral = p->sigma_chiral;
   P->bke = P->bkp = nullptr;
   P->sl_ep = P->sl_ce = P->sl_pe = nullptr;
   *d_bk = nullptr;
@@ -153,6 +157,7 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
       case KIND_HD: fn<KIND_HD>(__VA_ARGS__); break;              \
       case KIND_VISC: fn<KIND_VISC>(__VA_ARGS__); break;          \
       case KIND_MHD: fn<KIND_MHD>(__VA_ARGS__); break;            \
+      case KIND_RES: fn<KIND_RES>(__VA_ARGS__); break;            \
       default: fn<KIND_MHDGLM>(__VA_ARGS__); break;               \
     }                                                             \
   } while (0)
@@ -205,6 +210,10 @@ static void enqueue_stage_ssp(EchoCtx* c, int irk) {
   mark(c, PK_SCALARS);
   DISPATCH(c, launch_update, c, irk, MODE_RHS, c->d_dussp[irk - 1]);
   mark(c, PK_UPDATE);
+  if (irk == 1 && c->kind == KIND_RES) {
+    DISPATCH(c, launch_ssp_stage1, c);
+    mark(c, PK_UPDATE);
+  }
   if (irk == 4) {
     cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
     DISPATCH(c, launch_ssp_combine, c, 5);
@@ -280,8 +289,12 @@ int echo_gpu_nv(const EchoCtx* c) { return c ? c->nv : 0; }
 int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoCtx** out) {
   if (!p || !out) return ECHO_ERR_ARG;
   *out = nullptr;
-  if (p->mhd > 1 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
+  if (p->mhd > 2 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
   if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3 && p->nrk != ECHO_SSP) return ECHO_ERR_UNSUPPORTED;
+  // resistive runs: IMEX-SSP (common.f90:2114-2118), with GLM cleaning, the
+  // plain inversion (no learned seed for the resistive equations)
+  if (p->mhd == 2 && (p->nrk != ECHO_SSP || !p->divclean || p->algo_solver == ECHO_C2P_MLP))
+    return ECHO_ERR_UNSUPPORTED;
   if (p->imex != 0 && p->imex != 1) return ECHO_ERR_ARG;
   if (p->imex && p->nrk == ECHO_SSP) return ECHO_ERR_UNSUPPORTED;  // IMEX RK2/RK3 only
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return ECHO_ERR_ARG;
@@ -328,7 +341,12 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   }
   for (int q = 0; q < 4; q++) {
     c->d_dussp[q] = nullptr;
+    c->d_dss[q] = nullptr;
     if (p->nrk == ECHO_SSP) CK(cudaMalloc(&c->d_dussp[q], sizeof(double) * nvc));
+    if (c->kind == KIND_RES) {
+      CK(cudaMalloc(&c->d_dss[q], sizeof(double) * 3 * c->g.ncell));
+      CK(cudaMemset(c->d_dss[q], 0, sizeof(double) * 3 * c->g.ncell));
+    }
   }
   CK(cudaMalloc(&c->d_fail, c->g.ncell));
   CK(cudaMemset(c->d_fail, 0, c->g.ncell));
@@ -362,7 +380,10 @@ int echo_gpu_free(EchoCtx* c) {
     cudaFree(c->d_F[d]);
     cudaFree(c->d_WD[d]);
   }
-  for (int q = 0; q < 4; q++) cudaFree(c->d_dussp[q]);
+  for (int q = 0; q < 4; q++) {
+    cudaFree(c->d_dussp[q]);
+    cudaFree(c->d_dss[q]);
+  }
   cudaFree(c->d_fail);
   cudaFree(c->d_sc);
   cudaFree(c->d_tab);

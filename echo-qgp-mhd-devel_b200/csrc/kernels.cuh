@@ -332,9 +332,9 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
     if (T::GLM) {
       const int kb = DIR == 0 ? KBX : DIR == 1 ? KBY : KBZ;
       double ch = A.sc->glm_ch_old;
-      wl[KGLM] = 0.5 * (wl[KGLM] + wr[KGLM]) - (wr[kb] - wl[kb]) * ch / 2;
-      wr[KGLM] = wl[KGLM];
-      wl[kb] = 0.5 * (wl[kb] + wr[kb]) - (wr[KGLM] - wl[KGLM]) / (2 * ch);
+      wl[T::KG] = 0.5 * (wl[T::KG] + wr[T::KG]) - (wr[kb] - wl[kb]) * ch / 2;
+      wr[T::KG] = wl[T::KG];
+      wl[kb] = 0.5 * (wl[kb] + wr[kb]) - (wr[T::KG] - wl[T::KG]) / (2 * ch);
       wr[kb] = wl[kb];
     }
     // HLL (work.f90:195-229)
@@ -523,8 +523,11 @@ struct UpdateArgs {
   DevScalars* sc;
   double c1, c2;
   int irk, nrk, divclean, coordinates, algo, mode;
-  int imex;  // viscous: relaxation of the stresses linearly implicit per stage
   double tol;
+  // resistive runs: stiff right-hand side of E (MODE_RHS, 3 x ncell) and the
+  // boundary codes of E^x, E^y, E^eta along x, y, eta for the charge density
+  double* dus_out;
+  signed char ebc[3][2];
   MlpDev mlp;  // learned seed (algo == ECHO_C2P_MLP)
   // viscous, stage 1 of a batched step: vnewstep = v (echo.f90:192-202) is
   // taken here, per cell, instead of by a separate copy; null otherwise
@@ -554,7 +557,7 @@ __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, boo
 // con2prim).  Called by every thread of a warp together (the learned seed
 // and the counters are warp-collective); threads without a cell pass
 // active = false.
-template <int KIND, bool SEED>
+template <int KIND, bool SEED, bool IMEX = false>
 __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool active) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
@@ -640,11 +643,38 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
         dv[DZT] = (gamma2 * vz - gamma1 * vzo) / ti;
       }
     }
+    // resistive: charge density d_i E^i by central differences with the
+    // ghost fill (system_compute_divE, system.f90:1901-1919)
+    double rhoC = 0., stiff[3] = {0., 0., 0.};
+    if (T::RES) {
+      if (g.nx > 1) {
+        const double* a = A.vin + (size_t)KEX * g.ncell;
+        double dx = 2. / g.ddx;
+        rhoC = rhoC + (ghost_val(a, c - ix, 1, g.nx, ix + 2, A.ebc[0][0], A.ebc[0][1]) -
+                       ghost_val(a, c - ix, 1, g.nx, ix, A.ebc[0][0], A.ebc[0][1])) / dx;
+      }
+      if (g.ny > 1) {
+        const double* a = A.vin + (size_t)KEY * g.ncell;
+        size_t base = c - (size_t)iy * g.nx;
+        double dy = 2. / g.ddy;
+        rhoC = rhoC + (ghost_val(a, base, g.nx, g.ny, iy + 2, A.ebc[1][0], A.ebc[1][1]) -
+                       ghost_val(a, base, g.nx, g.ny, iy, A.ebc[1][0], A.ebc[1][1])) / dy;
+      }
+      if (g.nz > 1) {
+        const double* a = A.vin + (size_t)KEZ * g.ncell;
+        long long nxy = (long long)g.nx * g.ny;
+        size_t base = c - (size_t)iz * (size_t)nxy;
+        double dz = 2. / g.ddz;
+        rhoC = rhoC + (ghost_val(a, base, nxy, g.nz, iz + 2, A.ebc[2][0], A.ebc[2][1]) -
+                       ghost_val(a, base, nxy, g.nz, iz, A.ebc[2][0], A.ebc[2][1])) / dz;
+      }
+    }
     {
       double vs[NV];
 #pragma unroll
       for (int k = 0; k < NV; k++) vs[k] = vv[k];
-      int err = system_source<KIND>(A.P, M, vs, dv, src, T::VISC ? kap : nullptr);
+      int err = system_source<KIND>(A.P, M, vs, dv, src, (T::VISC && IMEX) ? kap : nullptr, rhoC,
+                                    T::RES ? stiff : nullptr);
       if (err) atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
     }
 #pragma unroll
@@ -652,18 +682,22 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
     if (A.mode == MODE_RHS) {
 #pragma unroll
       for (int k = 0; k < NV; k++) A.du_out[(size_t)k * g.ncell + c] = du[k];
+      if (T::RES && A.dus_out) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) A.dus_out[(size_t)i * g.ncell + c] = 0. - stiff[i];
+      }
     } else {
       // RK combination (evolve.f90:196-201)
       const double dt = A.sc->dt;
 #pragma unroll
       for (int k = 0; k < NV; k++) {
         double ui = A.uin[(size_t)k * g.ncell + c];
-        if (T::GLM && k == KGLM && A.irk == 1) {
+        if (T::GLM && k == T::KG && A.irk == 1) {
           ui = ui * A.sc->expfact;
           A.uin[(size_t)k * g.ncell + c] = ui;  // u0 = u after the GLM half step
         }
         double u0 = A.irk == 1 ? ui : A.u0[(size_t)k * g.ncell + c];
-        if (T::VISC && k >= KPIBU && A.imex) {
+        if (T::VISC && IMEX && k >= KPIBU) {
           // IMEX RK2/RK3: the relaxation -kap u of the stresses at the new
           // stage value, u_new = u_expl + c2 dt kap (u - u_new)
           double ck = A.c2 * dt * (k == KPIBU ? kap[0] : kap[1]);
@@ -672,7 +706,7 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
           uu[k] = A.c1 * u0 + A.c2 * (ui - dt * du[k]);
         }
       }
-      if (T::GLM && A.irk == A.nrk) uu[KGLM] = uu[KGLM] * A.sc->expfact;
+      if (T::GLM && A.irk == A.nrk) uu[T::KG] = uu[T::KG] * A.sc->expfact;
 #pragma unroll
       for (int k = 0; k < NV; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
     }
@@ -711,10 +745,10 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
   }
 }
 
-template <int KIND, bool SEED>
+template <int KIND, bool SEED, bool IMEX = false>
 __global__ void ECHO_UPDATE_BOUNDS(KIND, SEED) update_kernel(UpdateArgs A) {
   size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  update_cell<KIND, SEED>(A, c, c < A.g.ncell);
+  update_cell<KIND, SEED, IMEX>(A, c, c < A.g.ncell);
 }
 
 // ---------------------------------------------------------------------------
@@ -730,6 +764,13 @@ struct SspArgs {
   const double* __restrict__ du2;
   const double* __restrict__ du3;
   const double* __restrict__ du4;
+  // resistive runs: the stiff right-hand sides of E of stages 1..4 (3 x ncell
+  // each; null otherwise); stage 1 (ssp_stage1_kernel) writes ds1
+  const double* __restrict__ ds1;
+  const double* __restrict__ ds2;
+  const double* __restrict__ ds3;
+  const double* __restrict__ ds4;
+  double* ds_out;
   double* __restrict__ uout;
   const double* __restrict__ vin;
   double* __restrict__ vout;
@@ -753,24 +794,33 @@ __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
   const bool active = c < g.ncell;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
   double uu[NV], vv[NV];
+  const double dt = A.sc->dt;
   if (active) {
-    const double dt = A.sc->dt, ds = 0.0;
 #pragma unroll
     for (int k = 0; k < NV; k++) {
       size_t i = (size_t)k * g.ncell + c;
       double u0 = A.u0[i];
+      // stiff right-hand sides: zero but for E of resistive runs
+      double s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
+      if (T::RES && k >= KEX && k <= KEZ) {
+        size_t j = (size_t)(k - KEX) * g.ncell + c;
+        if (A.stage == 2 || A.stage == 4) s1 = A.ds1[j];
+        if (A.stage >= 3) s2 = A.ds2[j];
+        if (A.stage >= 4) s3 = A.ds3[j];
+        if (A.stage == 5) s4 = A.ds4[j];
+      }
       if (A.stage == 2) {
-        uu[k] = u0 + dt * alpha_imex * ds;
+        uu[k] = u0 + dt * alpha_imex * s1;
       } else if (A.stage == 3) {
-        uu[k] = u0 - dt * (A.du2[i] + (1. - alpha_imex) * ds);
+        uu[k] = u0 - dt * (A.du2[i] + (1. - alpha_imex) * s2);
       } else if (A.stage == 4) {
-        uu[k] = u0 - dt * (A.du2[i] / 4. + A.du3[i] / 4. + beta_imex * ds + eta_imex * ds + delta_imex * ds);
+        uu[k] = u0 - dt * (A.du2[i] / 4. + A.du3[i] / 4. + beta_imex * s1 + eta_imex * s2 + delta_imex * s3);
       } else {
-        uu[k] = u0 - dt * (A.du2[i] / 6. + A.du3[i] / 6. + A.du4[i] * 2. / 3. + ds / 6. + ds / 6. + ds * 2. / 3.);
+        uu[k] = u0 - dt * (A.du2[i] / 6. + A.du3[i] / 6. + A.du4[i] * 2. / 3. + s2 / 6. + s3 / 6. + s4 * 2. / 3.);
       }
       vv[k] = A.vin[i];
     }
-    if (T::GLM && A.stage == 5) uu[KGLM] = uu[KGLM] * A.sc->expfact;
+    if (T::GLM && A.stage == 5) uu[T::KG] = uu[T::KG] * A.sc->expfact;
 #pragma unroll
     for (int k = 0; k < NV; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
   }
@@ -782,7 +832,9 @@ __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
   }
   if (active) {
     int it = 0;
-    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp);
+    // the implicit stages of a resistive run solve Ohm's law in con2prim
+    const double h = (T::RES && A.stage < 5) ? alpha_imex * dt : 0.;
+    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, nullptr, h);
     my_iters = (unsigned long long)it;
     if (err) {
       A.fail[c] = 1;
@@ -791,11 +843,48 @@ __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
       A.fail[c] = 0;
 #pragma unroll
       for (int k = 0; k < NV; k++) A.vout[(size_t)k * g.ncell + c] = vv[k];
+      if (T::RES && h > 0.) {
+#pragma unroll
+        for (int k = KEX; k <= KEZ; k++) A.uout[(size_t)k * g.ncell + c] = uu[k];
+      }
     }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
   if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
+}
+
+// Resistive IMEX-SSP3(4,3,3), first stage: U1 = u^n + alpha dt S(U1), solved
+// from u0 = u^n cell by cell (the implicit stage the reference leaves to its
+// missing algo-7 con2prim); ds_out = -S(U1), the stiff E right-hand side the
+// later stages combine (only S(U1) enters them: F(U1) has weight 0).  v and
+// u stay at step n; a failed solve stops the run with its code.
+template <int KIND>
+__global__ void __launch_bounds__(128) ssp_stage1_kernel(SspArgs A) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  const double alpha_imex = 0.24169426078821;
+  const Grid& g = A.g;
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!T::RES || c >= g.ncell) return;
+  const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  double uu[NV], vv[NV], S[3];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    uu[k] = A.u0[(size_t)k * g.ncell + c];
+    vv[k] = A.vin[(size_t)k * g.ncell + c];
+  }
+  int it = 0;
+  int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, alpha_imex * A.sc->dt);
+  if (err) {
+    atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
+    return;
+  }
+  double v2 = M.g1 * vv[KVX] * vv[KVX] + M.g2 * vv[KVY] * vv[KVY] + M.g3 * vv[KVZ] * vv[KVZ];
+  double glf = 1. / sqrt(1. - v2);
+  ohm_stiff(A.P, M, vv + KVX, vv + KBX, vv + KEX, glf, S);
+#pragma unroll
+  for (int i = 0; i < 3; i++) A.ds_out[(size_t)i * g.ncell + c] = 0. - S[i] * M.gp;
 }
 
 // ---------------------------------------------------------------------------
@@ -811,6 +900,7 @@ struct RepairArgs {
   DevScalars* sc;
   int coordinates, algo;
   double maxspeed, tol;
+  double h_alpha;  // resistive implicit stages: a_ii, the solve uses h = a_ii dt
 };
 
 template <int KIND>
@@ -833,6 +923,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
   const int NV = T::NV;
   const Grid& g = A.g;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  const double h = A.h_alpha * A.sc->dt;
   if (threadIdx.x == 0) s_stop = 0;
   for (size_t chunk = 0; chunk < g.ncell; chunk += blockDim.x) {
     size_t c = chunk + threadIdx.x;
@@ -853,7 +944,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
         int it;
         for (int k = 0; k < NV; k++) vv[k] = A.vold[(size_t)k * g.ncell + cell];
         for (int k = 0; k < NV; k++) uu[k] = A.u[(size_t)k * g.ncell + cell];
-        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
         size_t totu = g.ncell * NV;
         long long nx = g.nx, nxy = (long long)g.nx * g.ny;
         for (int k = 0; k < NV; k++) {
@@ -863,7 +954,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
           A.u[o] = s / 6.;
           uu[k] = A.u[o];
         }
-        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
         double v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
         if (v2 > 1) {
           double fac = A.maxspeed / sqrt(v2);
@@ -879,7 +970,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
           vv[KPR] = (pxl + pxr + pyl + pyr + pzl + pzr) / 6.;
         }
         (void)prim2cons<KIND>(A.P, M, vv, uu);
-        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it);
+        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
         v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
         bool ok = (vv[KPR] > 0) && (v2 < 1);
         if (T::VISC && A.P.obtained_zz) A.vnew[(size_t)KPIZZ * g.ncell + cell] = vv[KPIZZ];

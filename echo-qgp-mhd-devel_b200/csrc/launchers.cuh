@@ -67,8 +67,14 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   A.coordinates = c->p.coordinates;
   A.algo = c->p.algo_solver;
   A.mode = mode;
-  A.imex = c->p.imex;
   A.tol = c->p.c2p_tol;
+  A.dus_out = nullptr;
+  if (Traits<KIND>::RES) {
+    if (mode == MODE_RHS) A.dus_out = c->d_dss[irk - 1];
+    const int ke[3] = {KEX, KEY, KEZ};
+    for (int d = 0; d < 3; d++)
+      for (int q = 0; q < 2; q++) A.ebc[d][q] = c->bc[d].c[ke[d]][q];
+  }
   A.mlp.frag = c->d_mlp_frag;
   A.mlp.par = c->d_mlp_par;
   A.vsnap = nullptr;
@@ -76,6 +82,8 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
   if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP && mode == MODE_RK)
     update_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
+  else if (Traits<KIND>::VISC && c->p.imex && mode == MODE_RK)
+    update_kernel<KIND, false, Traits<KIND>::VISC><<<blocks, 128, 0, c->stream>>>(A);
   else
     update_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
 }
@@ -94,6 +102,9 @@ void launch_repair_smooth(EchoCtx* c, int what) {
   R.algo = c->p.algo_solver;
   R.maxspeed = c->p.maxspeed;
   R.tol = c->p.c2p_tol;
+  // the con2prim of the implicit stages 2..4 (what == 1) of a resistive run
+  // solves Ohm's law, the repair's too
+  R.h_alpha = (Traits<KIND>::RES && what == 1) ? 0.24169426078821 : 0.;
   if (what & 1) repair_kernel<KIND><<<1, 256, 0, c->stream>>>(R);
   if ((what & 2) && KIND == KIND_VISC && c->p.enable_smooth_viscosity) {
     SmoothArgs S;
@@ -129,6 +140,11 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
   A.du2 = c->d_dussp[1];
   A.du3 = c->d_dussp[2];
   A.du4 = c->d_dussp[3];
+  A.ds1 = c->d_dss[0];
+  A.ds2 = c->d_dss[1];
+  A.ds3 = c->d_dss[2];
+  A.ds4 = c->d_dss[3];
+  A.ds_out = nullptr;
   A.uout = c->d_u[c->ucur];
   A.vin = c->d_v[c->vcur];
   A.vout = c->d_v[1 - c->vcur];
@@ -143,10 +159,42 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
   A.mlp.par = c->d_mlp_par;
   if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP)
+  if (Traits<KIND>::MHD && !Traits<KIND>::RES && A.algo == ECHO_C2P_MLP)
     ssp_combine_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
   else
     ssp_combine_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
+}
+
+// resistive IMEX-SSP first stage: the implicit solve from u^n (U[ucur]) and
+// the stiff E right-hand side of stage 1
+template <int KIND>
+void launch_ssp_stage1(EchoCtx* c) {
+  if constexpr (!Traits<KIND>::RES) {
+    (void)c;
+    return;
+  } else {
+  SspArgs A;
+  A.P = c->P;
+  A.g = c->g;
+  A.u0 = c->d_u[c->ucur];
+  A.du1 = A.du2 = A.du3 = A.du4 = nullptr;
+  A.ds1 = A.ds2 = A.ds3 = A.ds4 = nullptr;
+  A.ds_out = c->d_dss[0];
+  A.uout = nullptr;
+  A.vin = c->d_v[c->vcur];
+  A.vout = nullptr;
+  A.fail = c->d_fail;
+  A.sc = c->d_sc;
+  A.stage = 1;
+  A.coordinates = c->p.coordinates;
+  A.algo = c->p.algo_solver;
+  A.divclean = c->p.divclean;
+  A.tol = c->p.c2p_tol;
+  A.mlp.frag = nullptr;
+  A.mlp.par = nullptr;
+  unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
+  ssp_stage1_kernel<KIND><<<blocks, 128, 0, c->stream>>>(A);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -212,11 +260,14 @@ void launch_batch_update(EchoBatch* b, int irk) {
   A.coordinates = b->p.coordinates;
   A.algo = b->p.algo_solver;
   A.mode = MODE_RK;
-  A.imex = b->p.imex;
   A.tol = b->p.c2p_tol;
   A.mlp.frag = nullptr;
   A.mlp.par = nullptr;
-  batch_update_kernel<KIND, false><<<batch_grid(b, SL_UPDATE, PH_CELL), 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+  if (Traits<KIND>::VISC && b->p.imex)
+    batch_update_kernel<KIND, false, Traits<KIND>::VISC>
+        <<<batch_grid(b, SL_UPDATE, PH_CELL), 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+  else
+    batch_update_kernel<KIND, false><<<batch_grid(b, SL_UPDATE, PH_CELL), 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
 }
 
 template <int KIND>
@@ -271,12 +322,16 @@ void batch_occupancy(const EchoBatch* b, int* per_sm) {
 
 }  // namespace echo
 
-#define ECHO_INSTANTIATE(K)                                                   \
+#define ECHO_INSTANTIATE_GRID(K)                                              \
   template void echo::launch_faces<K>(EchoCtx*, int);                         \
   template void echo::launch_update<K>(EchoCtx*, int, int, double*);          \
-  template void echo::launch_repair_smooth<K>(EchoCtx*, int);                      \
+  template void echo::launch_repair_smooth<K>(EchoCtx*, int);                 \
   template void echo::launch_p2c<K>(EchoCtx*);                                \
   template void echo::launch_ssp_combine<K>(EchoCtx*, int);                   \
+  template void echo::launch_ssp_stage1<K>(EchoCtx*);
+
+#define ECHO_INSTANTIATE(K)                                                   \
+  ECHO_INSTANTIATE_GRID(K)                                                    \
   template void echo::launch_batch_faces<K>(EchoBatch*, int);                 \
   template void echo::launch_batch_update<K>(EchoBatch*, int);                \
   template void echo::launch_batch_repair_smooth<K>(EchoBatch*);              \

@@ -10,6 +10,7 @@
 //   KIND_VISC    Israel-Stewart viscous hydro, nv = 12
 //   KIND_MHD     ideal MHD, nv = 8
 //   KIND_MHDGLM  ideal MHD with GLM divergence cleaning, nv = 9
+//   KIND_RES     resistive MHD (E a primitive) with GLM, nv = 12
 #pragma once
 
 #include <cstdint>
@@ -19,35 +20,42 @@
 
 namespace echo {
 
-enum { KIND_HD = 0, KIND_VISC = 1, KIND_MHD = 2, KIND_MHDGLM = 3 };
+enum { KIND_HD = 0, KIND_VISC = 1, KIND_MHD = 2, KIND_MHDGLM = 3, KIND_RES = 4 };
 
 template <int KIND>
 struct Traits;
 template <>
 struct Traits<KIND_HD> {
-  static constexpr int NV = 5;
-  static constexpr bool MHD = false, VISC = false, GLM = false;
+  static constexpr int NV = 5, KG = -1;
+  static constexpr bool MHD = false, VISC = false, GLM = false, RES = false;
 };
 template <>
 struct Traits<KIND_VISC> {
-  static constexpr int NV = 12;
-  static constexpr bool MHD = false, VISC = true, GLM = false;
+  static constexpr int NV = 12, KG = -1;
+  static constexpr bool MHD = false, VISC = true, GLM = false, RES = false;
 };
 template <>
 struct Traits<KIND_MHD> {
-  static constexpr int NV = 8;
-  static constexpr bool MHD = true, VISC = false, GLM = false;
+  static constexpr int NV = 8, KG = -1;
+  static constexpr bool MHD = true, VISC = false, GLM = false, RES = false;
 };
 template <>
 struct Traits<KIND_MHDGLM> {
-  static constexpr int NV = 9;
-  static constexpr bool MHD = true, VISC = false, GLM = true;
+  static constexpr int NV = 9, KG = 8;
+  static constexpr bool MHD = true, VISC = false, GLM = true, RES = false;
+};
+// resistive runs (MHD = 2): B, E, psi (system.f90:92-105, 113-116)
+template <>
+struct Traits<KIND_RES> {
+  static constexpr int NV = 12, KG = 11;
+  static constexpr bool MHD = true, VISC = false, GLM = true, RES = true;
 };
 
 // variable indices (common.f90:63), 0-based
 enum { KRH = 0, KVX = 1, KVY = 2, KVZ = 3, KPR = 4, KPIBU = 5, KPIXY = 6, KPIXZ = 7,
        KPIYZ = 8, KPIXX = 9, KPIYY = 10, KPIZZ = 11 };
-enum { KBX = 5, KBY = 6, KBZ = 7, KGLM = 8 };
+enum { KBX = 5, KBY = 6, KBZ = 7, KGLM = 8 };  // KGLM: ideal MHD; Traits<K>::KG in general
+enum { KEX = 8, KEY = 9, KEZ = 10 };              // resistive E^i
 // derivative indices (common.f90:70-71), 0-based
 enum { DTX = 0, DTY, DTZ, DXX, DXY, DXZ, DYX, DYY, DYZ, DZX, DZY, DZZ, DTT, DXT, DYT, DZT, NDER = 16 };
 
@@ -70,6 +78,7 @@ struct DevPhys {
   const double* __restrict__ sl_ce;
   const double* __restrict__ sl_pe;
   double maxspeed, eta_over_s, tau_pi_coeff, enezero, przero, glm_alpha;
+  double sigma_el, sigma_chiral;  // resistive runs: conductivities (code units)
 };
 
 // metric (system_metric_*, system.f90:132-160), derived from t on device
@@ -612,6 +621,19 @@ __device__ __forceinline__ void exb(const Metric& M, const double E[3], double b
   o[1] = gp * (e2 * bx - e0 * bz);
   o[2] = gp * (e0 * by - e1 * bx);
 }
+// covariant E_i of a cell: the resistive primitive E^i lowered
+// (system.f90:203-205; the reference's system_flux omits g_33 for E_3,
+// system.f90:1365, which only Minkowski coordinates forgive), or -v x B
+template <int KIND>
+__device__ __forceinline__ void e_field(const Metric& M, const double* v, double E[3]) {
+  if (Traits<KIND>::RES) {
+    E[0] = v[KEX];
+    E[1] = v[KEY];
+    E[2] = v[KEZ] * M.g3;
+  } else {
+    e_ideal(M, v[KVX], v[KVY], v[KVZ], v[KBX], v[KBY], v[KBZ], E);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // system_prim2cons (system.f90:164-263)
@@ -647,7 +669,7 @@ __device__ __forceinline__ int prim2cons(const DevPhys& P, const Metric& M, doub
     u[KPIYY] = v[KPIYY] * u[KRH];
   } else if (T::MHD) {
     double E[3], EXB[3];
-    e_ideal(M, vx, vy, vz, v[KBX], v[KBY], v[KBZ], E);
+    e_field<KIND>(M, v, E);
     double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
     exb(M, E, v[KBX], v[KBY], v[KBZ], EXB);
     double bx = v[KBX], by = v[KBY], bz = v[KBZ];
@@ -660,7 +682,12 @@ __device__ __forceinline__ int prim2cons(const DevPhys& P, const Metric& M, doub
     u[KBX] = v[KBX];
     u[KBY] = v[KBY];
     u[KBZ] = v[KBZ];
-    if (T::GLM) u[KGLM] = v[KGLM] / gp;
+    if (T::RES) {
+      u[KEX] = v[KEX];
+      u[KEY] = v[KEY];
+      u[KEZ] = v[KEZ];
+    }
+    if (T::GLM) u[T::KG] = v[T::KG] / gp;
   } else {
     u[KVX] = ww * vx;
     u[KVY] = ww * vy;
@@ -702,7 +729,7 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
   if (!T::VISC) {
     w = en + pr;
     if (T::MHD) {
-      e_ideal(M, vx, vy, vz, v[KBX], v[KBY], v[KBZ], E);
+      e_field<KIND>(M, v, E);
       E2 = E[0] * E[0] + E[1] * E[1] + over_g3(M, E[2] * E[2]);
       exb(M, E, v[KBX], v[KBY], v[KBZ], EXB);
       B2 = v[KBX] * v[KBX] + v[KBY] * v[KBY] + (v[KBZ] * v[KBZ]) * g3;
@@ -729,7 +756,12 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
     u[KBX] = v[KBX];
     u[KBY] = v[KBY];
     u[KBZ] = v[KBZ];
-    if (T::GLM) u[KGLM] = over_gp(M, v[KGLM]);
+    if (T::RES) {
+      u[KEX] = v[KEX];
+      u[KEY] = v[KEY];
+      u[KEZ] = v[KEZ];
+    }
+    if (T::GLM) u[T::KG] = over_gp(M, v[T::KG]);
   } else {
     u[KVX] = ww * vx;
     u[KVY] = ww * vy;
@@ -757,9 +789,14 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
       f[KBX] = 0.;
       f[KBY] = -E[2] * gm;
       f[KBZ] = +E[1] * gm;
+      if (T::RES) {  // E fluxes (system.f90:1450-1452)
+        f[KEX] = 0.;
+        f[KEY] = +v[KBZ] * g3 * gm;
+        f[KEZ] = -v[KBY] * g2 * gm;
+      }
       if (T::GLM) {
-        f[KBX] = v[KGLM];
-        f[KGLM] = over_gp(M, v[KBX]);
+        f[KBX] = v[T::KG];
+        f[T::KG] = over_gp(M, v[KBX]);
       }
     } else {
       f[KVX] = wwdir * vx * g1 + pr;
@@ -787,9 +824,14 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
       f[KBX] = E[2] * gm;
       f[KBY] = 0.;
       f[KBZ] = -E[0] * gm;
+      if (T::RES) {  // system.f90:1491-1493
+        f[KEX] = -v[KBZ] * g3 * gm;
+        f[KEY] = 0.;
+        f[KEZ] = +v[KBX] * g1 * gm;
+      }
       if (T::GLM) {
-        f[KBY] = v[KGLM];
-        f[KGLM] = over_gp(M, v[KBY]);
+        f[KBY] = v[T::KG];
+        f[T::KG] = over_gp(M, v[KBY]);
       }
     } else {
       f[KVX] = wwdir * vx * g1;
@@ -817,9 +859,14 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
       f[KBX] = -E[1] * gm;
       f[KBY] = E[0] * gm;
       f[KBZ] = 0.;
+      if (T::RES) {  // system.f90:1532-1534
+        f[KEX] = +v[KBY] * g2 * gm;
+        f[KEY] = -v[KBX] * g1 * gm;
+        f[KEZ] = 0.;
+      }
       if (T::GLM) {
-        f[KBZ] = over_g3(M, v[KGLM]);
-        f[KGLM] = over_gp(M, v[KBZ]);
+        f[KBZ] = over_g3(M, v[T::KG]);
+        f[T::KG] = over_gp(M, v[KBZ]);
       }
     } else {
       f[KVX] = wwdir * vx * g1;
@@ -858,6 +905,12 @@ __device__ __forceinline__ int system_flux(const DevPhys& P, const Metric& M, do
   double vf2 = den * sqrt(a2 * (1. - v2) * (hdir - (1. - a2) * (vdir * vdir)));
   vfp = vf1 + vf2;
   vfm = vf1 - vf2;
+  if (T::RES) {
+    // resistive: the light cone bounds the Riemann fan of the E, B waves (the
+    // reference keeps the ideal fast speed here, system.f90:1557-1580)
+    vfp = 1. / sqrt(DIR == 3 ? g3 : 1.);
+    vfm = -vfp;
+  }
   return 0;
 }
 

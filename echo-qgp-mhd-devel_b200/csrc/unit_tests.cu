@@ -87,6 +87,7 @@ extern "C" int echo_gpu_test_recon(int recal, int m, int n, const double* f, dou
 extern "C" int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, int n_eos, int ncells, double g3,
                                  double gp, const double* u, double* v, int* err, int* iters) {
   if (!p || ncells <= 0 || !u || !v) return ECHO_ERR_ARG;
+  if (p->mhd > 1) return ECHO_ERR_UNSUPPORTED;  // the resistive inversion is tested through the step
   (void)cudaGetLastError();
   int kind = echo_kind_of(p), nv = echo_nv_of(kind);
   size_t nb = (size_t)ncells * nv * sizeof(double);
@@ -215,6 +216,7 @@ extern "C" int echo_gpu_test_c2p_seeded(const EchoParams* p, const double* eos_t
                                         const double* u, double* v, int* err, int* iters, int* seed_failed) {
   if (!p || !p->mhd || p->viscosity || ncells <= 0 || !u || !v || !err || !iters || !seed_failed)
     return ECHO_ERR_ARG;
+  if (p->mhd > 1) return ECHO_ERR_UNSUPPORTED;
   (void)cudaGetLastError();
   int kind = echo_kind_of(p), nv = echo_nv_of(kind);
   size_t nb = (size_t)ncells * nv * sizeof(double);

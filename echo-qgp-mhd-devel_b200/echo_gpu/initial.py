@@ -257,11 +257,14 @@ def primitives(cfg, tab: np.ndarray | None = None, seed: int = 7,
         fields += [zero] * 7
     if cfg.mhd:
         e_c = float(e2.max())
-        B0 = math.sqrt(2.0 * 0.1 * e_c)  # magnetisation B^2/(2e) = 0.1 at the centre
+        sigma_m = 0.3 if cfg.mhd == 2 else 0.1
+        B0 = math.sqrt(2.0 * sigma_m * e_c)  # magnetisation B^2/(2e) at the centre
         X = np.broadcast_to(x[None, None, :], shape)
         Hz = np.broadcast_to((eta_profile(z) if cfg.nz > 1 else np.ones(1))[:, None, None], shape)
         by = B0 * np.exp(-(X**2) / (2 * 2.5**2)) * np.sqrt(Hz)
         fields += [zero, by, zero]
+        if cfg.mhd == 2:
+            fields += [zero, zero, zero]  # E = -v x B = 0 at rest
         if cfg.divclean:
             fields += [zero]
     return _pack(fields)
@@ -277,5 +280,5 @@ def bjorken_uniform(cfg, e0: float = 10.0) -> np.ndarray:
     if cfg.viscosity:
         fields += [z] * 7
     if cfg.mhd:
-        fields += [z, z, z] + ([z] if cfg.divclean else [])
+        fields += [z] * (6 if cfg.mhd == 2 else 3) + ([z] if cfg.divclean else [])
     return _pack(fields)

@@ -48,6 +48,8 @@ class EchoParams(ctypes.Structure):
         ("przero", ctypes.c_double),
         ("c2p_tol", ctypes.c_double),
         ("imex", ctypes.c_int),
+        ("sigma_el", ctypes.c_double),
+        ("sigma_chiral", ctypes.c_double),
     ]
 
 
@@ -93,12 +95,14 @@ class Config:
     steps: int = 10
     c2p_tol: float = 1e-10
     imex: int = 0              # viscous: Israel-Stewart relaxation linearly implicit per stage
+    sigma_el: float = 0.0      # EL_COND (resistive runs, mhd = 2)
+    sigma_chiral: float = 0.0  # CHIR_COND
 
     @property
     def nv(self) -> int:
         nv = 12 if self.viscosity else 5
         if self.mhd:
-            nv += 3 + (1 if self.divclean else 0)
+            nv += (6 if self.mhd == 2 else 3) + (1 if self.divclean else 0)
         return nv
 
     @property
@@ -139,6 +143,8 @@ class Config:
         p.przero = przero
         p.c2p_tol = self.c2p_tol
         p.imex = self.imex
+        p.sigma_el = self.sigma_el
+        p.sigma_chiral = self.sigma_chiral
         return p
 
 
@@ -175,6 +181,18 @@ def config2() -> Config:
                   viscosity=1, recal="WENO5", nrk=RK2, eqstate=EOS_TABLE,
                   eta_over_s=0.12, tau_pi_coeff=5.0, smooth_temp=0.08,
                   cfl=0.4, maxdt=0.01, enezero=0.02, steps=100)
+
+
+def config4() -> Config:
+    """3+1D resistive RMHD in Milne coordinates, 193x193x129, dx=deta=0.1,
+    config-1 EoS and profile, B_y as config 1 at magnetisation 0.3, E =
+    -v x B initially, sigma_el = 5.8 MeV, IMEX-SSP3(4,3,3), 300 steps."""
+    x1, x2 = _grid(193, 0.1)
+    z1, z2 = _grid(129, 0.1)
+    return Config("resistive-rmhd-3d-193x193x129", 193, 193, 129, x1, x2, x1, x2, z1, z2,
+                  mhd=2, divclean=1, glm_alpha=10.0, recal="WENO5", nrk=SSP,
+                  eqstate=EOS_TABLE, cfl=0.4, maxdt=0.002, enezero=0.02,
+                  sigma_el=0.0058, sigma_chiral=0.0015, steps=300)
 
 
 def small(cfg: Config, n: int = 12, nz: int | None = None) -> Config:

@@ -23,6 +23,7 @@ module evolve_gpu
     real(c_double) :: cfl, maxdt, maxspeed, glm_alpha, eta_over_s
     real(c_double) :: tau_pi_coeff, smooth_pressure, enezero, przero, c2p_tol
     integer(c_int) :: imex   ! this library's implicit Israel-Stewart relaxation; set 0 for the reference's explicit
+    real(c_double) :: sigma_el, sigma_chiral   ! sigma_el_cond, sigma_chiral_cond (resistive runs)
   end type echo_params
 
   type(c_ptr), save :: echo_ctx = c_null_ptr

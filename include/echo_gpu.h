@@ -78,7 +78,7 @@ typedef struct EchoParams {
   int nx, ny, nz;                 /* NX NY NZ */
   double x1, x2, y1, y2, z1, z2;  /* XMIN..ZMAX (common_grid, common.f90:441) */
   int coordinates;                /* COORD */
-  int mhd;                        /* MHD (0/1; 2 resistive is rejected) */
+  int mhd;                        /* MHD: 0, 1 ideal, 2 resistive (ECHO_SSP only) */
   int divclean;                   /* DIVCLEAN */
   int viscosity;                  /* VISCOUS */
   int bulkvis;                    /* BULK */
@@ -105,6 +105,10 @@ typedef struct EchoParams {
                                      linearly implicitly in every RK2/RK3 stage
                                      (the "IMEX RK2" of the batched workload);
                                      0 = explicit, as the reference */
+  double sigma_el;                /* EL_COND: electrical conductivity, used in
+                                     code units as read (system.f90:1660);
+                                     resistive runs (mhd = 2) only */
+  double sigma_chiral;            /* CHIR_COND: chiral conductivity (idem) */
 } EchoParams;
 
 typedef struct EchoCtx EchoCtx;

@@ -31,6 +31,17 @@
  *     start at 0) and return the reference error code;
  *   - the repair reads neighbours through the flat Fortran address
  *     (column-major, no bounds check) and reads 0 outside the allocation.
+ *
+ * Resistive RMHD (MHD=2) has no runnable reference path: the reference
+ * forces algo_solver 7 and IMEX-SSP (common.f90:2109-2118) and then exits in
+ * system_cons2prim, which has no algo-7 branch (system.f90:1160-1162).  Its
+ * prim2cons, fluxes and sources for resistive runs exist and are restated
+ * here (system.f90:199-212, 1360-1545, 1645-1661, 1747-1756, 1901-1919),
+ * with E_3 = g_33 E^3 and metric-consistent cross products throughout (the
+ * reference mixes co- and contravariant components in Bjorken coordinates;
+ * the two agree in Minkowski coordinates).  The implicit Ohm's-law
+ * con2prim and the implicit stage solves of IMEX-SSP3(4,3,3) are written
+ * from their definitions (cons2prim_res, stage1_implicit).
  */
 #include "echo_oracle.h"
 
@@ -64,6 +75,8 @@ typedef struct Phys {
   const EchoParams* p;
   int nv, nu;
   int kbx, kby, kbz, kglm;
+  int kex, key, kez; /* resistive E^i (system.f90:92-105) */
+  double ohm_h;      /* a_ii dt of the implicit stage being solved, else 0 */
   /* metric (system_metric_*, system.f90:132-160) */
   double g1, g2, g3, gp, gm, g0;
   double t;
@@ -77,7 +90,20 @@ static void phys_setup(Phys* ph, const EchoParams* p) {
   ph->p = p;
   int nv = p->viscosity ? 12 : 5; /* system_setup, system.f90:80-88 */
   ph->kbx = ph->kby = ph->kbz = ph->kglm = -1;
-  if (p->mhd) {
+  ph->kex = ph->key = ph->kez = -1;
+  if (p->mhd == 2) {
+    nv += 6;
+    ph->kbx = nv - 6;
+    ph->kby = nv - 5;
+    ph->kbz = nv - 4;
+    ph->kex = nv - 3;
+    ph->key = nv - 2;
+    ph->kez = nv - 1;
+    if (p->divclean) {
+      nv += 1;
+      ph->kglm = nv - 1;
+    }
+  } else if (p->mhd) {
     nv += 3;
     ph->kbx = nv - 3;
     ph->kby = nv - 2;
@@ -624,6 +650,78 @@ static void exb(const Phys* ph, const double* E, const double* b, double* o) {
   o[2] = gp * (e0 * b[1] - e1 * b[0]);
 }
 
+/* covariant E_i of a cell: the resistive primitive E^i lowered
+   (system.f90:203-205), or the ideal -v x B */
+static void e_field(const Phys* ph, const double* v, double* E) {
+  if (ph->p->mhd == 2) {
+    E[0] = v[ph->kex];
+    E[1] = v[ph->key];
+    E[2] = v[ph->kez] * ph->g3;
+  } else {
+    e_ideal(ph, v + KVX, v + ph->kbx, E);
+  }
+}
+
+/* contravariant (a x b)^i = sqrt(gamma)/g_ii [ijk] a^j b^k of contravariant
+   a, b (system_crossprod, system.f90:1867-1880, in Minkowski coordinates) */
+static void cross_contra(const Phys* ph, const double* a, const double* b, double* o) {
+  double gp = ph->gp;
+  o[0] = gp * (a[1] * b[2] - a[2] * b[1]);
+  o[1] = gp * (a[2] * b[0] - a[0] * b[2]);
+  o[2] = gp / ph->g3 * (a[0] * b[1] - a[1] * b[0]);
+}
+
+/* stiff part of the E source, Ohm's law with chiral term (system.f90:
+   1656-1660), contravariant, before the sqrt(-g) factor:
+   S = -gamma [sigma (E - (E.v) v + v x B) + sigma_chi (B - (B.v) v - v x E)].
+   (The reference's Minkowski branch assigns E.v twice and leaves B.v unset,
+   system.f90:1750-1751; B.v is used here.) */
+static void ohm_stiff(const Phys* ph, const double* vel, const double* B, const double* E, double glf,
+                      double* S) {
+  double g3 = ph->g3, sig = ph->p->sigma_el, chi = ph->p->sigma_chiral;
+  double vxb[3], vxe[3];
+  cross_contra(ph, vel, B, vxb);
+  cross_contra(ph, vel, E, vxe);
+  double vdotb = vel[0] * B[0] + vel[1] * B[1] + vel[2] * B[2] * g3;
+  double vdote = vel[0] * E[0] + vel[1] * E[1] + vel[2] * E[2] * g3;
+  for (int i = 0; i < 3; i++)
+    S[i] = -glf * (sig * (E[i] - vdote * vel[i] + vxb[i]) + chi * (B[i] - vdotb * vel[i] - vxe[i]));
+}
+
+/* E = Es + h S(E) for fixed v and B: linear in E,
+   [(1 + lam) I - lam v v_cov - mu (v x .)] E = Es - lam v x B - mu (B - (B.v) v)
+   with lam = h gamma sigma, mu = h gamma sigma_chi; solved by cofactors. */
+static void ohm_solve(const Phys* ph, const double* Es, const double* vel, const double* B, double h,
+                      double* E) {
+  double g3 = ph->g3, gp = ph->gp, gq = ph->gp / ph->g3;
+  double v2 = vel[0] * vel[0] + vel[1] * vel[1] + g3 * (vel[2] * vel[2]);
+  double glf = 1. / sqrt(1. - v2);
+  double lam = h * glf * ph->p->sigma_el, mu = h * glf * ph->p->sigma_chiral;
+  double vxb[3];
+  cross_contra(ph, vel, B, vxb);
+  double vdotb = vel[0] * B[0] + vel[1] * B[1] + vel[2] * B[2] * g3;
+  double vc[3] = {vel[0], vel[1], g3 * vel[2]};
+  double C[3][3] = {{0., -gp * vel[2], gp * vel[1]}, {gp * vel[2], 0., -gp * vel[0]}, {-gq * vel[1], gq * vel[0], 0.}};
+  double r[3], M[3][3];
+  for (int i = 0; i < 3; i++) {
+    r[i] = Es[i] - lam * vxb[i] - mu * (B[i] - vdotb * vel[i]);
+    for (int j = 0; j < 3; j++) M[i][j] = (i == j ? 1. + lam : 0.) - lam * vel[i] * vc[j] - mu * C[i][j];
+  }
+  double c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+  double c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+  double c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+  double c10 = M[0][2] * M[2][1] - M[0][1] * M[2][2];
+  double c11 = M[0][0] * M[2][2] - M[0][2] * M[2][0];
+  double c12 = M[0][1] * M[2][0] - M[0][0] * M[2][1];
+  double c20 = M[0][1] * M[1][2] - M[0][2] * M[1][1];
+  double c21 = M[0][2] * M[1][0] - M[0][0] * M[1][2];
+  double c22 = M[0][0] * M[1][1] - M[0][1] * M[1][0];
+  double det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+  E[0] = (c00 * r[0] + c10 * r[1] + c20 * r[2]) / det;
+  E[1] = (c01 * r[0] + c11 * r[1] + c21 * r[2]) / det;
+  E[2] = (c02 * r[0] + c12 * r[1] + c22 * r[2]) / det;
+}
+
 /* ------------------------------------------------------------------------ */
 /* prim2cons (system.f90:164-263)                                           */
 /* ------------------------------------------------------------------------ */
@@ -641,7 +739,7 @@ static int prim2cons(const Phys* ph, double* v, double* u) {
   u[KRH] = rh * glf;
   double E[3], EXB[3], EEM = 0;
   if (p->mhd) {
-    e_ideal(ph, v + KVX, v + ph->kbx, E);
+    e_field(ph, v, E);
     double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
     exb(ph, E, v + ph->kbx, EXB);
     double bx = v[ph->kbx], by = v[ph->kby], bz = v[ph->kbz];
@@ -672,6 +770,11 @@ static int prim2cons(const Phys* ph, double* v, double* u) {
     u[ph->kbx] = v[ph->kbx];
     u[ph->kby] = v[ph->kby];
     u[ph->kbz] = v[ph->kbz];
+    if (p->mhd == 2) {
+      u[ph->kex] = v[ph->kex];
+      u[ph->key] = v[ph->key];
+      u[ph->kez] = v[ph->kez];
+    }
     if (p->divclean) u[ph->kglm] = v[ph->kglm] / gp;
   } else {
     u[KVX] = ww * vx;
@@ -861,8 +964,91 @@ static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL,
 /* u, v have nv entries; v holds the guess.  Returns errcode, *iters the    */
 /* number of solver iterations (Newton steps, or BRENTM function evals).    */
 /* ------------------------------------------------------------------------ */
+/* Resistive con2prim with the implicit Ohm's law of an IMEX stage: the
+   algo_solver 7 the reference names (common.f90:292-293, 2109-2113) but
+   does not contain.  Unknowns v, p, E.  Given the stage's explicit part E*
+   and h = a_ii dt (ph->ohm_h; 0 outside an implicit solve), E solves
+   E = E* + h S(E; v, B), linear in E for fixed v (ohm_solve).  Fixed-point
+   iteration on v: E(v); the fluid's share S - E x B, U - (E^2 + B^2)/2; the
+   ideal-HD Newton on p (system.f90:511-561) for p and the new v; until
+   max |dv| <= 1e-14 (one pass when h = 0).  Code 779 when 200 passes do
+   not converge.  With h > 0, u[kex..kez] receives sqrt(-g) E. */
+static int cons2prim_res(const Phys* ph, double* u, double* v, int* iters) {
+  const double tol = 1.e-12, vtol = 1.e-14;
+  const int iter_max = 100, outer_max = 200;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gm = ph->gm, gp = ph->gp, h = ph->ohm_h;
+  int kbx = ph->kbx, kex = ph->kex;
+  double d = gm * u[KRH], U = gm * u[KPR];
+  double S[3] = {gm * u[KVX], gm * u[KVY], gm * u[KVZ]};
+  double B[3] = {gm * u[kbx], gm * u[kbx + 1], gm * u[kbx + 2]};
+  double Es[3] = {gm * u[kex], gm * u[kex + 1], gm * u[kex + 2]};
+  double vel[3] = {v[KVX], v[KVY], v[KVZ]}, E[3];
+  double pr = v[KPR], rh = v[KRH];
+  double B2 = B[0] * B[0] + B[1] * B[1] + (B[2] * B[2]) * g3;
+  int errcode = 0, outer, total = 0;
+  for (outer = 1; outer <= outer_max; outer++) {
+    if (h > 0.) {
+      ohm_solve(ph, Es, vel, B, h, E);
+    } else {
+      E[0] = Es[0];
+      E[1] = Es[1];
+      E[2] = Es[2];
+    }
+    double Ec[3] = {E[0], E[1], E[2] * g3}, EXB[3];
+    exb(ph, Ec, B, EXB);
+    double E2 = Ec[0] * Ec[0] + Ec[1] * Ec[1] + (Ec[2] * Ec[2]) / g3;
+    double sx = S[0] - EXB[0], sy = S[1] - EXB[1], sz = (S[2] - EXB[2]) / g3;
+    double et = U - 0.5 * (E2 + B2);
+    double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
+    double w = 0, v2, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    int iter;
+    for (iter = 1; iter <= iter_max; iter++) {
+      w = et + pr;
+      v2 = s2 / (w * w);
+      if (v2 >= 1.) {
+        *iters = total + iter;
+        return 777;
+      }
+      glf = 1. / sqrt(1. - v2);
+      rh = d / glf;
+      en = w * (1. - v2) - pr;
+      drhdpr = rh * v2 * glf / (en + pr);
+      dendpr = v2;
+      errcode = eos_pressure(ph, rh, en, &pr_eos, &dprdrh, &dprden);
+      f = pr_eos - pr;
+      df = dprdrh * drhdpr + dprden * dendpr - 1.;
+      dpr = -f / df;
+      if (fabs(dpr) < tol * pr) break;
+      pr = pr + dpr;
+    }
+    total += iter;
+    double vn0 = sx / w, vn1 = sy / w, vn2 = sz / w;
+    double dv = fmax3(fabs(vn0 - vel[0]), fabs(vn1 - vel[1]), fabs(vn2 - vel[2]) * gp);
+    vel[0] = vn0;
+    vel[1] = vn1;
+    vel[2] = vn2;
+    if (!(h > 0.) || dv <= vtol) break;
+  }
+  *iters = total;
+  if (outer > outer_max) return 779;
+  v[KRH] = rh;
+  v[KVX] = vel[0];
+  v[KVY] = vel[1];
+  v[KVZ] = vel[2];
+  v[KPR] = pr;
+  for (int i = 0; i < 3; i++) {
+    v[kbx + i] = B[i];
+    v[kex + i] = E[i];
+    if (h > 0.) u[kex + i] = E[i] * gp;
+  }
+  if (ph->p->divclean) v[ph->kglm] = u[ph->kglm];
+  if (pr <= 0) errcode = 777;
+  return errcode;
+}
+
 static int cons2prim(const Phys* ph, double* u, double* v, int* iters) {
   const EchoParams* p = ph->p;
+  if (p->mhd == 2) return cons2prim_res(ph, u, v, iters);
   const double tol = 1.e-12, eps = 1.e-12;
   const int iter_max = 100, ivmax = 100, ipmax = 100;
   double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gm = ph->gm;
@@ -1045,7 +1231,7 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
   if (!p->viscosity) {
     w = en + pr;
     if (p->mhd) {
-      e_ideal(ph, v + KVX, v + kbx, E);
+      e_field(ph, v, E);
       E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
       exb(ph, E, v + kbx, EXB);
       B2 = v[kbx] * v[kbx] + v[kby] * v[kby] + (v[kbz] * v[kbz]) * g3;
@@ -1072,6 +1258,11 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
     u[kbx] = v[kbx];
     u[kby] = v[kby];
     u[kbz] = v[kbz];
+    if (p->mhd == 2) {
+      u[ph->kex] = v[ph->kex];
+      u[ph->key] = v[ph->key];
+      u[ph->kez] = v[ph->kez];
+    }
     if (p->divclean) u[kglm] = v[kglm] / gp;
   } else {
     u[KVX] = ww * vx;
@@ -1099,6 +1290,11 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
       f[kbx] = 0.;
       f[kby] = -E[2] * gm;
       f[kbz] = +E[1] * gm;
+      if (p->mhd == 2) {
+        f[ph->kex] = 0.;
+        f[ph->key] = +v[kbz] * g3 * gm;
+        f[ph->kez] = -v[kby] * g2 * gm;
+      }
       if (p->divclean) {
         f[kbx] = v[kglm];
         f[kglm] = v[kbx] / gp;
@@ -1128,6 +1324,11 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
       f[kbx] = E[2] * gm;
       f[kby] = 0.;
       f[kbz] = -E[0] * gm;
+      if (p->mhd == 2) {
+        f[ph->kex] = -v[kbz] * g3 * gm;
+        f[ph->key] = 0.;
+        f[ph->kez] = +v[kbx] * g1 * gm;
+      }
       if (p->divclean) {
         f[kby] = v[kglm];
         f[kglm] = v[kby] / gp;
@@ -1157,6 +1358,11 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
       f[kbx] = -E[1] * gm;
       f[kby] = E[0] * gm;
       f[kbz] = 0.;
+      if (p->mhd == 2) {
+        f[ph->kex] = +v[kby] * g2 * gm;
+        f[ph->key] = -v[kbx] * g1 * gm;
+        f[ph->kez] = 0.;
+      }
       if (p->divclean) {
         f[kbz] = v[kglm] / g3;
         f[kglm] = v[kbz] / gp;
@@ -1186,6 +1392,12 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
   double vf2 = den * sqrt(a2 * (1. - v2) * ((1. - v2 * a2) / gcov_dir - (1. - a2) * (vdir * vdir)));
   vf[0] = vf1 + vf2;
   vf[1] = vf1 - vf2;
+  if (p->mhd == 2) {
+    /* resistive: the light cone bounds the Riemann fan (the E, B waves); the
+       reference keeps the ideal fast speed here (system.f90:1557-1580) */
+    vf[0] = 1. / sqrt(gcov_dir);
+    vf[1] = -vf[0];
+  }
   return 0;
 }
 
@@ -1198,12 +1410,14 @@ static int system_flux(const Phys* ph, double* v, double* u, double* f,
    u[k] = sqrt(-g) rho gamma v[k] holds -kap u[k] with kap[0] = 1/(gamma tau_Pi)
    for the bulk pressure and kap[1] = 1/(gamma tau_pi) for the shear
    components (the -1/tau (v[k] + ...) terms times rho sqrt(-g)). */
-static int system_source(const Phys* ph, double* v, const double* dv,
-                         double* src, double* kap) {
+static int system_source(const Phys* ph, double* v, const double* dv, double rhoC,
+                         double* src, double* stiff, double* kap) {
   const EchoParams* p = ph->p;
   double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gp = ph->gp, g0 = ph->g0;
   double t = ph->t;
   for (int k = 0; k < ph->nv; k++) src[k] = 0.;
+  if (stiff)
+    for (int k = 0; k < ph->nv; k++) stiff[k] = 0.;
   double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR];
   double en = 0;
   int err = eos_energy(ph, rh, &en, pr);
@@ -1218,7 +1432,8 @@ static int system_source(const Phys* ph, double* v, const double* dv,
       double ww = w * (glf * glf);
       if (p->mhd) {
         double E[3];
-        e_ideal(ph, v + KVX, v + ph->kbx, E);
+        e_field(ph, v, E); /* the reference takes the ideal E here also for
+                              resistive runs (system.f90:1641) */
         double bx = v[ph->kbx], by = v[ph->kby], bz = v[ph->kbz];
         double B2 = bx * bx + by * by + (bz * bz) * g3;
         double E2 = E[0] * E[0] + E[1] * E[1] + (E[2] * E[2]) / g3;
@@ -1353,9 +1568,20 @@ static int system_source(const Phys* ph, double* v, const double* dv,
                    lambda2 * IVyy;
     }
   }
+  if (p->mhd == 2) {
+    /* charge current and Ohm's law (system.f90:1650-1661, 1747-1756) */
+    double vel[3] = {vx, vy, vz}, S[3];
+    ohm_stiff(ph, vel, v + ph->kbx, v + ph->kex, glf, S);
+    for (int i = 0; i < 3; i++) {
+      src[ph->kex + i] = -rhoC * vel[i];
+      if (stiff) stiff[ph->kex + i] = S[i];
+    }
+  }
   if (p->viscosity)
     for (int k = KPIBU; k < ph->nv; k++) src[k] = src[k] * v[KRH];
   for (int k = 0; k < ph->nv; k++) src[k] = src[k] * gp;
+  if (stiff)
+    for (int k = 0; k < ph->nv; k++) stiff[k] = stiff[k] * gp;
   return 0;
 }
 
@@ -1441,7 +1667,8 @@ static void table_attach(Phys* ph, double** tT, double** te, double** tp,
 
 Orc* orc_create(const EchoParams* p, const double* eos_table, int n_eos) {
   if (p->mhd && p->viscosity) return NULL;
-  if (p->mhd > 1) return NULL;
+  if (p->mhd > 2) return NULL;
+  if (p->mhd == 2 && p->nrk != ECHO_SSP) return NULL; /* common.f90:2114-2118 */
   if (p->imex && p->nrk == ECHO_SSP) return NULL;
   Orc* e = (Orc*)calloc(1, sizeof(Orc));
   e->p = *p;
@@ -1983,25 +2210,55 @@ static void evolve_dts(Orc* e) {
   }
 }
 
-/* evolve_src (evolve.f90:689-718) */
+/* charge density rho_C = d_i E^i by central differences of the ghosted
+   primitives w (system_compute_divE, system.f90:1901-1919); directions of
+   one cell contribute nothing */
+static double div_e(const Orc* e, int ix, int iy, int iz) {
+  const Phys* ph = &e->ph;
+  double r = 0.;
+  if (e->nx > 1) {
+    double dx = 2. / e->ddx;
+    r = r + (e->w[WIDX(e, ph->kex, ix + 1, iy, iz)] - e->w[WIDX(e, ph->kex, ix - 1, iy, iz)]) / dx;
+  }
+  if (e->ny > 1) {
+    double dy = 2. / e->ddy;
+    r = r + (e->w[WIDX(e, ph->key, ix, iy + 1, iz)] - e->w[WIDX(e, ph->key, ix, iy - 1, iz)]) / dy;
+  }
+  if (e->nz > 1) {
+    double dz = 2. / e->ddz;
+    r = r + (e->w[WIDX(e, ph->kez, ix, iy, iz + 1)] - e->w[WIDX(e, ph->kez, ix, iy, iz - 1)]) / dz;
+  }
+  return r;
+}
+
+/* evolve_src (evolve.f90:689-718): du -= src, du_stiff -= src_stiff */
 static int evolve_src(Orc* e, int iteration) {
   size_t nc = e->ncell;
   int nv = e->nv;
   if (e->p.viscosity) evolve_dts(e);
   int err = 0;
   double* du = e->du[iteration - 1];
+  double* dus = e->dus[iteration - 1];
   for (size_t c = 0; c < nc && !err; c++) {
-    double vv[ECHO_MAX_NV], src[ECHO_MAX_NV], dv[NDERIV];
+    double vv[ECHO_MAX_NV], src[ECHO_MAX_NV], stiff[ECHO_MAX_NV], dv[NDERIV];
     for (int k = 0; k < nv; k++) vv[k] = e->v[(size_t)k * nc + c];
     if (e->p.viscosity)
       for (int d = 0; d < NDERIV; d++) dv[d] = e->deriv[(size_t)d * nc + c];
+    double rhoC = 0.;
+    if (e->p.mhd == 2) {
+      int ix = (int)(c % (size_t)e->nx) + 1, iy = (int)((c / (size_t)e->nx) % (size_t)e->ny) + 1;
+      int iz = (int)(c / ((size_t)e->nx * e->ny)) + 1;
+      rhoC = div_e(e, ix, iy, iz);
+    }
     double* kap = e->kap ? e->kap + 2 * c : NULL;
-    int ec = system_source(&e->ph, vv, dv, src, kap);
+    int ec = system_source(&e->ph, vv, dv, rhoC, src, stiff, kap);
     if (ec) {
       err = ec;
       break;
     }
     for (int k = 0; k < e->nu; k++) du[(size_t)k * nc + c] = du[(size_t)k * nc + c] - src[k];
+    if (dus)
+      for (int k = 0; k < e->nu; k++) dus[(size_t)k * nc + c] = dus[(size_t)k * nc + c] - stiff[k];
   }
   if (err) {
     e->errcode = err;
@@ -2094,6 +2351,9 @@ static int evolve_u2v(Orc* e) {
       e->fail[c] = 1;
     } else {
       for (int k = 0; k < nv; k++) e->vtmp[(size_t)k * nc + c] = vv[k];
+      /* the implicit Ohm solve of a resistive stage sets E in u */
+      if (ph->p->mhd == 2 && ph->ohm_h > 0.)
+        for (int k = ph->kex; k <= ph->kez; k++) e->u[(size_t)k * nc + c] = uu[k];
     }
   }
   e->c2p_iters = c2p;
@@ -2226,6 +2486,47 @@ static double dt_clip(Orc* e, double dt_local) { /* evolve.f90:181-188 */
   return dt_local;
 }
 
+/* Resistive IMEX-SSP3(4,3,3), first stage: U1 = u^n + alpha dt S(U1), the
+   implicit solve the reference leaves to its missing algo-7 con2prim.  U1
+   is solved from u0 cell by cell and dus[0] = -S(U1) replaces the stiff
+   source the stage's right-hand side took at u^n (only S(U1) enters the
+   later stages; the explicit F(U1) has weight 0).  v and u stay at step n. */
+static int stage1_implicit(Orc* e, double h) {
+  Phys* ph = &e->ph;
+  size_t nc = e->ncell;
+  int nv = e->nv;
+  ph->ohm_h = h;
+  for (size_t c = 0; c < nc; c++) {
+    double uu[ECHO_MAX_NV], vv[ECHO_MAX_NV], S[3];
+    for (int k = 0; k < nv; k++) {
+      uu[k] = e->u0[(size_t)k * nc + c];
+      vv[k] = e->v[(size_t)k * nc + c];
+    }
+    int it = 0, err = cons2prim(ph, uu, vv, &it);
+    if (err) {
+      ph->ohm_h = 0.;
+      e->errcode = err;
+      e->run_crashed = 1;
+      return err;
+    }
+    double v2 = ph->g1 * vv[KVX] * vv[KVX] + ph->g2 * vv[KVY] * vv[KVY] + ph->g3 * vv[KVZ] * vv[KVZ];
+    double glf = 1. / sqrt(1. - v2);
+    ohm_stiff(ph, vv + KVX, vv + ph->kbx, vv + ph->kex, glf, S);
+    for (int i = 0; i < 3; i++) e->dus[0][(size_t)(ph->kex + i) * nc + c] = 0. - S[i] * ph->gp;
+  }
+  ph->ohm_h = 0.;
+  return 0;
+}
+
+/* u2v of an implicit IMEX stage: the resistive con2prim solves Ohm's law
+   with h = alpha dt (the diagonal of the implicit tableau) */
+static int u2v_implicit(Orc* e, double h) {
+  if (e->p.mhd == 2) e->ph.ohm_h = h;
+  int err = evolve_u2v(e);
+  e->ph.ohm_h = 0.;
+  return err;
+}
+
 /* evolve_main (evolve.f90:114-298) */
 int orc_evolve_main(Orc* e, int irk, double* dt_out) {
   size_t n = e->ncell * e->nv;
@@ -2270,23 +2571,24 @@ int orc_evolve_main(Orc* e, int irk, double* dt_out) {
       memcpy(e->u0, e->u, sizeof(double) * n);
       if (rhs_all(e, 1)) return e->errcode;
       if (e->p.divclean) glm_source(e, e->dt / 2.);
+      if (e->p.mhd == 2 && stage1_implicit(e, alpha_imex * e->dt)) return e->errcode;
     } else if (irk == 2) {
       dt = e->dt;
       for (size_t i = 0; i < n; i++) e->u[i] = e->u0[i] + dt * alpha_imex * e->dus[0][i];
-      if (evolve_u2v(e)) return e->errcode;
+      if (u2v_implicit(e, alpha_imex * dt)) return e->errcode;
       if (rhs_all(e, 2)) return e->errcode;
     } else if (irk == 3) {
       dt = e->dt;
       for (size_t i = 0; i < n; i++)
         e->u[i] = e->u0[i] - dt * (e->du[1][i] + (1. - alpha_imex) * e->dus[1][i]);
-      if (evolve_u2v(e)) return e->errcode;
+      if (u2v_implicit(e, alpha_imex * dt)) return e->errcode;
       if (rhs_all(e, 3)) return e->errcode;
     } else {
       dt = e->dt;
       for (size_t i = 0; i < n; i++)
         e->u[i] = e->u0[i] - dt * (e->du[1][i] / 4. + e->du[2][i] / 4. + beta_imex * e->dus[0][i] +
                                    eta_imex * e->dus[1][i] + delta_imex * e->dus[2][i]);
-      if (evolve_u2v(e)) return e->errcode;
+      if (u2v_implicit(e, alpha_imex * dt)) return e->errcode;
       if (rhs_all(e, 4)) return e->errcode;
       for (size_t i = 0; i < n; i++)
         e->u[i] = e->u0[i] - dt * (e->du[1][i] / 6. + e->du[2][i] / 6. + e->du[3][i] * 2. / 3. +

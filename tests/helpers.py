@@ -48,14 +48,17 @@ def field_groups(nv: int) -> list[list[int]]:
     return [[0], [1, 2, 3], [4], list(range(5, nv))]
 
 
-def rel_linf(a: np.ndarray, b: np.ndarray, nv: int) -> float:
+RES_GROUPS = [[0], [1, 2, 3], [4], list(range(5, 12))]  # resistive: B, E, psi share a scale
+
+
+def rel_linf(a: np.ndarray, b: np.ndarray, nv: int, groups=None) -> float:
     """Relative L-inf error over primitives: max over variables of
     max|a-b| / S, where S is the largest |b| in the variable's field group
-    (see field_groups)."""
+    (see field_groups; RES_GROUPS for resistive runs)."""
     a = a.reshape(nv, -1)
     b = b.reshape(nv, -1)
     worst = 0.0
-    for grp in field_groups(nv):
+    for grp in (groups if groups is not None else field_groups(nv)):
         scale = max(float(np.max(np.abs(b[k]))) for k in grp)
         if scale == 0.0:
             scale = 1.0
@@ -68,7 +71,30 @@ CASES = {
     "hd2d": lambda: P.small(P.config0(), 12),
     "rmhd3d": lambda: P.small(P.config1(), 10, nz=8),
     "visc2d": lambda: P.small(P.config2(), 14),
+    "res3d": lambda: P.small(P.config4(), 10, nz=8),
 }
+
+
+def resistive_state(cfg, tab, amp: float = 0.2, ideal: float = 0.7) -> np.ndarray:
+    """The resistive workload's initial state (at rest, E = 0) given a
+    smooth flow along x, y and eta and an electric field that is `ideal`
+    times the ideal -v x B: a state with Ohm currents and charges from the
+    first step."""
+    v = I.primitives(cfg, tab).reshape(cfg.nv, cfg.nz, cfg.ny, cfg.nx)
+    x = I.cell_centres(cfg.nx, cfg.x1, cfg.x2)
+    y = I.cell_centres(cfg.ny, cfg.y1, cfg.y2)
+    z = I.cell_centres(cfg.nz, cfg.z1, cfg.z2)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    Lx, Lz = cfg.x2 - cfg.x1, max(cfg.z2 - cfg.z1, 1e-300)
+    tau = cfg.tstart if cfg.coordinates == P.BJORKEN else 1.0
+    v[1] = amp * np.sin(np.pi * Y / Lx) * np.cos(np.pi * Z / Lz)
+    v[2] = amp * np.sin(np.pi * X / Lx)
+    v[3] = 0.5 * amp / tau * np.sin(np.pi * (X + Y) / Lx)
+    vx, vy, vz, bx, by, bz = v[1], v[2], v[3], v[5], v[6], v[7]
+    # ideal covariant E_i = -sqrt(-g) [ijk] v^j B^k, raised with g_33 = tau^2
+    e_cov = [-tau * (vy * bz - vz * by), -tau * (vz * bx - vx * bz), -tau * (vx * by - vy * bx)]
+    v[8], v[9], v[10] = ideal * e_cov[0], ideal * e_cov[1], ideal * e_cov[2] / tau**2
+    return v.reshape(-1)
 
 
 def gubser(tau, X, Y, q=1.0, T0=0.4):

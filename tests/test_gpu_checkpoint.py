@@ -11,7 +11,7 @@ from helpers import CASES, setup
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("case,nrk", [("hd2d", None), ("rmhd3d", None), ("visc2d", None), ("hd2d", P.SSP)])
+@pytest.mark.parametrize("case,nrk", [("hd2d", None), ("rmhd3d", None), ("visc2d", None), ("hd2d", P.SSP), ("res3d", None)])
 def test_restart_continues_bit_for_bit(case, nrk):
     cfg = CASES[case]()
     if nrk is not None:
