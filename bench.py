@@ -115,7 +115,7 @@ class Clocks:
 # CPU side: the reference algorithm (oracle restatement)
 # ---------------------------------------------------------------------------
 def cpu_rate(cfg, tab, przero, threads: int, target_s: float, steps: int | None = None,
-             warmup: int = 0):
+             warmup: int = 0, state=None):
     """cell-updates/s of the reference algorithm on the host on a z-slab of
     the workload sized so one step takes about target_s seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -127,16 +127,17 @@ def cpu_rate(cfg, tab, przero, threads: int, target_s: float, steps: int | None 
         z1, z2 = P._grid(nz, (cfg.z2 - cfg.z1) / cfg.nz)
         return cfg.replace(nz=nz, z1=z1, z2=z2)
 
+    state = state or (lambda c: I.primitives(c, tab))
     probe = slab(6)
     o = O.Oracle(probe.to_c(przero=przero), tab, threads=threads)
-    o.set_state(I.primitives(probe, tab), None, probe.tstart)
+    o.set_state(state(probe), None, probe.tstart)
     t0 = time.perf_counter()
     o.step()
     rate = probe.ncell / (time.perf_counter() - t0)
     nz = int(max(6, min(cfg.nz, round(target_s * rate / (cfg.nx * cfg.ny)))))
     c = slab(nz)
     o = O.Oracle(c.to_c(przero=przero), tab, threads=threads)
-    o.set_state(I.primitives(c, tab), None, c.tstart)
+    o.set_state(state(c), None, c.tstart)
     for _ in range(warmup):
         o.step()
     n = steps if steps is not None else 2
@@ -144,7 +145,7 @@ def cpu_rate(cfg, tab, przero, threads: int, target_s: float, steps: int | None 
     for _ in range(n):
         o.step()
     el = time.perf_counter() - t0
-    sample = (f"{n} full RK3 steps of a {c.nx}x{c.ny}x{c.nz} slab of the workload "
+    sample = (f"{n} full steps of a {c.nx}x{c.ny}x{c.nz} slab of the workload "
               f"(same spacing, EoS, scheme), after {warmup} untimed steps")
     return c.ncell * n / el, el, sample
 
@@ -188,6 +189,70 @@ def algorithmic_bytes(kclass: str, cfg) -> float:
         # read F(x,y,z), v, u and (two stages in three) u0; write u and v
         return 8.0 * nv * (sum(nf) + nc * (2 + 2.0 / 3.0) + 2 * nc) + nc
     return 0.0
+
+
+B_ALG_RES = 1896  # bytes per cell-update of a stage-fused IMEX-SSP3(4,3,3) resistive step, nv = 12
+
+
+def run_resistive(args, torch, barrier, world, rank):
+    """The resistive workload: 3+1D resistive RMHD (MHD = 2) on 193x193x129
+    (dx = deta = 0.1), sigma_el = 5.8 MeV and the chiral term, IMEX-SSP3(4,3,3)
+    with the implicit Ohm's law in every implicit stage's con2prim, GLM,
+    WENO5 + HLL, tabulated EoS.  The reference cannot run this path (its
+    con2prim has no branch for MHD = 2); the CPU figure beside it is the
+    oracle's statement of the same scheme on a slab of the grid."""
+    from echo_gpu import initial as I
+    from echo_gpu import params as P
+    from echo_gpu.lib import Evolve
+
+    cfg = P.config4()
+    tab = I.eos_table_loaded()
+    przero = float(I.table_pressure(tab, np.array([cfg.enezero]))[0])
+    ev = Evolve(cfg.to_c(przero=przero), tab, exact=False)
+    ev.upload(I.primitives(cfg, tab), None, cfg.tstart)
+    stream = torch.cuda.ExternalStream(ev.stream_handle())
+    steps = max(3, min(args.steps, 20))
+    ev.run(max(args.warmup, 3))
+    ev.sync()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ev.run(steps)
+    e1.record(stream)
+    ev.sync()
+    torch.cuda.synchronize()
+    barrier()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    st = ev.stats()
+    prof = ev.profile_step()
+    ev.sync()
+    ev.close()
+    value = cfg.ncell * steps * world / (ms / 1e3)
+    pk = peaks()
+    out = {
+        "workload": cfg.name, "grid": [cfg.nx, cfg.ny, cfg.nz], "nv": cfg.nv,
+        "scheme": "WENO5+HLL (light-cone speeds)+GLM, IMEX-SSP3(4,3,3), implicit Ohm's law, tabulated EoS",
+        "sigma_el": cfg.sigma_el, "sigma_chiral": cfg.sigma_chiral,
+        "value": value, "unit": UNIT, "steps": steps, "ms_per_step": ms / steps,
+        "step_roofline": {"bytes_per_cell_update": B_ALG_RES, "achieved_gbs": value / world * B_ALG_RES / 1e9,
+                          "frac": value / world * B_ALG_RES / 1e9 / pk["hbm_gbs"],
+                          "peak_src": pk["src"] + " (hbm_gbs)"},
+        "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()},
+        "c2p_iters_per_cell_last_stage": st.c2p_iters / max(cfg.ncell, 1),
+        "errcode": int(st.errcode), "repairs": int(st.repairs),
+        "parity": "unpinned against the reference (no runnable resistive path); device = oracle at 1e-12",
+    }
+    if world == 1 and rank == 0:
+        rate, el, sample = cpu_rate(cfg, tab, przero, threads=1, target_s=4.0, steps=1)
+        out["cpu_oracle"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+    return out
 
 
 def run_batched(args, torch, barrier, world, rank):
@@ -397,6 +462,7 @@ def run_b200(args):
     e2e_value = cfg0.ncell * e2e_steps * world / (float(e2e_ms.item()) / 1e3)
     st2 = ev.stats()
     batched = run_batched(args, torch, barrier, world, rank) if args.batched else None
+    resistive = run_resistive(args, torch, barrier, world, rank) if args.resistive else None
 
     if world > 1:
         dist.barrier()
@@ -457,6 +523,7 @@ def run_b200(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * nbytes, "d2h_bytes_per_step": 2 * nbytes,
                 "steps": e2e_steps},
         "batched": batched,
+        "resistive": resistive,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "stats": {"errcode": st.errcode, "repairs": st.repairs, "t": st2.t, "dt": st.dt},
@@ -476,6 +543,7 @@ def main():
     ap.add_argument("--pairs", type=int, default=600_000, help="training pairs for the con2prim seed")
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--batched", type=int, default=1, help="also run the batched event-by-event workload")
+    ap.add_argument("--resistive", type=int, default=1, help="also run the resistive RMHD workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

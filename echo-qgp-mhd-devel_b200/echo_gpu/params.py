@@ -186,12 +186,16 @@ def config2() -> Config:
 def config4() -> Config:
     """3+1D resistive RMHD in Milne coordinates, 193x193x129, dx=deta=0.1,
     config-1 EoS and profile, B_y as config 1 at magnetisation 0.3, E =
-    -v x B initially, sigma_el = 5.8 MeV, IMEX-SSP3(4,3,3), 300 steps."""
+    -v x B initially, sigma_el = 5.8 MeV, IMEX-SSP3(4,3,3), 300 steps.
+    ENEZERO = 0.05 GeV/fm^3 (param.dat:115): B_y(x, eta) fills the whole y
+    range, and at the y edges, where e = ENEZERO, the magnetic work of the
+    Bjorken source over one frozen-metric step (dt B^2 / (2 tau) ~ 0.02)
+    would take the fluid energy below the table with 0.02."""
     x1, x2 = _grid(193, 0.1)
     z1, z2 = _grid(129, 0.1)
     return Config("resistive-rmhd-3d-193x193x129", 193, 193, 129, x1, x2, x1, x2, z1, z2,
                   mhd=2, divclean=1, glm_alpha=10.0, recal="WENO5", nrk=SSP,
-                  eqstate=EOS_TABLE, cfl=0.4, maxdt=0.002, enezero=0.02,
+                  eqstate=EOS_TABLE, cfl=0.4, maxdt=0.002, enezero=0.05,
                   sigma_el=0.0058, sigma_chiral=0.0015, steps=300)
 
 
