@@ -47,7 +47,11 @@ struct EchoCtx {
   // per-kernel timing (echo_gpu_profile_step): events recorded after each launch group
   std::vector<std::pair<int, cudaEvent_t>>* marks;
   EchoHyp* hyp;             // set up by echo_gpu_hyp_init
+  void* d_out;              // output staging (echo_gpu_out_vars), grown on demand
+  size_t out_bytes;
+  unsigned long long* d_out_err;
 };
+void echo_out_free(EchoCtx* c);
 
 // kernel classes reported by echo_gpu_profile_step
 enum { PK_FACES_X = 0, PK_FACES_Y = 1, PK_FACES_Z = 2, PK_SCALARS = 3, PK_UPDATE = 4, PK_REPAIR = 5, PK_END = 6,

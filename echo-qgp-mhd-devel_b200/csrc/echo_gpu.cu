@@ -362,6 +362,9 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->d_mlp_frag = nullptr;
   c->d_mlp_par = nullptr;
   c->hyp = nullptr;
+  c->d_out = nullptr;
+  c->out_bytes = 0;
+  c->d_out_err = nullptr;
   *out = c;
   return ECHO_OK;
 }
@@ -393,6 +396,7 @@ int echo_gpu_free(EchoCtx* c) {
   cudaFree(c->d_mlp_par);
   cudaFreeHost(c->h_sc);
   echo_hyp_free(c->hyp);
+  echo_out_free(c);
   cudaStreamDestroy(c->stream);
   free(c);
   return ECHO_OK;

@@ -20,7 +20,7 @@ from . import initial as I
 from . import params as P
 from .lib import Evolve
 
-CONFIGS = {"hd": P.config0, "rmhd": P.config1, "visc": P.config2}
+CONFIGS = {"hd": P.config0, "rmhd": P.config1, "visc": P.config2, "res": P.config4}
 
 
 def run_batch(a) -> None:

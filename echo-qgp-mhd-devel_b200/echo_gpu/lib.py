@@ -87,6 +87,8 @@ FUNCTIONS = {
     "echo_gpu_checkpoint": (ctypes.c_int, [P, P]),
     "echo_gpu_restart": (ctypes.c_int, [P, P]),
     "echo_gpu_check_temp": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, D, I]),
+    "echo_gpu_out_vars_size": (ctypes.c_int, [P, ctypes.c_uint, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
+    "echo_gpu_out_vars": (ctypes.c_int, [P, ctypes.c_uint, ctypes.c_int, P, ctypes.c_size_t, I]),
     "echo_batch_set_stop": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
     "echo_batch_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.POINTER(EchoEventGrid),
                                        ctypes.POINTER(P)]),
@@ -286,6 +288,17 @@ class Evolve:
         self._check(self.lib.echo_gpu_check_temp(self.h, freeze_type, temp_end, ctypes.byref(m),
                                                  ctypes.byref(stop)), "check_temp")
         return m.value, bool(stop.value)
+
+    def out_vars(self, sel: int, precision: int = 8):
+        """out_vars (out.f90:232-591) staged on the device: (bytes of one
+        outNNNN.dat, errcode of the first cell whose derived data fail)."""
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.echo_gpu_out_vars_size(self.h, sel, precision, ctypes.byref(n)), "out_vars_size")
+        buf = ctypes.create_string_buffer(n.value)
+        err = ctypes.c_int(0)
+        self._check(self.lib.echo_gpu_out_vars(self.h, sel, precision, ctypes.cast(buf, ctypes.c_void_p), n.value,
+                                               ctypes.byref(err)), "out_vars")
+        return bytes(buf.raw), err.value
 
     def rhs(self):
         du = np.empty(self.ncell * self.nv)

@@ -194,6 +194,41 @@ int echo_gpu_stream(EchoCtx* ctx, void** stream);
 int echo_gpu_check_temp(EchoCtx* ctx, int freeze_type, double temp_end,
                         double* max_value, int* stop);
 
+/* Output staging in the reference's binary layout (out_vars, out.f90:232-591):
+ * the contents of one outNNNN.dat -- t, then every selected field over the
+ * whole grid in Fortran order (x fastest), in the reference's field order,
+ * in double (precision 8) or single (4) precision -- assembled on the device
+ * and copied once into host memory; the caller writes the bytes to the file.
+ * Derived fields (energy density, temperature, entropy density: the
+ * get_derived_data of eos.f90:645-701; pi^{tmu} from get_derived_pi(_zz),
+ * viscous.f90:236-279; the Lorentz factor v0; the ideal E = -v x B,
+ * contravariant, for ideal MHD) are computed from the current primitives
+ * at the current t.  Viscous fields are written only for viscous runs, B
+ * and E only for MHD runs, psi only with divclean, as in the reference; the
+ * comoving charge density (out_sel%rc) is not offered.  pi^{eta eta}: the
+ * derived value for TRACE_IMP 'zz', else the primitive (the reference writes
+ * an array it fills only when one of pi^{t mu} is selected).  `sel` is a
+ * mask of ECHO_OUT_* bits (the out_sel flags, common.f90:122-151; their
+ * defaults, common.f90:724-805, are ECHO_OUT_DEFAULT).  out_vars_size gives
+ * the bytes; out_vars fills `buf` (that many bytes) and sets *errcode to the
+ * reference code of the first cell, in Fortran loop order, whose derived
+ * data fall outside the EoS table (0: none).  Synchronises the stream. */
+enum {
+  ECHO_OUT_DENSITY = 1 << 0, ECHO_OUT_VX = 1 << 1, ECHO_OUT_VY = 1 << 2, ECHO_OUT_VZ = 1 << 3,
+  ECHO_OUT_PRESSURE = 1 << 4, ECHO_OUT_ENERGY_DENSITY = 1 << 5, ECHO_OUT_TEMPERATURE = 1 << 6,
+  ECHO_OUT_ENTROPY_DENSITY = 1 << 7, ECHO_OUT_BULK = 1 << 8, ECHO_OUT_PITT = 1 << 9,
+  ECHO_OUT_PITX = 1 << 10, ECHO_OUT_PITY = 1 << 11, ECHO_OUT_PITZ = 1 << 12, ECHO_OUT_PIXY = 1 << 13,
+  ECHO_OUT_PIXZ = 1 << 14, ECHO_OUT_PIYZ = 1 << 15, ECHO_OUT_PIXX = 1 << 16, ECHO_OUT_PIYY = 1 << 17,
+  ECHO_OUT_PIZZ = 1 << 18, ECHO_OUT_V0 = 1 << 19, ECHO_OUT_BX = 1 << 20, ECHO_OUT_BY = 1 << 21,
+  ECHO_OUT_BZ = 1 << 22, ECHO_OUT_EX = 1 << 23, ECHO_OUT_EY = 1 << 24, ECHO_OUT_EZ = 1 << 25,
+  ECHO_OUT_GLM = 1 << 26
+};
+#define ECHO_OUT_DEFAULT                                                                                  \
+  (ECHO_OUT_DENSITY | ECHO_OUT_VX | ECHO_OUT_VY | ECHO_OUT_VZ | ECHO_OUT_PRESSURE | ECHO_OUT_ENERGY_DENSITY | \
+   ECHO_OUT_BX | ECHO_OUT_BY | ECHO_OUT_BZ | ECHO_OUT_EX | ECHO_OUT_EY | ECHO_OUT_EZ)
+int echo_gpu_out_vars_size(const EchoCtx* ctx, unsigned sel, int precision, size_t* bytes);
+int echo_gpu_out_vars(EchoCtx* ctx, unsigned sel, int precision, void* buf, size_t bytes, int* errcode);
+
 /* Checkpoint / restart of a run at a step boundary (the role of out_dump and
  * out_restart, out.f90:1313-1483, which the reference turns off for MHD and
  * Monte Carlo runs; here every equation set).  The blob (checkpoint_size

@@ -1643,6 +1643,100 @@ double orc_check_temp(const Orc* e, int freeze_type) {
   return mx;
 }
 
+/* out_vars (out.f90:232-591): field k of the output is bit k of sel, in the
+   order the reference writes them; viscous fields need a viscous run, B, E
+   and psi an MHD run (psi with divclean) */
+static int out_field_on(const EchoParams* p, unsigned sel, int k) {
+  if (!(sel >> k & 1u)) return 0;
+  if (k >= 8 && k <= 18) return p->viscosity != 0;
+  if (k >= 20 && k <= 25) return p->mhd != 0;
+  if (k == 26) return p->mhd != 0 && p->divclean != 0;
+  return k <= 26;
+}
+
+size_t orc_out_vars(const Orc* e, unsigned sel, int precision, void* buf, int* errcode) {
+  const Phys* ph = &e->ph;
+  size_t nc = e->ncell;
+  int nf = 0, fields[32];
+  for (int k = 0; k <= 26; k++)
+    if (out_field_on(&e->p, sel, k)) fields[nf++] = k;
+  size_t prec = precision == 4 ? 4 : 8;
+  size_t bytes = prec + (size_t)nf * nc * prec;
+  if (errcode) *errcode = 0;
+  if (!buf) return bytes;
+  unsigned char* out = (unsigned char*)buf;
+  if (prec == 8) {
+    double t = e->t;
+    memcpy(out, &t, 8);
+  } else {
+    float t = (float)e->t;
+    memcpy(out, &t, 4);
+  }
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3;
+  int first_err = 0;
+  for (size_t c = 0; c < nc; c++) {
+    double p[ECHO_MAX_NV];
+    for (int k = 0; k < e->nv; k++) p[k] = e->v[(size_t)k * nc + c];
+    double en = 0., temp = 0., sd = 0.;
+    if ((sel & (ECHO_OUT_ENERGY_DENSITY | ECHO_OUT_TEMPERATURE | ECHO_OUT_ENTROPY_DENSITY)) != 0) {
+      int err = get_derived_data(ph, p[KRH], p[KPR], &en, &temp, &sd);
+      if (err && !first_err) first_err = err;
+    }
+    Pit pi = {0, 0, 0, 0, 0};
+    if (e->p.viscosity) {
+      if (e->p.obtained_zz)
+        derived_pi_zz(ph, p, &pi);
+      else
+        derived_pi(ph, p, &pi);
+    }
+    double E[3] = {0, 0, 0};
+    if (e->p.mhd == 1) e_ideal(ph, p + KVX, p + ph->kbx, E);
+    for (int f = 0; f < nf; f++) {
+      double x = 0.;
+      switch (fields[f]) {
+        case 0: x = p[KRH]; break;
+        case 1: x = p[KVX]; break;
+        case 2: x = p[KVY]; break;
+        case 3: x = p[KVZ]; break;
+        case 4: x = p[KPR]; break;
+        case 5: x = en; break;
+        case 6: x = temp; break;
+        case 7: x = sd; break;
+        case 8: x = p[KPIBU]; break;
+        case 9: x = pi.tt; break;
+        case 10: x = pi.tx; break;
+        case 11: x = pi.ty; break;
+        case 12: x = pi.tz; break;
+        case 13: x = p[KPIXY]; break;
+        case 14: x = p[KPIXZ]; break;
+        case 15: x = p[KPIYZ]; break;
+        case 16: x = p[KPIXX]; break;
+        case 17: x = p[KPIYY]; break;
+        case 18: x = e->p.obtained_zz ? pi.zz : p[KPIZZ]; break;
+        case 19:
+          x = 1. / sqrt(1. - p[KVX] * p[KVX] * g1 - p[KVY] * p[KVY] * g2 - p[KVZ] * p[KVZ] * g3);
+          break;
+        case 20: x = p[ph->kbx]; break;
+        case 21: x = p[ph->kby]; break;
+        case 22: x = p[ph->kbz]; break;
+        case 23: x = e->p.mhd == 2 ? p[ph->kex] : E[0]; break;
+        case 24: x = e->p.mhd == 2 ? p[ph->key] : E[1]; break;
+        case 25: x = e->p.mhd == 2 ? p[ph->kez] : E[2] / g3; break;
+        default: x = p[ph->kglm]; break;
+      }
+      size_t at = prec + ((size_t)f * nc + c) * prec;
+      if (prec == 8) {
+        memcpy(out + at, &x, 8);
+      } else {
+        float y = (float)x;
+        memcpy(out + at, &y, 4);
+      }
+    }
+  }
+  if (errcode) *errcode = first_err;
+  return bytes;
+}
+
 static void table_attach(Phys* ph, double** tT, double** te, double** tp,
                          double** tc, int* nt, const double* tab, int n) {
   *nt = n;

@@ -50,6 +50,10 @@ long long orc_repairs(const Orc* e);
 long long orc_c2p_iters(const Orc* e);
 /* check_temp (out.f90:1487-1557) over the current primitives */
 double orc_check_temp(const Orc* e, int freeze_type);
+/* out_vars (out.f90:232-591): the bytes of one outNNNN.dat (see
+   echo_gpu_out_vars); returns the byte count, *errcode the first derived-data
+   error in Fortran loop order; buf may be NULL to get the size only */
+size_t orc_out_vars(const Orc* e, unsigned sel, int precision, void* buf, int* errcode);
 /* freeze-out hypersurface (out_hyp / find_hypersurface_*): records of
  * 8 + nv doubles (tau, x, y, eta, primitives, dV with sign) */
 int orc_hyp_init(Orc* e, int freeze_type, double freeze_value);

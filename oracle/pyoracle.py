@@ -54,6 +54,8 @@ def lib():
         L.orc_hyp_get.argtypes = [P, D]
         L.orc_check_temp.restype = ctypes.c_double
         L.orc_check_temp.argtypes = [P, ctypes.c_int]
+        L.orc_out_vars.restype = ctypes.c_size_t
+        L.orc_out_vars.argtypes = [P, ctypes.c_uint, ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
         L.orc_recon.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]
         L.orc_c2p.argtypes = [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                               ctypes.c_double, D, D, I, I]
@@ -154,6 +156,14 @@ class Oracle:
     @property
     def glm_ch(self) -> float:
         return lib().orc_glm_ch(self.h)
+
+    def out_vars(self, sel: int, precision: int = 8):
+        """out_vars (out.f90:232-591): (bytes of one outNNNN.dat, errcode)."""
+        n = lib().orc_out_vars(self.h, sel, precision, None, None)
+        buf = ctypes.create_string_buffer(n)
+        err = ctypes.c_int(0)
+        lib().orc_out_vars(self.h, sel, precision, ctypes.cast(buf, ctypes.c_void_p), ctypes.byref(err))
+        return bytes(buf.raw), err.value
 
     def check_temp(self, freeze_type: int = 1) -> float:
         """check_temp (out.f90:1487-1557): maximum T (0) or e (1) over the grid."""
