@@ -111,7 +111,15 @@ __device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, 
 #ifndef ECHO_FACE_MINB_VISC
 #define ECHO_FACE_MINB_VISC 5
 #endif
-#define ECHO_FACE_BOUNDS(KIND) __launch_bounds__(128, (KIND) == KIND_VISC ? ECHO_FACE_MINB_VISC : ECHO_FACE_MINB)
+// resistive (nv = 12, 193x193x129, per step): faces 7 (6: +3 %, 5: +11 %);
+// update 5 (7: +1.9 ms, 6: +2.0, 4: +0.05); the IMEX-SSP combination 8
+// (uncapped 118 registers: +3.6 ms; 5: +1.1, 6: +0.5, 7: +0.14)
+#ifndef ECHO_FACE_MINB_RES
+#define ECHO_FACE_MINB_RES 7
+#endif
+#define ECHO_FACE_BOUNDS(KIND)                                                      \
+  __launch_bounds__(128, (KIND) == KIND_VISC  ? ECHO_FACE_MINB_VISC              \
+                         : (KIND) == KIND_RES ? ECHO_FACE_MINB_RES : ECHO_FACE_MINB)
 #ifndef ECHO_UPDATE_MINB
 #define ECHO_UPDATE_MINB 7
 #endif
@@ -121,9 +129,17 @@ __device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, 
 #ifndef ECHO_UPDATE_MINB_SEED
 #define ECHO_UPDATE_MINB_SEED 6
 #endif
+#ifndef ECHO_UPDATE_MINB_RES
+#define ECHO_UPDATE_MINB_RES 5
+#endif
+// the IMEX-SSP combination (con2prim) kernels
+#ifndef ECHO_SSP_MINB
+#define ECHO_SSP_MINB 8
+#endif
 #define ECHO_UPDATE_BOUNDS(KIND, SEED)                                       \
   __launch_bounds__(128, (SEED)                 ? ECHO_UPDATE_MINB_SEED   \
                          : (KIND) == KIND_VISC ? ECHO_UPDATE_MINB_VISC   \
+                         : (KIND) == KIND_RES  ? ECHO_UPDATE_MINB_RES    \
                                                : ECHO_UPDATE_MINB)
 
 struct FaceArgs {
@@ -783,7 +799,7 @@ struct SspArgs {
 };
 
 template <int KIND, bool SEED>
-__global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
+__global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_combine_kernel(SspArgs A) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const double alpha_imex = 0.24169426078821, beta_imex = 0.06042356519705, eta_imex = 0.12915286960590;
@@ -860,7 +876,7 @@ __global__ void __launch_bounds__(128) ssp_combine_kernel(SspArgs A) {
 // later stages combine (only S(U1) enters them: F(U1) has weight 0).  v and
 // u stay at step n; a failed solve stops the run with its code.
 template <int KIND>
-__global__ void __launch_bounds__(128) ssp_stage1_kernel(SspArgs A) {
+__global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_stage1_kernel(SspArgs A) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const double alpha_imex = 0.24169426078821;
