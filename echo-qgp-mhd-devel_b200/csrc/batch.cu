@@ -123,6 +123,7 @@ int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos, int
   if (p->mhd > 1 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
   if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3) return ECHO_ERR_UNSUPPORTED;
   if (p->imex != 0 && p->imex != 1) return ECHO_ERR_ARG;
+  if (p->mhd && c2p_alt_algo(p->algo_solver)) return ECHO_ERR_UNSUPPORTED;  // ALG_SOLV 2..6: single grid
   if (p->algo_solver == ECHO_C2P_MLP) return ECHO_ERR_UNSUPPORTED;
   if (p->eqstate == ECHO_EOS_TABLE && (!eos_table || n_eos < 2)) return ECHO_ERR_ARG;
   for (int e = 0; e < nev; e++) {

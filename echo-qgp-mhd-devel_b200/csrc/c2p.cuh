@@ -27,12 +27,12 @@ __device__ __forceinline__ double sist3_f(const DevPhys& P, const Sist3& s, cons
 
 __device__ __forceinline__ double dmax1(double a, double b) { return b > a ? b : a; }
 
+// BRENTM on N unknowns; sys.f(X, K) is the K-th equation (sist3, sist4).
 // Returns INFO; X in/out; *nfev = NFEV.  MAXFEV bounds the iteration count.
-static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, double FTOL, double XTOL, int MAXFEV,
-                       int MOPT, int* nfev_out) {
-  const int N = 3;
-  double Q[9], SIGMA[3], WA1[3], WA2[3];
-#define QQ(i, j) Q[((j)-1) * 3 + ((i)-1)]
+template <int N, class Sys>
+static __device__ int brentm(Sys& sys, double* X, double FTOL, double XTOL, int MAXFEV, int MOPT, int* nfev_out) {
+  double Q[N * N], SIGMA[N], WA1[N], WA2[N];
+#define QQ(i, j) Q[((j)-1) * N + ((i)-1)]
   int NFCALL = 0, NIER6 = -1, NIER7 = -1, NIER8 = 0, NSING, INFO = 0, NFEV = 0;
   bool CONV;
   double DELTA, DIFIT = 0., DIFIT1, EPS, FKY, FKZ, FNORM = 0., FNORM1, H, SKNORM, TEMP, XNORM = 0., ETA;
@@ -58,7 +58,7 @@ static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, doubl
     }
 #pragma unroll
     for (int K = 1; K <= N; K++) {
-      FKY = sist3_f(P, s, WA1, K);
+      FKY = sys.f(WA1, K);
       NFCALL = NFCALL + 1;
       NFEV = NFCALL / N;
       FNORM = dmax1(FNORM, fabs(FKY));
@@ -66,7 +66,7 @@ static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, doubl
       for (int J = K; J <= N; J++) {
 #pragma unroll
         for (int I = 1; I <= N; I++) WA2[I - 1] = WA1[I - 1] + QQ(I, J);
-        FKZ = sist3_f(P, s, WA2, K);
+        FKZ = sys.f(WA2, K);
         NFCALL = NFCALL + 1;
         NFEV = NFCALL / N;
         SIGMA[J - 1] = FKZ - FKY;
@@ -140,7 +140,7 @@ static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, doubl
 #pragma unroll
       for (int K = 1; K <= N; K++) {
         if (!stop_refine) {
-          FKY = sist3_f(P, s, WA1, K);
+          FKY = sys.f(WA1, K);
           NFCALL = NFCALL + 1;
           NFEV = NFCALL / N;
           FNORM = dmax1(FNORM, fabs(FKY));
@@ -177,6 +177,462 @@ static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, doubl
 #undef QQ
   *nfev_out = NFEV;
   return INFO;
+}
+
+struct Sist3F {
+  const DevPhys& P;
+  const Sist3& s;
+  __device__ double f(const double* X, int K) const { return sist3_f(P, s, X, K); }
+};
+static __device__ int brentm3(const DevPhys& P, const Sist3& s, double* X, double FTOL, double XTOL, int MAXFEV,
+                              int MOPT, int* nfev_out) {
+  Sist3F sys{P, s};
+  return brentm<3>(sys, X, FTOL, XTOL, MAXFEV, MOPT, nfev_out);
+}
+
+// ---------------------------------------------------------------------------
+// The other ideal-MHD inversions, algo_solver 2..6 (system.f90:732-1158),
+// out of line: the kernels that run algo 1 or Newton keep their registers.
+// ---------------------------------------------------------------------------
+// sist4 (system.f90:1235-1266): 2x2 in (y, p), x = v^2 from y; every call
+// leaves its x in xinner, which algo 2 reads after BRENTM
+struct Sist4F {
+  const DevPhys& P;
+  double B2, SB2, S2, U, D, xinner;
+  __device__ double f(const double* X, int K) {
+    double yy = X[0], pp = X[1];
+    double xx = (S2 + SB2 * (2. * yy + B2) / (yy * yy)) / ((yy + B2) * (yy + B2));
+    xinner = xx;
+    if (K == 2) {
+      double rh = D * sqrt(1 - xx), en = 0;
+      (void)eos_energy(P, rh, &en, pp);
+      return yy - (pp + en) / (1 - xx);
+    }
+    return yy - pp + 0.5 * (1. + xx) * B2 - 0.5 * SB2 / (yy * yy) - U;
+  }
+};
+
+// eos_energy_with_ders (eos.f90:236-246, 527-584, 1189-1215); de/drho and
+// de/dp are 0 where the reference leaves them unset or zeroes them
+__device__ __forceinline__ int eos_energy_ders(const DevPhys& P, double rh, double* en, double pr, double* dendrh,
+                                               double* dendpr) {
+  *dendrh = 0.;
+  *dendpr = 0.;
+  if (P.eqstate == ECHO_EOS_TABLE) return eos_energy(P, rh, en, pr);
+  if (pr <= P.przero) {
+    *en = P.enezero * pr / P.przero;
+    return 0;
+  }
+  if (P.eqstate == ECHO_EOS_CONFORMAL) {
+    *en = 3. * pr;
+    *dendpr = 3.;
+  } else {
+    *en = rh + pr / (4.0 / 3.0 - 1.);
+    *dendrh = 1.;
+    *dendpr = 1. / (4.0 / 3.0 - 1.);
+  }
+  return 0;
+}
+
+// getfun (system.f90:2060-2097); Fnorm, which the reference never assigns,
+// is the Euclidean norm of F
+__device__ __forceinline__ void getfun(const DevPhys& P, const Sist3& s, const double* X, double* F, double J[3][3],
+                                       double* Fnorm, int sw) {
+  double xx = X[0], yy = X[1], pp = X[2];
+  double B2 = s.B2, SB2 = s.SB2, S2 = s.S2, U = s.U, D = s.D;
+  F[0] = (yy + B2) * (yy + B2) * xx - SB2 / (yy * yy) * (2 * yy + B2) - S2;
+  F[1] = yy - pp + 0.5 * (1. + xx) * B2 - 0.5 * SB2 / (yy * yy) - U;
+  double rh = D * sqrt(1 - xx), en = 0, dendrh = 0, dendpr = 0;
+  (void)eos_energy_ders(P, rh, &en, pp, &dendrh, &dendpr);
+  F[2] = yy - (pp + en) / (1 - xx);
+  *Fnorm = sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+  if (sw == 0) return;
+  J[0][0] = (yy + B2) * (yy + B2);
+  J[0][1] = 2 * (yy + B2) * xx + (2 * SB2 * (2 * yy + B2)) / (yy * yy * yy) - 2 * SB2 / (yy * yy);
+  J[0][2] = dendrh * (-D / (2. * sqrt(1. - xx)));
+  J[1][0] = B2 / 2.;
+  J[1][1] = 1. + SB2 / (yy * yy * yy);
+  J[1][2] = -1.;
+  J[2][0] = -(pp + en) / ((1 - xx) * (1 - xx));
+  J[2][1] = 1.;
+  J[2][2] = -(1 + dendpr) / (1 - xx);
+}
+
+// ludecompose and solve (system.f90:1924-1986, 2026-2058), the pivot test as
+// written (the pivot starts as A(i,i), not its modulus); A becomes U
+__device__ __forceinline__ void ludecompose(double A[3][3], double L[3][3], int Pm[3], double smallvalue) {
+  const int n = 3;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) L[i][j] = 0.;
+  for (int i = 0; i < n; i++) Pm[i] = i;
+  for (int i = 0; i < n; i++) L[i][i] = 1.;
+  for (int i = 0; i < n - 1; i++) {
+    double piv = A[i][i];
+    int indP = -1;
+    for (int j = i; j < n; j++)
+      if (fabs(A[j][i]) > piv) {
+        piv = A[j][i];
+        indP = j;
+      }
+    if (indP >= 0) {
+      int t = Pm[i];
+      Pm[i] = Pm[indP];
+      Pm[indP] = t;
+      for (int k = i; k < n; k++) {
+        double x = A[i][k];
+        A[i][k] = A[indP][k];
+        A[indP][k] = x;
+      }
+      for (int k = 0; k < i; k++) {
+        double x = L[i][k];
+        L[i][k] = L[indP][k];
+        L[indP][k] = x;
+      }
+    }
+    for (int j = i + 1; j < n; j++) {
+      double m = A[j][i] / piv;
+      L[j][i] = m;
+      for (int k = i; k < n; k++) {
+        A[j][k] = A[j][k] - m * A[i][k];
+        if (fabs(A[j][k]) <= smallvalue) A[j][k] = 0.;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void lusolve(double L[3][3], double U[3][3], const int Pm[3], double* X, const double* B) {
+  const int n = 3;
+  double Z[3];
+  Z[0] = B[Pm[0]];
+  for (int i = 1; i < n; i++) {
+    double rowsum = B[Pm[i]];
+    for (int k = 0; k < i; k++) rowsum = rowsum - L[i][k] * Z[k];
+    Z[i] = rowsum;
+  }
+  X[n - 1] = Z[n - 1] / U[n - 1][n - 1];
+  for (int j = 1; j <= n - 1; j++) {
+    int i = n - 1 - j;
+    double rowsum = Z[i];
+    for (int k = i + 1; k < n; k++) rowsum = rowsum - U[i][k] * X[k];
+    X[i] = rowsum / U[i][i];
+  }
+}
+
+// solver7 / solver8 (system.f90:2102-2201) and rtsafe (:2227-2286)
+struct RtCtx {
+  double B2, SB2, S2, UU, D, gam, w;
+  int which;  // 7: ideal gas, 8: p = e/3
+};
+__device__ __forceinline__ void rt_func(RtCtx& c, double x, double* f, double* df) {
+  const double third = 1.0 / 3.0;
+  double B2 = c.B2, SB2 = c.SB2, S2 = c.S2, UU = c.UU, D = c.D, gam = c.gam;
+  double v2 = x, rho = 0, c0, c2, c3, dw, dlogw, dc2, dc3, wb, vb2, w;
+  c3 = 1.0 - gam * (1.0 - v2);
+  if (c.which == 7) {
+    rho = D * sqrt(1.0 - v2);
+    c2 = gam * rho + .5 * B2 * (1.0 + v2) - UU;
+  } else {
+    c2 = .5 * B2 * (1.0 + v2) - UU;
+  }
+  c0 = -0.5 * SB2;
+  if (c.which == 8 && c0 == 0.0) {
+    w = -c2 / c3;
+  } else {
+    w = fmax(-c2 / c3, pow(-c0 / c3, third));
+    int maxit = c.which == 7 ? 50 : 100;
+    double wtol = c.which == 7 ? 1.e-10 : 1.e-12;
+    for (int iter = 1; iter <= maxit; iter++) {
+      dw = -((c3 * w + c2) * (w * w) + c0) / ((3 * c3 * w + 2 * c2) * w);
+      if (fabs(dw / w) < wtol) break;
+      w = w + dw;
+    }
+  }
+  dc3 = gam;
+  if (c.which == 7)
+    dc2 = .5 * (B2 - gam * rho / (1. - v2));
+  else
+    dc2 = .5 * B2;
+  dlogw = -(dc3 * w + dc2) / (3 * c3 * w + 2 * c2);
+  wb = w + B2;
+  vb2 = SB2 / (w * w);
+  *f = wb * wb * v2 - (2 * w + B2) * vb2 - S2;
+  *df = wb * (wb + 2 * dlogw * (w * v2 + vb2));
+  c.w = w;
+}
+__device__ __forceinline__ double rtsafe(RtCtx& c, double x0, double x1, double x2, double xacc, int* ierr) {
+  double f, df, xl = x1, xh = x2, dx, dxold, temp, r = x0;
+  *ierr = 0;
+  dxold = fabs(x2 - x1);
+  dx = dxold;
+  rt_func(c, r, &f, &df);
+  for (int j = 1; j <= 100; j++) {
+    if (((r - xh) * df - f) * ((r - xl) * df - f) > 0. || fabs(2. * f) > fabs(dxold * df)) {
+      dxold = dx;
+      dx = 0.5 * (xh - xl);
+      r = xl + dx;
+      if (xl == r) {
+        rt_func(c, r, &f, &df);
+        return r;
+      }
+    } else {
+      dxold = dx;
+      dx = f / df;
+      temp = r;
+      r = r - dx;
+      if (temp == r) {
+        rt_func(c, r, &f, &df);
+        return r;
+      }
+    }
+    if (fabs(dx) < xacc) return r;
+    rt_func(c, r, &f, &df);
+    if (f < 0.)
+      xl = r;
+    else
+      xh = r;
+  }
+  *ierr = 1;
+  return r;
+}
+
+// solver10_approximate (system.f90:2205-2223) and get_x9 (:2290-2297); 12
+// only when the exit test is met on the last allowed iteration, as written
+__device__ __forceinline__ int solver10_approximate(double b, double c, double d, double oldsol, double* x) {
+  int iter;
+  *x = oldsol;
+  for (iter = 1; iter <= 100; iter++) {
+    double xx = *x;
+    double dx = -(12 * (xx * xx * xx) + 3 * b * (xx * xx) + 2 * c * xx + d);
+    if (fabs(dx / xx) < 1.e-12) break;
+    *x = xx + dx;
+  }
+  return iter == 100 ? 12 : 0;
+}
+__device__ __forceinline__ double get_x9(double y, double s2, double b2, double sb2) {
+  return (s2 * (y * y) + b2 * sb2 + 2 * sb2 * y) / ((y * y) * ((b2 * b2) + 2 * b2 * y + (y * y)));
+}
+
+// algo_solver 2..6; the reference's exit() calls become codes: 8 (algo 3
+// out of iterations), 12 (algo 6 without a solution), 11 (no such solver).
+// v[0..NV) in/out (guess in), u: conserved of the cell.
+template <int KIND>
+static __device__ __noinline__ int cons2prim_mhd_algo(const DevPhys& P, const Metric& M, int algo, const double* u,
+                                                      double* v, int* iters) {
+  typedef Traits<KIND> T;
+  const double eps = 1.e-12;
+  double g1 = M.g1, g2 = M.g2, g3 = M.g3, gm = M.gm;
+  double uin[T::NV];
+#pragma unroll
+  for (int k = 0; k < T::NV; k++) uin[k] = gm * u[k];
+  double DD = uin[KRH], sx = uin[KVX], sy = uin[KVY], sz = uin[KVZ], UU = uin[KPR];
+  double bx = uin[KBX], by = uin[KBY], bz = uin[KBZ];
+  int errcode = 0;
+  *iters = 0;
+  if (algo == 2 || algo == 3) {
+    v[KBX] = uin[KBX];
+    v[KBY] = uin[KBY];
+    v[KBZ] = uin[KBZ];
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = sx * bx + sy * by + sz * bz;
+    double SB2 = SB * SB;
+    double SS2 = sx * sx + sy * sy + sz * sz / g3;
+    double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR], en = 0;
+    errcode = eos_energy(P, rh, &en, pr);
+    double xs, ys;
+    if (algo == 2) {
+      double v2old = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+      double X[2] = {(en + pr) / (1 - v2old), pr};
+      Sist4F sys{P, B2, SB2, SS2, UU, DD, 0.};
+      int nfev = 0;
+      (void)brentm<2>(sys, X, 1.e-14, 1.e-14, 300, 3, &nfev);
+      *iters = nfev;
+      ys = X[0];
+      pr = X[1];
+      xs = sys.xinner;
+    } else {
+      double v2 = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+      double X[3] = {v2, (en + pr) / (1 - v2), pr}, F[3], J[3][3], L[3][3], DX[3], mF[3], Xt[3];
+      double Fnorm = 0, Fnl = 0;
+      int Pm[3], it = 0;
+      Sist3 s3 = {B2, SB2, SS2, UU, DD, 0.};
+      getfun(P, s3, X, F, J, &Fnorm, 1);
+      while (Fnorm >= 1.e-14) {
+        ludecompose(J, L, Pm, 4.e-16);
+        for (int i = 0; i < 3; i++) mF[i] = -F[i];
+        lusolve(L, J, Pm, DX, mF);
+        double lambda = 1.;
+        for (int i = 0; i < 3; i++) Xt[i] = X[i] + lambda * DX[i];
+        getfun(P, s3, Xt, F, J, &Fnl, 1);
+        if ((Fnl > (1 - lambda / 2) * Fnorm) && (lambda > 1. / 64)) {
+          for (;;) {
+            lambda = lambda / 2.;
+            for (int i = 0; i < 3; i++) Xt[i] = X[i] + lambda * DX[i];
+            getfun(P, s3, Xt, F, J, &Fnl, 0);
+            if (!((Fnl > (1 - lambda / 2) * Fnorm) && (lambda > 1. / 64))) {
+              for (int i = 0; i < 3; i++) X[i] = X[i] + lambda * DX[i];
+              Fnorm = Fnl;
+              break;
+            }
+          }
+        } else {
+          for (int i = 0; i < 3; i++) X[i] = X[i] + lambda * DX[i];
+          Fnorm = Fnl;
+        }
+        it = it + 1;
+        if (it > 300) {
+          *iters = it;
+          return 8;
+        }
+      }
+      *iters = it;
+      xs = X[0];
+      ys = X[1];
+      pr = X[2];
+    }
+    rh = DD * sqrt(1 - xs);
+    v[KRH] = rh;
+    v[KVX] = (sx + SB * bx / ys) / (ys + B2);
+    v[KVY] = (sy + SB * by / ys) / (ys + B2);
+    v[KVZ] = (sz / g3 + SB * bz / ys) / (ys + B2);
+    v[KPR] = pr;
+    if (T::GLM) v[T::KG] = u[T::KG];
+    return errcode;
+  }
+  if (algo == 4 || algo == 5) {
+    double S2 = sx * sx + sy * sy + sz * sz / g3;
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = (sx * bx + sy * by + sz * bz);
+    double SB2 = SB * SB;
+    RtCtx c{B2, SB2, S2, UU, DD, algo == 4 ? (4.0 / 3.0 - 1) / (4.0 / 3.0) : 0.25, 0., algo == 4 ? 7 : 8};
+    double v2_old = algo == 4 ? v[KVX] * v[KVX] + v[KVY] * v[KVY] + v[KVZ] * v[KVZ]
+                              : v[KVX] * v[KVX] + v[KVY] * v[KVY] + v[KVZ] * v[KVZ] * g3;
+    int ierr = 0;
+    double v2 = rtsafe(c, v2_old, 0., 1. - 1.e-11, 1.e-12, &ierr);
+    if (algo == 4 && ierr > 0) return 0;  // system.f90:926: returns, v untouched
+    if (algo == 5 && ((v2 >= 1) || (ierr > 0))) return 778;
+#pragma unroll
+    for (int k = 0; k < T::NV; k++) v[k] = uin[k];
+    if (T::GLM) v[T::KG] = u[T::KG];
+    double w = c.w, rh = DD * sqrt(1. - v2);
+    v[KRH] = rh;
+    if (algo == 4) {
+      double pg = c.gam * (w * (1. - v2) - rh);
+      v[KPR] = fmax(pg, eps);
+    } else {
+      v[KPR] = 0.25 * (1 - v2) * w;
+    }
+    double vb = SB / w;
+    v[KVX] = (sx + vb * bx) / (w + B2);
+    v[KVY] = (sy + vb * by) / (w + B2);
+    v[KVZ] = (sz / g3 + vb * bz) / (w + B2);
+    return 0;
+  }
+  if (algo == 6) {
+    bool exact9 = true;
+    double v2_old = v[KVX] * v[KVX] + v[KVY] * v[KVY] + v[KVZ] * v[KVZ];
+    double oldsol9 = 4 * v[KPR] / (1 - v2_old);
+    double S2 = sx * sx + sy * sy + sz * sz;
+    double B2 = bx * bx + by * by + bz * bz;
+    double SB = (sx * bx + sy * by + sz * bz);
+    double SB2 = SB * SB;
+    double b9 = 8 * B2 - 4 * UU;
+    double c9 = 7 * (B2 * B2) - 8 * B2 * UU + S2;
+    double d9 = 2 * (B2 * B2 * B2) - 4 * (B2 * B2) * UU + 2 * B2 * S2;
+    double e9 = SB2 * B2;
+    double p9 = (24 * c9 - 3 * (b9 * b9)) / 72;
+    double q9 = ((b9 * b9 * b9) - 12 * b9 * c9 + 72 * d9) / 216;
+    double dnull9 = (c9 * c9) - 3 * b9 * d9 + 36 * e9;
+    double deinz9 = 2 * (c9 * c9 * c9) - 9 * b9 * c9 * d9 + 27 * (b9 * b9) * e9 + 81 * (d9 * d9) - 216 * c9 * e9;
+    double discr9 = (deinz9 * deinz9) - 4 * (dnull9 * dnull9 * dnull9);
+    double sbig9 = 0., sol9 = -1., v2 = 0.;
+    if (discr9 > 0) {
+      double droot9 = sqrt(discr9);
+      double qbig9 = pow(0.5 * (deinz9 + droot9), 1. / 3.);
+      double drad9 = -2 * p9 / 3 + (qbig9 + dnull9 / qbig9) / 9;
+      if (drad9 <= 0) return 12;
+      sbig9 = 0.5 * sqrt(drad9);
+    } else if (dnull9 > 0) {
+      double phi9 = acos(deinz9 / (2 * sqrt(dnull9 * dnull9 * dnull9)));
+      sbig9 = 0.5 * sqrt(-2. * p9 / 3 + 2. / 9. * sqrt(dnull9) * cos(phi9 / 3.));
+    } else {
+      if (solver10_approximate(b9, c9, d9, oldsol9, &sol9)) return 12;
+      exact9 = false;
+      v2 = get_x9(sol9, S2, B2, SB2);
+      if ((v2 < 0) || (v2 > 1) || (sol9 < 0)) return 12;
+    }
+    if (exact9) {
+      // sol1..sol4 start at -1 (the reference leaves those of a negative
+      // radicand unset)
+      double sol1 = -1., sol2 = -1., sol3 = -1., sol4 = -1.;
+      double rad129 = -4 * (sbig9 * sbig9) - 2 * p9 + q9 / sbig9;
+      double rad349 = -4 * (sbig9 * sbig9) - 2 * p9 - q9 / sbig9;
+      double rapp9 = -b9 / 12;
+      if (rad129 >= 0) {
+        double root129 = 0.5 * sqrt(rad129);
+        sol1 = rapp9 - sbig9 - root129;
+        sol2 = rapp9 - sbig9 + root129;
+      }
+      if (rad349 >= 0) {
+        double root349 = 0.5 * sqrt(rad349);
+        sol3 = rapp9 + sbig9 - root349;
+        sol4 = rapp9 + sbig9 + root349;
+      }
+      double dist9 = 1.e100, v9;
+      sol9 = -1.;
+      if (sol2 > 0) {
+        v9 = get_x9(sol2, S2, B2, SB2);
+        if ((v9 >= 0) && (v9 < 1)) {
+          sol9 = sol2;
+          v2 = v9;
+          dist9 = fabs(oldsol9 - sol9);
+          if (sol1 > 0) {
+            v9 = get_x9(sol1, S2, B2, SB2);
+            if ((v9 >= 0) && (v9 < 1)) {
+              double d19 = fabs(oldsol9 - sol1);
+              if (d19 <= dist9) {
+                sol9 = sol1;
+                dist9 = d19;
+                v2 = v9;
+              }
+            }
+          }
+        }
+      }
+      if (sol4 > 0) {
+        v9 = get_x9(sol4, S2, B2, SB2);
+        if ((v9 >= 0) && (v9 < 1)) {
+          double d49 = fabs(oldsol9 - sol4);
+          if (d49 <= dist9) {
+            sol9 = sol4;
+            dist9 = d49;
+            v2 = v9;
+          }
+        }
+        if (sol3 > 0) {
+          v9 = get_x9(sol3, S2, B2, SB2);
+          if ((v9 >= 0) && (v9 < 1)) {
+            double d39 = fabs(oldsol9 - sol3);
+            if (d39 <= dist9) {
+              sol9 = sol3;
+              dist9 = d39;
+              v2 = v9;
+            }
+          }
+        }
+      }
+      if (sol9 < 0) return 12;
+    }
+#pragma unroll
+    for (int k = 0; k < T::NV; k++) v[k] = uin[k];
+    v[KRH] = DD * sqrt(1. - v2);
+    v[KPR] = sol9 / 4 * (1 - v2);
+    double vb = SB / sol9;
+    v[KVX] = (sx + vb * bx) / (sol9 + B2);
+    v[KVY] = (sy + vb * by) / (sol9 + B2);
+    v[KVZ] = (sz + vb * bz) / (sol9 + B2);
+    if (T::GLM) v[T::KG] = u[T::KG];
+    return 0;
+  }
+  return 11;
 }
 
 // ---------------------------------------------------------------------------
@@ -430,9 +886,16 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
 // system_cons2prim (system.f90:423-1166).  u, v of length NV; v holds the
 // initial guess.  Returns the reference errcode; *iters gets the iteration
 // count (Newton steps, or BRENTM function evaluations).  h: the implicit
-// coefficient of a resistive IMEX stage (cons2prim_res).
+// coefficient of a resistive IMEX stage (cons2prim_res).  ALT: the
+// instantiation that also runs ALG_SOLV 2..6 (cons2prim_mhd_algo); the step
+// kernels use the other one and leave those algorithms to c2p_alt_kernel, so
+// that the out-of-line call does not cost them registers.
 // ---------------------------------------------------------------------------
-template <int KIND>
+__host__ __device__ __forceinline__ bool c2p_alt_algo(int algo) {
+  return algo != ECHO_C2P_BRENT && algo != ECHO_C2P_NEWTON && algo != ECHO_C2P_MLP;
+}
+
+template <int KIND, bool ALT = false>
 __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol, const double* u,
                          double* v, int* iters, const float* seed = nullptr, int* seed_failed = nullptr,
                          double h = 0.) {
@@ -555,6 +1018,9 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     return errcode;
   } else {
     // ideal MHD (system.f90:668-730): BRENTM on sist3, or Newton on the same system
+    if constexpr (ALT && T::MHD && !T::RES) {
+      if (c2p_alt_algo(algo)) return cons2prim_mhd_algo<KIND>(P, M, algo, u, v, iters);
+    }
     double uin[T::NV];
 #pragma unroll
     for (int k = 0; k < T::NV; k++) uin[k] = gm * u[k];

@@ -735,7 +735,7 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
       mlp_seed<KIND>(A.mlp, M, active, uu, seed);
       sp = seed;
     }
-    if (active) {
+    if (active && !(T::MHD && !T::RES && c2p_alt_algo(A.algo))) {  // ALG_SOLV 2..6: c2p_alt_kernel
       // con2prim (evolve_u2v, evolve.f90:789-866)
       int it = 0, sfail = 0;
       int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail);
@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_combine_kernel(SspArgs
     mlp_seed<KIND>(A.mlp, M, active, uu, seed);
     sp = seed;
   }
-  if (active) {
+  if (active && !(T::MHD && !T::RES && c2p_alt_algo(A.algo))) {  // ALG_SOLV 2..6: c2p_alt_kernel
     int it = 0;
     // the implicit stages of a resistive run solve Ohm's law in con2prim
     const double h = (T::RES && A.stage < 5) ? alpha_imex * dt : 0.;
@@ -906,6 +906,41 @@ __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_stage1_kernel(SspArgs 
 // ---------------------------------------------------------------------------
 // repair of failed cells (evolve.f90:795-842) in Fortran loop order
 // ---------------------------------------------------------------------------
+// con2prim of every cell with ALG_SOLV 2..6 (the step kernels wrote u and
+// skipped the inversion): the same flags, counters and outputs as theirs
+template <int KIND>
+__global__ void __launch_bounds__(128) c2p_alt_kernel(DevPhys P, Grid g, int coordinates, int algo, double tol,
+                                                     DevScalars* sc, const double* __restrict__ u,
+                                                     const double* __restrict__ vin, double* __restrict__ vout,
+                                                     unsigned char* fail) {
+  typedef Traits<KIND> T;
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long my_iters = 0;
+  if (c < g.ncell) {
+    const Metric M = make_metric(coordinates, sc->t, sc->t3);
+    double uu[T::NV], vv[T::NV];
+#pragma unroll
+    for (int k = 0; k < T::NV; k++) {
+      uu[k] = u[(size_t)k * g.ncell + c];
+      vv[k] = vin[(size_t)k * g.ncell + c];
+    }
+    int it = 0;
+    int err = cons2prim<KIND, true>(P, M, algo, tol, uu, vv, &it);
+    my_iters = (unsigned long long)it;
+    if (err) {
+      fail[c] = 1;
+      atomicAdd(&sc->nfail, 1);
+    } else {
+      fail[c] = 0;
+#pragma unroll
+      for (int k = 0; k < T::NV; k++) vout[(size_t)k * g.ncell + c] = vv[k];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+  if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&sc->c2p_iters, my_iters);
+}
+
 struct RepairArgs {
   DevPhys P;
   Grid g;
@@ -960,7 +995,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
         int it;
         for (int k = 0; k < NV; k++) vv[k] = A.vold[(size_t)k * g.ncell + cell];
         for (int k = 0; k < NV; k++) uu[k] = A.u[(size_t)k * g.ncell + cell];
-        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
+        (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
         size_t totu = g.ncell * NV;
         long long nx = g.nx, nxy = (long long)g.nx * g.ny;
         for (int k = 0; k < NV; k++) {
@@ -970,7 +1005,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
           A.u[o] = s / 6.;
           uu[k] = A.u[o];
         }
-        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
+        (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
         double v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
         if (v2 > 1) {
           double fac = A.maxspeed / sqrt(v2);
@@ -986,7 +1021,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
           vv[KPR] = (pxl + pxr + pyl + pyr + pzl + pzr) / 6.;
         }
         (void)prim2cons<KIND>(A.P, M, vv, uu);
-        (void)cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
+        (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
         v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
         bool ok = (vv[KPR] > 0) && (v2 < 1);
         if (T::VISC && A.P.obtained_zz) A.vnew[(size_t)KPIZZ * g.ncell + cell] = vv[KPIZZ];

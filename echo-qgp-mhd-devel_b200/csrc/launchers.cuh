@@ -86,6 +86,9 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
     update_kernel<KIND, false, Traits<KIND>::VISC><<<blocks, 128, 0, c->stream>>>(A);
   else
     update_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
+  if (Traits<KIND>::MHD && !Traits<KIND>::RES && mode == MODE_RK && c2p_alt_algo(A.algo))
+    c2p_alt_kernel<KIND><<<blocks, 128, 0, c->stream>>>(c->P, c->g, c->p.coordinates, A.algo, A.tol, c->d_sc, A.uout,
+                                                         A.vin, A.vout, c->d_fail);
 }
 
 template <int KIND>
@@ -163,6 +166,9 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
     ssp_combine_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
   else
     ssp_combine_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
+  if (Traits<KIND>::MHD && !Traits<KIND>::RES && c2p_alt_algo(A.algo))
+    c2p_alt_kernel<KIND><<<blocks, 128, 0, c->stream>>>(c->P, c->g, c->p.coordinates, A.algo, A.tol, c->d_sc, A.uout,
+                                                         A.vin, A.vout, c->d_fail);
 }
 
 // resistive IMEX-SSP first stage: the implicit solve from u^n (U[ucur]) and

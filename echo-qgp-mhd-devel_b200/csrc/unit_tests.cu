@@ -52,7 +52,7 @@ __global__ void c2p_test_kernel(DevPhys P, Metric M, int algo, double tol, int n
     vv[k] = v[(size_t)c * T::NV + k];
   }
   int it = 0;
-  int e = cons2prim<KIND>(P, M, algo, tol, uu, vv, &it);
+  int e = cons2prim<KIND, true>(P, M, algo, tol, uu, vv, &it);
   for (int k = 0; k < T::NV; k++) v[(size_t)c * T::NV + k] = vv[k];
   if (err) err[c] = e;
   if (iters) iters[c] = it;

@@ -56,7 +56,9 @@ enum { ECHO_EOS_CONFORMAL = 1, ECHO_EOS_IDEALGAS = 2, ECHO_EOS_TABLE = 3 };
 
 /* con2prim solvers for ideal MHD (ALG_SOLV, common.f90:289) */
 enum {
-  ECHO_C2P_BRENT = 1,   /* reference default: BRENTM on (v^2, w*gamma^2, p) */
+  ECHO_C2P_BRENT = 1,   /* reference default: BRENTM on (v^2, w*gamma^2, p);
+                           2..6 are the reference's other ideal-MHD solvers
+                           (system.f90:732-1158), single grid only */
   ECHO_C2P_NEWTON = 100, /* this library: analytic-Jacobian Newton from the
                             previous primitives, same root; BRENTM fallback */
   ECHO_C2P_MLP = 101     /* Newton from the learned seed (<= 3 steps), then the

@@ -810,10 +810,13 @@ static double dmax1(double a, double b) { return b > a ? b : a; }
 static double dsign(double a, double b) { return copysign(fabs(a), b); }
 
 /* returns INFO; *nfev_out = NFEV */
-static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL,
-                   double XTOL, int MAXFEV, int MOPT, int* nfev_out) {
-  enum { N = 3, LDQ = 3 };
-  double Q[LDQ * N], SIGMA[N], WA1[N], WA2[N];
+/* the system a BRENTM call solves: F(K) of X, as sist3 / sist4 */
+typedef void (*SysFn)(void* ctx, const double* X, double* F, int K);
+
+static int brentm(int N, SysFn fn, void* ctx, double* X, double* FVEC, double FTOL,
+                  double XTOL, int MAXFEV, int MOPT, int* nfev_out) {
+  const int LDQ = N;
+  double Q[9], SIGMA[3], WA1[3], WA2[3];
 #define QQ(i, j) Q[((j)-1) * LDQ + ((i)-1)]
   int I, J, K, M, NFCALL, NIER6, NIER7, NIER8, NSING, INFO, NFEV, IFLAG;
   int CONV;
@@ -849,14 +852,14 @@ static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL,
     }
     for (K = 1; K <= N; K++) {
       IFLAG = K;
-      sist3(s, WA1, FVEC, IFLAG);
+      fn(ctx, WA1, FVEC, IFLAG);
       FKY = FVEC[K - 1];
       NFCALL = NFCALL + 1;
       NFEV = NFCALL / N;
       FNORM = dmax1(FNORM, fabs(FKY));
       for (J = K; J <= N; J++) {
         for (I = 1; I <= N; I++) WA2[I - 1] = WA1[I - 1] + QQ(I, J);
-        sist3(s, WA2, FVEC, IFLAG);
+        fn(ctx, WA2, FVEC, IFLAG);
         FKZ = FVEC[K - 1];
         NFCALL = NFCALL + 1;
         NFEV = NFCALL / N;
@@ -922,7 +925,7 @@ static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL,
       FNORM = ZERO;
       for (K = 1; K <= N; K++) {
         IFLAG = K;
-        sist3(s, WA1, FVEC, IFLAG);
+        fn(ctx, WA1, FVEC, IFLAG);
         FKY = FVEC[K - 1];
         NFCALL = NFCALL + 1;
         NFEV = NFCALL / N;
@@ -957,6 +960,13 @@ static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL,
 #undef QQ
   *nfev_out = NFEV;
   return INFO;
+}
+
+static void sist3_fn(void* ctx, const double* X, double* F, int K) { sist3((const Sist3*)ctx, X, F, K); }
+
+static int brentm3(const Sist3* s, double* X, double* FVEC, double FTOL, double XTOL, int MAXFEV, int MOPT,
+                   int* nfev_out) {
+  return brentm(3, sist3_fn, (void*)s, X, FVEC, FTOL, XTOL, MAXFEV, MOPT, nfev_out);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1046,9 +1056,467 @@ static int cons2prim_res(const Phys* ph, double* u, double* v, int* iters) {
   return errcode;
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* the other MHD inversions, algo_solver 2..6 (system.f90:732-1158)          */
+/* ------------------------------------------------------------------------ */
+/* sist4 (system.f90:1235-1266): the 2x2 system in (y, p) with x = v^2 from
+   y; every call leaves its x in xinner, which algo 2 reads after BRENTM */
+typedef struct Sist4 {
+  const Phys* ph;
+  double B2, SB2, S2, U, D, xinner;
+} Sist4;
+
+static void sist4_fn(void* ctx, const double* X, double* F, int K) {
+  Sist4* s = (Sist4*)ctx;
+  double yy = X[0], pp = X[1];
+  double xx = (s->S2 + s->SB2 * (2. * yy + s->B2) / (yy * yy)) / ((yy + s->B2) * (yy + s->B2));
+  s->xinner = xx;
+  if (K == 2) {
+    double rh = s->D * sqrt(1 - xx), en = 0;
+    (void)eos_energy(s->ph, rh, &en, pp);
+    F[1] = yy - (pp + en) / (1 - xx);
+  }
+  if (K == 1) F[0] = yy - pp + 0.5 * (1. + xx) * s->B2 - 0.5 * s->SB2 / (yy * yy) - s->U;
+}
+
+/* eos_energy_with_ders (eos.f90:236-246, 527-584, 1189-1215): e and its
+   derivatives.  The tabulated routine sets de/dp = 0 and leaves de/drho
+   unset, as does the analytic one below p(ENEZERO): both are 0 here. */
+static int eos_energy_ders(const Phys* ph, double rh, double* en, double pr, double* dendrh, double* dendpr) {
+  const EchoParams* p = ph->p;
+  *dendrh = 0.;
+  *dendpr = 0.;
+  if (p->eqstate == ECHO_EOS_TABLE) return eos_energy(ph, rh, en, pr);
+  if (pr <= p->przero) {
+    *en = p->enezero * pr / p->przero;
+    return 0;
+  }
+  if (p->eqstate == ECHO_EOS_CONFORMAL) {
+    *en = 3. * pr;
+    *dendpr = 3.;
+  } else {
+    *en = rh + pr / (4.0 / 3.0 - 1.);
+    *dendrh = 1.;
+    *dendpr = 1. / (4.0 / 3.0 - 1.);
+  }
+  return 0;
+}
+
+/* getfun (system.f90:2060-2097): F(X) of sist3 and, for sw = 1, the
+   reference's Jacobian.  The reference never assigns Fnorm (an intent(out)
+   it reads back); it is the Euclidean norm of F here. */
+static void getfun(const Sist3* s, const double* X, double* F, double J[3][3], double* Fnorm, int sw) {
+  double xx = X[0], yy = X[1], pp = X[2];
+  double B2 = s->B2, SB2 = s->SB2, S2 = s->S2, U = s->U, D = s->D;
+  F[0] = (yy + B2) * (yy + B2) * xx - SB2 / (yy * yy) * (2 * yy + B2) - S2;
+  F[1] = yy - pp + 0.5 * (1. + xx) * B2 - 0.5 * SB2 / (yy * yy) - U;
+  double rh = D * sqrt(1 - xx), en = 0, dendrh = 0, dendpr = 0;
+  (void)eos_energy_ders(s->ph, rh, &en, pp, &dendrh, &dendpr);
+  F[2] = yy - (pp + en) / (1 - xx);
+  *Fnorm = sqrt(F[0] * F[0] + F[1] * F[1] + F[2] * F[2]);
+  if (sw == 0) return;
+  J[0][0] = (yy + B2) * (yy + B2);
+  J[0][1] = 2 * (yy + B2) * xx + (2 * SB2 * (2 * yy + B2)) / (yy * yy * yy) - 2 * SB2 / (yy * yy);
+  J[0][2] = dendrh * (-D / (2. * sqrt(1. - xx)));
+  J[1][0] = B2 / 2.;
+  J[1][1] = 1. + SB2 / (yy * yy * yy);
+  J[1][2] = -1.;
+  J[2][0] = -(pp + en) / ((1 - xx) * (1 - xx));
+  J[2][1] = 1.;
+  J[2][2] = -(1 + dendpr) / (1 - xx);
+}
+
+/* ludecompose (system.f90:1924-1986), its pivot test included: the pivot
+   starts as A(i,i) itself, not its modulus.  A becomes U. */
+static void ludecompose(double A[3][3], double L[3][3], int P[3], double smallvalue) {
+  const int n = 3;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) L[i][j] = 0.;
+  for (int i = 0; i < n; i++) P[i] = i;
+  for (int i = 0; i < n; i++) L[i][i] = 1.;
+  for (int i = 0; i < n - 1; i++) {
+    double piv = A[i][i];
+    int indP = -1;
+    for (int j = i; j < n; j++)
+      if (fabs(A[j][i]) > piv) {
+        piv = A[j][i];
+        indP = j;
+      }
+    if (indP >= 0) {
+      int t = P[i];
+      P[i] = P[indP];
+      P[indP] = t;
+      for (int k = i; k < n; k++) {
+        double x = A[i][k];
+        A[i][k] = A[indP][k];
+        A[indP][k] = x;
+      }
+      for (int k = 0; k < i; k++) {
+        double x = L[i][k];
+        L[i][k] = L[indP][k];
+        L[indP][k] = x;
+      }
+    }
+    for (int j = i + 1; j < n; j++) {
+      double m = A[j][i] / piv;
+      L[j][i] = m;
+      for (int k = i; k < n; k++) {
+        A[j][k] = A[j][k] - m * A[i][k];
+        if (fabs(A[j][k]) <= smallvalue) A[j][k] = 0.;
+      }
+    }
+  }
+}
+
+/* solve (system.f90:2026-2058): L Z = P B, U X = Z */
+static void lusolve(double L[3][3], double U[3][3], const int P[3], double* X, const double* B) {
+  const int n = 3;
+  double Z[3];
+  Z[0] = B[P[0]];
+  for (int i = 1; i < n; i++) {
+    double rowsum = B[P[i]];
+    for (int k = 0; k < i; k++) rowsum = rowsum - L[i][k] * Z[k];
+    Z[i] = rowsum;
+  }
+  X[n - 1] = Z[n - 1] / U[n - 1][n - 1];
+  for (int j = 1; j <= n - 1; j++) {
+    int i = n - 1 - j;
+    double rowsum = Z[i];
+    for (int k = i + 1; k < n; k++) rowsum = rowsum - U[i][k] * X[k];
+    X[i] = rowsum / U[i][i];
+  }
+}
+
+/* solver7 / solver8 (system.f90:2102-2201): for x = v^2 the cubic in W
+   (Newton from the larger root bound), then the residual in v^2 and its
+   derivative; *w the W of this x (the reference's w_algo_solver7/8 global) */
+typedef struct RtCtx {
+  double B2, SB2, S2, UU, D, gam, w;
+  int which; /* 7: ideal gas, 8: p = e/3 */
+} RtCtx;
+
+static void rt_func(RtCtx* c, double x, double* f, double* df) {
+  const double third = 1.0 / 3.0;
+  double B2 = c->B2, SB2 = c->SB2, S2 = c->S2, UU = c->UU, D = c->D;
+  double v2 = x, rho = 0, c0, c2, c3, dw, dlogw, dc2, dc3, wb, vb2, w, gam = c->gam;
+  c3 = 1.0 - gam * (1.0 - v2);
+  if (c->which == 7) {
+    rho = D * sqrt(1.0 - v2);
+    c2 = gam * rho + .5 * B2 * (1.0 + v2) - UU;
+  } else {
+    c2 = .5 * B2 * (1.0 + v2) - UU;
+  }
+  c0 = -0.5 * SB2;
+  if (c->which == 8 && c0 == 0.0) {
+    w = -c2 / c3;
+  } else {
+    w = fmax(-c2 / c3, pow(-c0 / c3, third));
+    int maxit = c->which == 7 ? 50 : 100;
+    double wtol = c->which == 7 ? 1.e-10 : 1.e-12;
+    for (int iter = 1; iter <= maxit; iter++) {
+      dw = -((c3 * w + c2) * (w * w) + c0) / ((3 * c3 * w + 2 * c2) * w);
+      if (fabs(dw / w) < wtol) break;
+      w = w + dw;
+    }
+  }
+  dc3 = gam;
+  if (c->which == 7)
+    dc2 = .5 * (B2 - gam * rho / (1. - v2));
+  else
+    dc2 = .5 * B2;
+  dlogw = -(dc3 * w + dc2) / (3 * c3 * w + 2 * c2);
+  wb = w + B2;
+  vb2 = SB2 / (w * w);
+  *f = wb * wb * v2 - (2 * w + B2) * vb2 - S2;
+  *df = wb * (wb + 2 * dlogw * (w * v2 + vb2));
+  c->w = w;
+}
+
+/* rtsafe (system.f90:2227-2286): safeguarded Newton on [x1, x2] from x0 */
+static double rtsafe(RtCtx* c, double x0, double x1, double x2, double xacc, int* ierr) {
+  const int maxit = 100;
+  double f, df, xl = x1, xh = x2, dx, dxold, temp, r = x0;
+  *ierr = 0;
+  dxold = fabs(x2 - x1);
+  dx = dxold;
+  rt_func(c, r, &f, &df);
+  for (int j = 1; j <= maxit; j++) {
+    if (((r - xh) * df - f) * ((r - xl) * df - f) > 0. || fabs(2. * f) > fabs(dxold * df)) {
+      dxold = dx;
+      dx = 0.5 * (xh - xl);
+      r = xl + dx;
+      if (xl == r) {
+        rt_func(c, r, &f, &df);
+        return r;
+      }
+    } else {
+      dxold = dx;
+      dx = f / df;
+      temp = r;
+      r = r - dx;
+      if (temp == r) {
+        rt_func(c, r, &f, &df);
+        return r;
+      }
+    }
+    if (fabs(dx) < xacc) return r;
+    rt_func(c, r, &f, &df);
+    if (f < 0.)
+      xl = r;
+    else
+      xh = r;
+  }
+  *ierr = 1;
+  return r;
+}
+
+/* solver10_approximate (system.f90:2205-2223): Newton-like iteration on the
+   depressed quartic; 12 (the reference's exit code) only when the exit test
+   is met on the last allowed iteration, as the reference's test reads */
+static int solver10_approximate(double b, double c, double d, double oldsol, double* x) {
+  const int maxiterations = 100;
+  int iter;
+  *x = oldsol;
+  for (iter = 1; iter <= maxiterations; iter++) {
+    double xx = *x;
+    double dx = -(12 * (xx * xx * xx) + 3 * b * (xx * xx) + 2 * c * xx + d);
+    if (fabs(dx / xx) < 1.e-12) break;
+    *x = xx + dx;
+  }
+  return iter == maxiterations ? 12 : 0;
+}
+
+static double get_x9(double y, double s2, double b2, double sb2) { /* system.f90:2290-2297 */
+  return (s2 * (y * y) + b2 * sb2 + 2 * sb2 * y) / ((y * y) * ((b2 * b2) + 2 * b2 * y + (y * y)));
+}
+
+/* algo_solver 2..6 of the ideal-MHD inversion (system.f90:732-1158); the
+   reference's exit() calls become error codes: 8 (algo 3 out of
+   iterations), 12 (algo 6 without a solution), 11 (no such solver) */
+static int cons2prim_mhd_algo(const Phys* ph, double* u, double* v, int* iters) {
+  const EchoParams* p = ph->p;
+  const double eps = 1.e-12;
+  int algo = p->algo_solver, nu = ph->nu, nv = ph->nv, kbx = ph->kbx, kby = ph->kby, kbz = ph->kbz;
+  double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gm = ph->gm;
+  double uin[ECHO_MAX_NV];
+  for (int k = 0; k < nu; k++) uin[k] = gm * u[k];
+  double DD = uin[KRH], sx = uin[KVX], sy = uin[KVY], sz = uin[KVZ], UU = uin[KPR];
+  double bx = uin[kbx], by = uin[kby], bz = uin[kbz];
+  int errcode = 0;
+  *iters = 0;
+  if (algo == 2 || algo == 3) {
+    v[kbx] = uin[kbx];
+    v[kby] = uin[kby];
+    v[kbz] = uin[kbz];
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = sx * bx + sy * by + sz * bz;
+    double SB2 = SB * SB;
+    double SS2 = sx * sx + sy * sy + sz * sz / g3;
+    double rh = v[KRH], vx = v[KVX], vy = v[KVY], vz = v[KVZ], pr = v[KPR], en = 0;
+    errcode = eos_energy(ph, rh, &en, pr);
+    double xs, ys;
+    if (algo == 2) {
+      double v2old = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+      double X[2] = {(en + pr) / (1 - v2old), pr}, F[2] = {0, 0};
+      Sist4 s4 = {ph, B2, SB2, SS2, UU, DD, 0.};
+      int nfev = 0;
+      (void)brentm(2, sist4_fn, &s4, X, F, 1.e-14, 1.e-14, 300, 3, &nfev);
+      *iters = nfev;
+      ys = X[0];
+      pr = X[1];
+      xs = s4.xinner;
+    } else {
+      double v2 = g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz);
+      double X[3] = {v2, (en + pr) / (1 - v2), pr}, F[3], J[3][3], L[3][3], DX[3], mF[3], Xt[3];
+      double Fnorm = 0, Fnl = 0;
+      int P[3], it = 0;
+      Sist3 s3 = {ph, B2, SB2, SS2, UU, DD};
+      getfun(&s3, X, F, J, &Fnorm, 1);
+      while (Fnorm >= 1.e-14) {
+        ludecompose(J, L, P, 4.e-16);
+        for (int i = 0; i < 3; i++) mF[i] = -F[i];
+        lusolve(L, J, P, DX, mF);
+        double lambda = 1.;
+        for (int i = 0; i < 3; i++) Xt[i] = X[i] + lambda * DX[i];
+        getfun(&s3, Xt, F, J, &Fnl, 1);
+        if ((Fnl > (1 - lambda / 2) * Fnorm) && (lambda > 1. / 64)) {
+          for (;;) {
+            lambda = lambda / 2.;
+            for (int i = 0; i < 3; i++) Xt[i] = X[i] + lambda * DX[i];
+            getfun(&s3, Xt, F, J, &Fnl, 0);
+            if (!((Fnl > (1 - lambda / 2) * Fnorm) && (lambda > 1. / 64))) {
+              for (int i = 0; i < 3; i++) X[i] = X[i] + lambda * DX[i];
+              Fnorm = Fnl;
+              break;
+            }
+          }
+        } else {
+          for (int i = 0; i < 3; i++) X[i] = X[i] + lambda * DX[i];
+          Fnorm = Fnl;
+        }
+        it = it + 1;
+        if (it > 300) {
+          *iters = it;
+          return 8;
+        }
+      }
+      *iters = it;
+      xs = X[0];
+      ys = X[1];
+      pr = X[2];
+    }
+    rh = DD * sqrt(1 - xs);
+    v[KRH] = rh;
+    v[KVX] = (sx + SB * bx / ys) / (ys + B2);
+    v[KVY] = (sy + SB * by / ys) / (ys + B2);
+    v[KVZ] = (sz / g3 + SB * bz / ys) / (ys + B2);
+    v[KPR] = pr;
+    if (p->divclean) v[ph->kglm] = u[ph->kglm];
+    return errcode;
+  }
+  if (algo == 4 || algo == 5) {
+    double S2 = sx * sx + sy * sy + sz * sz / g3;
+    double B2 = bx * bx + by * by + bz * bz * g3;
+    double SB = (sx * bx + sy * by + sz * bz);
+    double SB2 = SB * SB;
+    RtCtx c = {B2, SB2, S2, UU, DD, algo == 4 ? (4.0 / 3.0 - 1) / (4.0 / 3.0) : 0.25, 0., algo == 4 ? 7 : 8};
+    double v2_old = algo == 4 ? v[KVX] * v[KVX] + v[KVY] * v[KVY] + v[KVZ] * v[KVZ]
+                              : v[KVX] * v[KVX] + v[KVY] * v[KVY] + v[KVZ] * v[KVZ] * g3;
+    int ierr = 0;
+    double v2 = rtsafe(&c, v2_old, 0., 1. - 1.e-11, 1.e-12, &ierr);
+    if (algo == 4 && ierr > 0) return 0; /* system.f90:926: returns, v untouched */
+    if (algo == 5 && ((v2 >= 1) || (ierr > 0))) return 778;
+    for (int k = 0; k < nv; k++) v[k] = uin[k];
+    if (p->divclean) v[ph->kglm] = u[ph->kglm];
+    double w = c.w, rh = DD * sqrt(1. - v2);
+    v[KRH] = rh;
+    if (algo == 4) {
+      double pg = c.gam * (w * (1. - v2) - rh);
+      v[KPR] = fmax(pg, eps);
+    } else {
+      v[KPR] = 0.25 * (1 - v2) * w;
+    }
+    double vb = SB / w;
+    v[KVX] = (sx + vb * bx) / (w + B2);
+    v[KVY] = (sy + vb * by) / (w + B2);
+    v[KVZ] = (sz / g3 + vb * bz) / (w + B2);
+    return 0;
+  }
+  if (algo == 6) {
+    int exact9 = 1;
+    double v2_old = v[KVX] * v[KVX] + v[KVY] * v[KVY] + v[KVZ] * v[KVZ];
+    double oldsol9 = 4 * v[KPR] / (1 - v2_old);
+    double S2 = sx * sx + sy * sy + sz * sz;
+    double B2 = bx * bx + by * by + bz * bz;
+    double SB = (sx * bx + sy * by + sz * bz);
+    double SB2 = SB * SB;
+    double b9 = 8 * B2 - 4 * UU;
+    double c9 = 7 * (B2 * B2) - 8 * B2 * UU + S2;
+    double d9 = 2 * (B2 * B2 * B2) - 4 * (B2 * B2) * UU + 2 * B2 * S2;
+    double e9 = SB2 * B2;
+    double p9 = (24 * c9 - 3 * (b9 * b9)) / 72;
+    double q9 = ((b9 * b9 * b9) - 12 * b9 * c9 + 72 * d9) / 216;
+    double dnull9 = (c9 * c9) - 3 * b9 * d9 + 36 * e9;
+    double deinz9 = 2 * (c9 * c9 * c9) - 9 * b9 * c9 * d9 + 27 * (b9 * b9) * e9 + 81 * (d9 * d9) - 216 * c9 * e9;
+    double discr9 = (deinz9 * deinz9) - 4 * (dnull9 * dnull9 * dnull9);
+    double sbig9 = 0., sol9 = -1., v2 = 0.;
+    if (discr9 > 0) {
+      double droot9 = sqrt(discr9);
+      double qbig9 = pow(0.5 * (deinz9 + droot9), 1. / 3.);
+      double drad9 = -2 * p9 / 3 + (qbig9 + dnull9 / qbig9) / 9;
+      if (drad9 <= 0) return 12;
+      sbig9 = 0.5 * sqrt(drad9);
+    } else if (dnull9 > 0) {
+      double phi9 = acos(deinz9 / (2 * sqrt(dnull9 * dnull9 * dnull9)));
+      sbig9 = 0.5 * sqrt(-2. * p9 / 3 + 2. / 9. * sqrt(dnull9) * cos(phi9 / 3.));
+    } else {
+      if (solver10_approximate(b9, c9, d9, oldsol9, &sol9)) return 12;
+      exact9 = 0;
+      v2 = get_x9(sol9, S2, B2, SB2);
+      if ((v2 < 0) || (v2 > 1) || (sol9 < 0)) return 12;
+    }
+    if (exact9) {
+      /* sol1..sol4 start at -1 each call (the reference leaves the ones of
+         a negative radicand unset) */
+      double sol1 = -1., sol2 = -1., sol3 = -1., sol4 = -1.;
+      double rad129 = -4 * (sbig9 * sbig9) - 2 * p9 + q9 / sbig9;
+      double rad349 = -4 * (sbig9 * sbig9) - 2 * p9 - q9 / sbig9;
+      double rapp9 = -b9 / 12;
+      if (rad129 >= 0) {
+        double root129 = 0.5 * sqrt(rad129);
+        sol1 = rapp9 - sbig9 - root129;
+        sol2 = rapp9 - sbig9 + root129;
+      }
+      if (rad349 >= 0) {
+        double root349 = 0.5 * sqrt(rad349);
+        sol3 = rapp9 + sbig9 - root349;
+        sol4 = rapp9 + sbig9 + root349;
+      }
+      double dist9 = 1.e100, v9;
+      sol9 = -1.;
+      if (sol2 > 0) {
+        v9 = get_x9(sol2, S2, B2, SB2);
+        if ((v9 >= 0) && (v9 < 1)) {
+          sol9 = sol2;
+          v2 = v9;
+          dist9 = fabs(oldsol9 - sol9);
+          if (sol1 > 0) {
+            v9 = get_x9(sol1, S2, B2, SB2);
+            if ((v9 >= 0) && (v9 < 1)) {
+              double d19 = fabs(oldsol9 - sol1);
+              if (d19 <= dist9) {
+                sol9 = sol1;
+                dist9 = d19;
+                v2 = v9;
+              }
+            }
+          }
+        }
+      }
+      if (sol4 > 0) {
+        v9 = get_x9(sol4, S2, B2, SB2);
+        if ((v9 >= 0) && (v9 < 1)) {
+          double d49 = fabs(oldsol9 - sol4);
+          if (d49 <= dist9) {
+            sol9 = sol4;
+            dist9 = d49;
+            v2 = v9;
+          }
+        }
+        if (sol3 > 0) {
+          v9 = get_x9(sol3, S2, B2, SB2);
+          if ((v9 >= 0) && (v9 < 1)) {
+            double d39 = fabs(oldsol9 - sol3);
+            if (d39 <= dist9) {
+              sol9 = sol3;
+              dist9 = d39;
+              v2 = v9;
+            }
+          }
+        }
+      }
+      if (sol9 < 0) return 12;
+    }
+    for (int k = 0; k < nv; k++) v[k] = uin[k];
+    v[KRH] = DD * sqrt(1. - v2);
+    v[KPR] = sol9 / 4 * (1 - v2);
+    double vb = SB / sol9;
+    v[KVX] = (sx + vb * bx) / (sol9 + B2);
+    v[KVY] = (sy + vb * by) / (sol9 + B2);
+    v[KVZ] = (sz + vb * bz) / (sol9 + B2);
+    if (p->divclean) v[ph->kglm] = u[ph->kglm];
+    return 0;
+  }
+  return 11;
+}
+
 static int cons2prim(const Phys* ph, double* u, double* v, int* iters) {
   const EchoParams* p = ph->p;
   if (p->mhd == 2) return cons2prim_res(ph, u, v, iters);
+  if (p->mhd == 1 && !p->viscosity && p->algo_solver != ECHO_C2P_BRENT && p->algo_solver != ECHO_C2P_NEWTON &&
+      p->algo_solver != ECHO_C2P_MLP)
+    return cons2prim_mhd_algo(ph, u, v, iters); /* 2..6, else 11 */
   const double tol = 1.e-12, eps = 1.e-12;
   const int iter_max = 100, ivmax = 100, ipmax = 100;
   double g1 = ph->g1, g2 = ph->g2, g3 = ph->g3, gm = ph->gm;
