@@ -550,10 +550,9 @@ struct UpdateArgs {
   double* vsnap;
 };
 
-// Learned con2prim seed of the calling thread's cell from its conserved
-// variables uu (times sqrt(-g)).  Called by all 128 threads of the CTA
-// together (tensor-core inference per CTA); threads without a cell pass
-// active = false.
+// Learned con2prim seed of the calling lane's cell from its conserved
+// variables uu (times sqrt(-g)).  Called by all lanes of the warp together;
+// lanes without a cell pass active = false.
 template <int KIND>
 __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, bool active, const double* uu,
                                          float seed[2]) {
@@ -567,7 +566,7 @@ __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, boo
     double SS2 = sx * sx + sy * sy + sz * sz / g3;
     if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, f);
   }
-  mlp_cta(net, f, seed);
+  mlp_warp(net, f, seed);
 }
 
 // The update of cell c (flux divergence, sources, RK combination,

@@ -8,13 +8,12 @@
 // follows from the EoS (sist3's third equation).  The seed is finished by
 // the FP64 Newton solve on sist3; it is never used on its own.
 //
-// Inference runs per CTA of 128 threads, one cell per thread, on the
-// fifth-generation tensor cores: every layer is one M=128 tcgen05.mma chain
-// (BF16 operands from shared memory in the canonical no-swizzle K-major
-// layout, FP32 accumulators in tensor memory).  Thread t of the CTA owns row
-// t of the tile and of the accumulator (TMEM lane t), so bias, tanh and the
-// BF16 repacking of the next layer's input happen in the thread's registers
-// after one tcgen05.ld of its row.
+// Inference runs per warp (32 cells) on the tensor cores: BF16 operands,
+// FP32 accumulation, mma.sync.m16n8k16.  The accumulator fragment of an
+// m16n8 tile holds, per thread, rows (g, g+8) and columns (2t, 2t+1) -- the
+// same elements the A fragment of an m16n8k16 operand holds for the k-tile
+// that covers those columns -- so one layer's output becomes the next
+// layer's input in registers, with no shuffles or shared memory.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -25,20 +24,16 @@ namespace echo {
 
 enum { MLP_NIN = 5, MLP_H = 64, MLP_NOUT = 2, MLP_NHID = 4 };
 
-// Weights: one BF16 image per layer in the canonical K-major layout of a
-// tcgen05 B operand (core matrices of 8 rows x 16 bytes; rows n of W^T, K
-// contiguous): element (n, k) at byte (k/8)*LBO + (n/8)*128 + (n%8)*16 +
-// (k%8)*2 with LBO = (N/8)*128.  Layer 0 is K=16 (5 inputs, zero padded) x
-// N=64, layers 1..3 64 x 64, the output layer 64 x N=16 (2 outputs).  Offsets
-// and sizes in bytes; MLP_FRAG_N in u32.
+// Weight fragments (u32 = two bf16) in the order the mma B operand needs:
+// layer 0: [k-tile 0][n-tile 0..7][lane][2]; layers 1..3: [kt 0..3][nt 0..7]
+// [lane][2]; layer 4: [kt 0..3][nt 0][lane][2].
 enum {
-  MLP_IMG_L0 = 0,
-  MLP_IMG_L1 = MLP_IMG_L0 + 16 * 64 * 2,
-  MLP_IMG_L2 = MLP_IMG_L1 + 64 * 64 * 2,
-  MLP_IMG_L3 = MLP_IMG_L2 + 64 * 64 * 2,
-  MLP_IMG_L4 = MLP_IMG_L3 + 64 * 64 * 2,
-  MLP_IMG_BYTES = MLP_IMG_L4 + 64 * 16 * 2,
-  MLP_FRAG_N = MLP_IMG_BYTES / 4
+  MLP_FRAG_L0 = 0,
+  MLP_FRAG_L1 = MLP_FRAG_L0 + 1 * 8 * 64,
+  MLP_FRAG_L2 = MLP_FRAG_L1 + 4 * 8 * 64,
+  MLP_FRAG_L3 = MLP_FRAG_L2 + 4 * 8 * 64,
+  MLP_FRAG_L4 = MLP_FRAG_L3 + 4 * 8 * 64,
+  MLP_FRAG_N = MLP_FRAG_L4 + 4 * 1 * 64
 };
 // biases and normalisation, FP32: b0..b3 (64 each), b4 (8, two used),
 // feature mean/std (5+5), target mean/std (2+2)
@@ -72,6 +67,14 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
   return *reinterpret_cast<unsigned*>(&h);
 }
 
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
 // tanh of two FP32 accumulators, packed as the BF16 pair the next layer's A
 // fragment takes: one conversion and one packed tanh
 __device__ __forceinline__ unsigned tanh_pack_bf16(float lo, float hi) {
@@ -80,182 +83,97 @@ __device__ __forceinline__ unsigned tanh_pack_bf16(float lo, float hi) {
   return y;
 }
 
-// ---------------------------------------------------------------------------
-// tcgen05 plumbing (PTX ISA: tcgen05.alloc/mma/commit/ld, mbarrier)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// shared-memory matrix descriptor, no swizzle, K-major: start address,
-// leading byte offset (between the two 8-element K halves of a K=16 step)
-// and stride byte offset (between 8-row core-matrix groups), version 1
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
-}
-// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, M = 128, N
-__host__ __device__ constexpr uint32_t umma_idesc(int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-}
-__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// bounded wait for the phase of the given parity: false if it never came
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < (1 << 20); i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-// one thread: the bulk copy (TMA engine) of `bytes` from global memory into
-// shared memory, completing on mbarrier `bar` (which expects the bytes)
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-
-// the calling thread's TMEM lane, columns [col, col + 16)
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
-      "[%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+// Seed for the calling lane's cell.  Must be called by all 32 lanes of the
+// warp together (inactive lanes pass any finite features).  f: raw
+// invariants; out: (x, q) de-standardised.  The warp's 32 cells are two
+// m-tiles of 16 rows, run one after the other so that only one tile's
+// accumulators (32 registers) and A fragments (16) are live.
+__device__ __forceinline__ void mlp_warp(const MlpDev& M, const float f[5], float out[2]) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float fs[5];
 #pragma unroll
-  for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
-}
-
-// ---------------------------------------------------------------------------
-// Seed of the calling thread's cell.  Called by all 128 threads of the CTA
-// together (blockDim.x == 128; threads without a cell pass any finite
-// features).  f: raw invariants; out: (x, q) de-standardised.  A tensor-core
-// wait that never completes (bounded) leaves out = NaN, which the seeded
-// Newton treats as a failed seed (the plain Newton then runs).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void mlp_cta(const MlpDev& M, const float f[5], float out[2]) {
-  __shared__ __align__(1024) uint4 s_act[128 * 64 * 2 / 16];   // 16 KB: the 128 x K activation tile
-  __shared__ __align__(1024) uint4 s_w[2][64 * 64 * 2 / 16];   // 2 x 8 KB: weight images, double-buffered
-  __shared__ __align__(8) unsigned long long s_bar[3];         // [0]: MMA done, [1], [2]: weights landed
-  __shared__ uint32_t s_tmem;
-  __shared__ int s_fail;  // a weight copy that never landed
-  const int tid = threadIdx.x, warp = tid >> 5;
-  unsigned char* act = reinterpret_cast<unsigned char*>(s_act);
-  const unsigned char* img = reinterpret_cast<const unsigned char*>(M.frag);
-  const uint32_t bar = smem_addr(&s_bar[0]);
-  auto layer_img = [](int layer) {
-    return layer == 0 ? (int)MLP_IMG_L0 : layer == 4 ? (int)MLP_IMG_L4 : (int)MLP_IMG_L1 + (layer - 1) * (64 * 64 * 2);
-  };
-  auto layer_bytes = [](int layer) { return layer == 0 || layer == 4 ? 2048u : 8192u; };
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                 "r"(64u));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (tid == 0) {
-    s_fail = 0;
-    for (int i = 0; i < 3; i++) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&s_bar[i])), "r"(1u));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    // the first two layers' weights, while the features are computed
-    for (int l = 0; l < 2; l++)
-      bulk_load(smem_addr(&s_w[l][0]), img + layer_img(l), layer_bytes(l), smem_addr(&s_bar[1 + l]));
-  }
-  // layer-0 input: the standardised invariants in columns 0..4 of 16
-  {
-    float fs[8];
-#pragma unroll
-    for (int j = 0; j < 5; j++) fs[j] = (f[j] - __ldg(M.par + MLP_FMEAN + j)) / __ldg(M.par + MLP_FSTD + j);
-    fs[5] = fs[6] = fs[7] = 0.f;
-    uint4 lo = make_uint4(pack_bf16(fs[0], fs[1]), pack_bf16(fs[2], fs[3]), pack_bf16(fs[4], fs[5]),
-                          pack_bf16(fs[6], fs[7]));
-    const int row_off = (tid >> 3) * 128 + (tid & 7) * 16;
-    *reinterpret_cast<uint4*>(act + row_off) = lo;                                    // k 0..7
-    *reinterpret_cast<uint4*>(act + 2048 + row_off) = make_uint4(0u, 0u, 0u, 0u);     // k 8..15
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = s_tmem;
-  const uint32_t my_lane = tmem + ((uint32_t)(warp * 32) << 16);
-  bool ok = true;
+  for (int j = 0; j < 5; j++) fs[j] = (f[j] - __ldg(M.par + MLP_FMEAN + j)) / __ldg(M.par + MLP_FSTD + j);
+  // row r = mt*16 + h*8 + g' of the output sits in lane g'*4 (t = 0), element 2h / 2h+1
+  const int mt_me = lane >> 4, h_me = (lane >> 3) & 1, src = (lane & 7) * 4;
   float y0 = 0.f, y1 = 0.f;
 #pragma unroll 1
-  for (int layer = 0; layer < 5; layer++) {
-    const int K = layer == 0 ? 16 : 64, N = layer == 4 ? 16 : 64, buf = layer & 1;
-    // generic-proxy smem writes (this layer's input) -> visible to the
-    // tensor core; TMEM reads of the previous layer done before overwrite
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      bool w_ok = mbar_wait(smem_addr(&s_bar[1 + buf]), (uint32_t)((layer >> 1) & 1));
-      const uint32_t lbo_b = (uint32_t)(N / 8) * 128;
-      const uint32_t wbase = smem_addr(&s_w[buf][0]);
-      if (w_ok)
-        for (int j = 0; j < K / 16; j++)
-          umma_bf16(tmem, umma_desc(smem_addr(act + j * 2 * 2048), 2048, 128), umma_desc(wbase + j * 2 * lbo_b, lbo_b, 128),
-                    umma_idesc(N), j > 0 ? 1u : 0u);
-      umma_commit(bar);  // arrives when the MMAs above are done (at once if none was issued)
-      if (!w_ok) s_fail = 1;
-    }
-    ok = mbar_wait(bar, (uint32_t)(layer & 1)) && ok;
-    tc_fence_after();
-    // the weights of layer + 2 into the buffer this layer's MMAs have released
-    if (tid == 0 && layer + 2 < 5)
-      bulk_load(smem_addr(&s_w[buf][0]), img + layer_img(layer + 2), layer_bytes(layer + 2), smem_addr(&s_bar[1 + buf]));
-    if (layer < 4) {
-      const float* b = M.par + MLP_B0 + layer * 64;
-      const int row_off = (tid >> 3) * 128 + (tid & 7) * 16;
+  for (int mt = 0; mt < 2; mt++) {
+    // layer-0 A fragment (16 input columns, 5 used): rows g and g + 8 of this tile
+    unsigned A[4][4];  // [k-tile][reg]
+    {
+      float lo[5], hi[5];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {  // columns 16q .. 16q+15 -> K chunks 2q, 2q+1 of the next input
-        float v[16];
-        tmem_ld16(my_lane + 16 * q, v);
-        uint32_t p[8];
-#pragma unroll
-        for (int j = 0; j < 8; j++)
-          p[j] = tanh_pack_bf16(v[2 * j] + __ldg(b + 16 * q + 2 * j), v[2 * j + 1] + __ldg(b + 16 * q + 2 * j + 1));
-        *reinterpret_cast<uint4*>(act + (2 * q) * 2048 + row_off) = make_uint4(p[0], p[1], p[2], p[3]);
-        *reinterpret_cast<uint4*>(act + (2 * q + 1) * 2048 + row_off) = make_uint4(p[4], p[5], p[6], p[7]);
+      for (int j = 0; j < 5; j++) {
+        lo[j] = __shfl_sync(full, fs[j], mt * 16 + g);
+        hi[j] = __shfl_sync(full, fs[j], mt * 16 + g + 8);
       }
-    } else {
-      float v[16];
-      tmem_ld16(my_lane, v);
-      y0 = v[0] + __ldg(M.par + MLP_B4 + 0);
-      y1 = v[1] + __ldg(M.par + MLP_B4 + 1);
+      // columns 2t and 2t+1
+      float l0 = t == 0 ? lo[0] : t == 1 ? lo[2] : t == 2 ? lo[4] : 0.f;
+      float l1 = t == 0 ? lo[1] : t == 1 ? lo[3] : 0.f;
+      float h0 = t == 0 ? hi[0] : t == 1 ? hi[2] : t == 2 ? hi[4] : 0.f;
+      float h1 = t == 0 ? hi[1] : t == 1 ? hi[3] : 0.f;
+      A[0][0] = pack_bf16(l0, l1);
+      A[0][1] = pack_bf16(h0, h1);
+      A[0][2] = 0u;
+      A[0][3] = 0u;
+    }
+    // hidden layers 0..3
+#pragma unroll
+    for (int layer = 0; layer < 4; layer++) {
+      const int nk = layer == 0 ? 1 : 4;
+      const unsigned* W = M.frag + (layer == 0 ? MLP_FRAG_L0 : MLP_FRAG_L1 + (layer - 1) * (4 * 8 * 64));
+      const float* b = M.par + MLP_B0 + layer * 64;
+      float C[8][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        float b0 = __ldg(b + nt * 8 + 2 * t), b1 = __ldg(b + nt * 8 + 2 * t + 1);
+        C[nt][0] = b0;
+        C[nt][1] = b1;
+        C[nt][2] = b0;
+        C[nt][3] = b1;
+      }
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        if (kt >= nk) break;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+          const uint2 w = __ldg(reinterpret_cast<const uint2*>(W) + (kt * 8 + nt) * 32 + lane);
+          mma_bf16(C[nt], A[kt], w.x, w.y);
+        }
+      }
+      // tanh; the accumulators become the next layer's A fragments
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        A[kt][0] = tanh_pack_bf16(C[2 * kt][0], C[2 * kt][1]);
+        A[kt][1] = tanh_pack_bf16(C[2 * kt][2], C[2 * kt][3]);
+        A[kt][2] = tanh_pack_bf16(C[2 * kt + 1][0], C[2 * kt + 1][1]);
+        A[kt][3] = tanh_pack_bf16(C[2 * kt + 1][2], C[2 * kt + 1][3]);
+      }
+    }
+    // output layer: 64 -> 8 (two used), linear
+    float O[4];
+    {
+      float b0 = __ldg(M.par + MLP_B4 + 2 * t), b1 = __ldg(M.par + MLP_B4 + 2 * t + 1);
+      O[0] = b0;
+      O[1] = b1;
+      O[2] = b0;
+      O[3] = b1;
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        const uint2 w = __ldg(reinterpret_cast<const uint2*>(M.frag + MLP_FRAG_L4) + kt * 32 + lane);
+        mma_bf16(O, A[kt], w.x, w.y);
+      }
+    }
+    float a0 = __shfl_sync(full, O[0], src), a1 = __shfl_sync(full, O[1], src);
+    float a2 = __shfl_sync(full, O[2], src), a3 = __shfl_sync(full, O[3], src);
+    if (mt == mt_me) {
+      y0 = h_me ? a2 : a0;
+      y1 = h_me ? a3 : a1;
     }
   }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) {
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64u));
-  }
-  if (ok && !s_fail) {
-    out[0] = y0 * __ldg(M.par + MLP_TSTD + 0) + __ldg(M.par + MLP_TMEAN + 0);
-    out[1] = y1 * __ldg(M.par + MLP_TSTD + 1) + __ldg(M.par + MLP_TMEAN + 1);
-  } else {
-    out[0] = out[1] = __int_as_float(0x7fc00000);
-  }
+  out[0] = y0 * __ldg(M.par + MLP_TSTD + 0) + __ldg(M.par + MLP_TMEAN + 0);
+  out[1] = y1 * __ldg(M.par + MLP_TSTD + 1) + __ldg(M.par + MLP_TMEAN + 1);
 }
 
 }  // namespace echo

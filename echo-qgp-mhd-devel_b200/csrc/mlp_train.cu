@@ -43,29 +43,32 @@ unsigned short bf16_bits(float f) {
   return (unsigned short)(r >> 16);
 }
 
-// One layer's weight image (see mlp.cuh): W[k][n] (K x N, row-major) as
-// the BF16 K-major B operand of a tcgen05.mma, padded with zeros to
-// Kp x Np: element (n, k) at byte (k/8)*LBO + (n/8)*128 + (n%8)*16 + (k%8)*2,
-// LBO = (Np/8)*128.
-void pack_layer(const float* W, int K, int N, int Kp, int Np, unsigned char* out) {
-  const int lbo = (Np / 8) * 128;
-  for (int n = 0; n < Np; n++)
-    for (int k = 0; k < Kp; k++) {
-      float w = (k < K && n < N) ? W[k * N + n] : 0.f;
-      unsigned short b = bf16_bits(w);
-      memcpy(out + (k / 8) * lbo + (n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2, &b, 2);
-    }
+// B-operand fragments of mma.m16n8k16 (see mlp.cuh): for k-tile kt, n-tile
+// nt and lane (g = lane/4, t = lane%4): .x = (W[k0][n], W[k0+1][n]),
+// .y = (W[k0+8][n], W[k0+9][n]) with k0 = 16 kt + 2t, n = 8 nt + g; zero
+// outside the layer's K x N.
+void pack_layer(const float* W, int K, int N, int nkt, int nnt, unsigned* out) {
+  auto w = [&](int k, int n) -> float { return (k < K && n < N) ? W[k * N + n] : 0.f; };
+  for (int kt = 0; kt < nkt; kt++)
+    for (int nt = 0; nt < nnt; nt++)
+      for (int lane = 0; lane < 32; lane++) {
+        int g = lane / 4, t = lane % 4, n = nt * 8 + g, k0 = kt * 16 + 2 * t;
+        unsigned lo = bf16_bits(w(k0, n)) | ((unsigned)bf16_bits(w(k0 + 1, n)) << 16);
+        unsigned hi = bf16_bits(w(k0 + 8, n)) | ((unsigned)bf16_bits(w(k0 + 9, n)) << 16);
+        unsigned* o = out + ((size_t)(kt * nnt + nt) * 32 + lane) * 2;
+        o[0] = lo;
+        o[1] = hi;
+      }
 }
 
 void pack_network(const float* W, const float* norm, std::vector<unsigned>& frag, std::vector<float>& par) {
   frag.assign(echo::MLP_FRAG_N, 0u);
   par.assign(echo::MLP_PARAMS_N, 0.f);
-  unsigned char* img = reinterpret_cast<unsigned char*>(frag.data());
-  pack_layer(W + WOFF[0], 5, 64, 16, 64, img + echo::MLP_IMG_L0);
-  pack_layer(W + WOFF[1], 64, 64, 64, 64, img + echo::MLP_IMG_L1);
-  pack_layer(W + WOFF[2], 64, 64, 64, 64, img + echo::MLP_IMG_L2);
-  pack_layer(W + WOFF[3], 64, 64, 64, 64, img + echo::MLP_IMG_L3);
-  pack_layer(W + WOFF[4], 64, 2, 64, 16, img + echo::MLP_IMG_L4);
+  pack_layer(W + WOFF[0], 5, 64, 1, 8, frag.data() + echo::MLP_FRAG_L0);
+  pack_layer(W + WOFF[1], 64, 64, 4, 8, frag.data() + echo::MLP_FRAG_L1);
+  pack_layer(W + WOFF[2], 64, 64, 4, 8, frag.data() + echo::MLP_FRAG_L2);
+  pack_layer(W + WOFF[3], 64, 64, 4, 8, frag.data() + echo::MLP_FRAG_L3);
+  pack_layer(W + WOFF[4], 64, 2, 4, 1, frag.data() + echo::MLP_FRAG_L4);
   for (int l = 0; l < 4; l++)
     for (int n = 0; n < 64; n++) par[echo::MLP_B0 + l * 64 + n] = W[BOFF[l] + n];
   par[echo::MLP_B4 + 0] = W[BOFF[4] + 0];
@@ -234,8 +237,7 @@ bool echo_mlp_pack(const float* W, const float* norm, std::vector<unsigned>& fra
 }
 
 // ---------------------------------------------------------------------------
-// standalone tensor-core inference (the same mlp_cta the update kernel runs;
-// 128 threads per block)
+// standalone tensor-core inference (the same mlp_warp the update kernel runs)
 // ---------------------------------------------------------------------------
 static __global__ void k_infer(echo::MlpDev net, const float* X, int n, float* out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -243,7 +245,7 @@ static __global__ void k_infer(echo::MlpDev net, const float* X, int n, float* o
   if (i < n)
     for (int j = 0; j < 5; j++) f[j] = X[(size_t)i * 5 + j];
   float o[2];
-  echo::mlp_cta(net, f, o);
+  echo::mlp_warp(net, f, o);
   if (i < n) {
     out[(size_t)i * 2 + 0] = o[0];
     out[(size_t)i * 2 + 1] = o[1];

@@ -196,7 +196,7 @@ __global__ void c2p_seed_kernel(DevPhys P, Metric M, MlpDev net, int use_seed, d
       double SS2 = sx * sx + sy * sy + sz * sz / g3;
       if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, f);
     }
-    mlp_cta(net, f, seed);
+    mlp_warp(net, f, seed);
   }
   if (!active) return;
   int it = 0, sf = 0;
