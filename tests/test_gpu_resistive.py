@@ -74,3 +74,13 @@ def test_rejected_combinations():
     for cfg in (base.replace(nrk=P.RK3), base.replace(divclean=0), base.replace(algo_solver=P.C2P_MLP)):
         with pytest.raises(RuntimeError, match="status -3"):
             Evolve(cfg.to_c(przero=przero_of(cfg)), tab)
+
+
+@pytest.mark.parametrize("bc", [0, 1, 2, 3])
+def test_boundaries(bc):
+    """Every ghost fill (periodic, reflecting, outflow, extrapolation) in the
+    faces and in the charge density's neighbours."""
+    cfg = CASES["res3d"]().replace(sigma_el=500.0, boundary=bc)
+    _, tab, _ = setup(cfg)
+    ev, eu, _ = _pair(cfg, resistive_state(cfg, tab), 3, True, tab=tab)
+    assert ev <= 1e-13 and eu <= 1e-13, (bc, ev, eu)
