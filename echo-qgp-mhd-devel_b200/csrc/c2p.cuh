@@ -807,10 +807,15 @@ __device__ __forceinline__ void ohm_solve(const DevPhys& P, const Metric& M, con
 // inversion).  Fixed point on v: E(v) from ohm_solve; the fluid's share
 // S - E x B, U - (E^2 + B^2)/2; the ideal-HD Newton on p (system.f90:511-561)
 // for p and the new v; until max |dv| <= 1e-14 (one pass for h = 0), 779
-// after 200 passes.  v[KEX..KEZ] receives E and, when h > 0, u[KEX..KEZ]
+// after 200 passes.  It starts from the previous primitives in v (the
+// reference's warm start) or, given the learned seed (x = v^2, q = p/U of
+// the total energy U), from p = q U and v along the fluid momentum S - E x B
+// (E of u) with |v|^2 = x; the seeded first pass gets 3 Newton steps, and a
+// seed that fails them restarts the fixed point from the warm start
+// (*seed_failed = 1).  v[KEX..KEZ] receives E and, when h > 0, u[KEX..KEZ]
 // sqrt(-g) E: the implicit solve changes the conserved E.
 inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u, double* v, int* iters,
-                                    double h) {
+                                    double h, const float* seed = nullptr, int* seed_failed = nullptr) {
   const double ntol = 1.e-12, vtol = 1.e-14;
   double g1 = M.g1, g2 = M.g2, g3 = M.g3, gm = M.gm, gp = M.gp;
   double d = gm * u[KRH], U = gm * u[KPR];
@@ -820,6 +825,24 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
   double vel[3] = {v[KVX], v[KVY], v[KVZ]}, E[3];
   double pr = v[KPR], rh = v[KRH];
   double B2 = B[0] * B[0] + B[1] * B[1] + (B[2] * B[2]) * g3;
+  int cap = 1 << 30;  // Newton steps the current pass may take
+  if (seed) {
+    const double x = (double)seed[0], q = (double)seed[1];
+    if (x >= 0. && x < 1. && q > 0. && U > 0.) {
+      double Ec[3] = {Es[0], Es[1], Es[2] * g3}, EXB[3];
+      exb(M, Ec, B[0], B[1], B[2], EXB);
+      double sx = S[0] - EXB[0], sy = S[1] - EXB[1], sz = (S[2] - EXB[2]) / g3;
+      double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
+      double a = s2 > 0. ? sqrt(x / s2) : 0.;
+      vel[0] = a * sx;
+      vel[1] = a * sy;
+      vel[2] = a * sz;
+      pr = q * U;
+      cap = 3;
+    } else if (seed_failed) {
+      *seed_failed = 1;
+    }
+  }
   int errcode = 0, outer, total = 0;
   for (outer = 1; outer <= 200; outer++) {
     if (h > 0.) {
@@ -835,15 +858,13 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
     double sx = S[0] - EXB[0], sy = S[1] - EXB[1], sz = (S[2] - EXB[2]) / g3;
     double et = U - 0.5 * (E2 + B2);
     double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
-    double w = 0, v2, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    double w = 0, v2 = 0, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
+    bool conv = false;
     int iter;
     for (iter = 1; iter <= 100; iter++) {
       w = et + pr;
       v2 = s2 / (w * w);
-      if (v2 >= 1.) {
-        *iters = total + iter;
-        return 777;
-      }
+      if (v2 >= 1.) break;
       glf = 1. / sqrt(1. - v2);
       rh = d / glf;
       en = w * (1. - v2) - pr;
@@ -853,10 +874,30 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
       f = pr_eos - pr;
       df = dprdrh * drhdpr + dprden * dendpr - 1.;
       dpr = -f / df;
-      if (fabs(dpr) < ntol * pr) break;
+      if (fabs(dpr) < ntol * pr) {
+        conv = true;
+        break;
+      }
+      if (iter >= cap) break;
       pr = pr + dpr;
     }
     total += iter;
+    if (cap < 100 && (v2 >= 1. || !conv)) {
+      // the seed failed: the fixed point from the warm start
+      if (seed_failed) *seed_failed = 1;
+      vel[0] = v[KVX];
+      vel[1] = v[KVY];
+      vel[2] = v[KVZ];
+      pr = v[KPR];
+      cap = 1 << 30;
+      outer = 0;
+      continue;
+    }
+    if (v2 >= 1.) {
+      *iters = total;
+      return 777;
+    }
+    cap = 1 << 30;
     double vn0 = sx / w, vn1 = sy / w, vn2 = sz / w;
     double dv = fmax3(fabs(vn0 - vel[0]), fabs(vn1 - vel[1]), fabs(vn2 - vel[2]) * gp);
     vel[0] = vn0;
@@ -902,7 +943,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
   typedef Traits<KIND> T;
   // every resistive caller passes its own copy of u, which the implicit
   // solve updates (the reference's con2prim may modify u, evolve.f90:848)
-  if (T::RES) return cons2prim_res(P, M, const_cast<double*>(u), v, iters, h);
+  if (T::RES) return cons2prim_res(P, M, const_cast<double*>(u), v, iters, h, seed, seed_failed);
   const double eps = 1.e-12;
   const double ntol = 1.e-12;
   double g1 = M.g1, g2 = M.g2, g3 = M.g3, gm = M.gm;

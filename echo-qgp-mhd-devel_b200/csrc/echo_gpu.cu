@@ -291,9 +291,8 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   *out = nullptr;
   if (p->mhd > 2 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
   if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3 && p->nrk != ECHO_SSP) return ECHO_ERR_UNSUPPORTED;
-  // resistive runs: IMEX-SSP (common.f90:2114-2118), with GLM cleaning, the
-  // plain inversion (no learned seed for the resistive equations)
-  if (p->mhd == 2 && (p->nrk != ECHO_SSP || !p->divclean || p->algo_solver == ECHO_C2P_MLP))
+  // resistive runs: IMEX-SSP (common.f90:2114-2118), with GLM cleaning
+  if (p->mhd == 2 && (p->nrk != ECHO_SSP || !p->divclean))
     return ECHO_ERR_UNSUPPORTED;
   if (p->imex != 0 && p->imex != 1) return ECHO_ERR_ARG;
   if (p->imex && p->nrk == ECHO_SSP) return ECHO_ERR_UNSUPPORTED;  // IMEX RK2/RK3 only

@@ -556,7 +556,7 @@ struct UpdateArgs {
 template <int KIND>
 __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, bool active, const double* uu,
                                          float seed[2]) {
-  float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  float f[MLP_NIN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (active) {
     double gm = M.gm, g3 = M.g3;
     double D = gm * uu[KRH], sx = gm * uu[KVX], sy = gm * uu[KVY], sz = gm * uu[KVZ], U = gm * uu[KPR];
@@ -564,7 +564,13 @@ __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, boo
     double B2 = bx * bx + by * by + bz * bz * g3;
     double SB = sx * bx + sy * by + sz * bz;
     double SS2 = sx * sx + sy * sy + sz * sz / g3;
-    if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, f);
+    double E2 = 0.;
+    if (Traits<KIND>::RES) {
+      // E contravariant: E^2 = E1^2 + E2^2 + g3 E3^2
+      double ex = gm * uu[KEX], ey = gm * uu[KEY], ez = gm * uu[KEZ];
+      E2 = ex * ex + ey * ey + ez * ez * g3;
+    }
+    if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, E2, f);
   }
   mlp_warp(net, f, seed);
 }
@@ -846,12 +852,14 @@ __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_combine_kernel(SspArgs
     mlp_seed<KIND>(A.mlp, M, active, uu, seed);
     sp = seed;
   }
+  unsigned long long my_fallbacks = 0;
   if (active && !(T::MHD && !T::RES && c2p_alt_algo(A.algo))) {  // ALG_SOLV 2..6: c2p_alt_kernel
-    int it = 0;
+    int it = 0, sfail = 0;
     // the implicit stages of a resistive run solve Ohm's law in con2prim
     const double h = (T::RES && A.stage < 5) ? alpha_imex * dt : 0.;
-    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, nullptr, h);
+    int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail, h);
     my_iters = (unsigned long long)it;
+    my_fallbacks = (unsigned long long)sfail;
     if (err) {
       A.fail[c] = 1;
       atomicAdd(&A.sc->nfail, 1);
@@ -866,32 +874,47 @@ __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_combine_kernel(SspArgs
     }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+  for (int o = 16; o > 0; o >>= 1) {
+    my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
+    if (SEED) my_fallbacks += __shfl_xor_sync(0xffffffffu, my_fallbacks, o);
+  }
   if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
+  if (SEED && (threadIdx.x & 31) == 0 && my_fallbacks) atomicAdd(&A.sc->fallbacks, my_fallbacks);
 }
 
 // Resistive IMEX-SSP3(4,3,3), first stage: U1 = u^n + alpha dt S(U1), solved
 // from u0 = u^n cell by cell (the implicit stage the reference leaves to its
 // missing algo-7 con2prim); ds_out = -S(U1), the stiff E right-hand side the
 // later stages combine (only S(U1) enters them: F(U1) has weight 0).  v and
-// u stay at step n; a failed solve stops the run with its code.
-template <int KIND>
+// u stay at step n; a failed solve stops the run with its code.  SEED: the
+// solve starts from the learned seed (warp-collective inference, so every
+// lane reaches it).
+template <int KIND, bool SEED>
 __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_stage1_kernel(SspArgs A) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const double alpha_imex = 0.24169426078821;
   const Grid& g = A.g;
   size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (!T::RES || c >= g.ncell) return;
+  const bool active = c < g.ncell;
+  if (!T::RES || (!SEED && !active)) return;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
   double uu[NV], vv[NV], S[3];
 #pragma unroll
   for (int k = 0; k < NV; k++) {
-    uu[k] = A.u0[(size_t)k * g.ncell + c];
-    vv[k] = A.vin[(size_t)k * g.ncell + c];
+    uu[k] = active ? A.u0[(size_t)k * g.ncell + c] : 1.0;
+    vv[k] = active ? A.vin[(size_t)k * g.ncell + c] : 0.0;
   }
-  int it = 0;
-  int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, alpha_imex * A.sc->dt);
+  float seed[2] = {0.f, 0.f};
+  const float* sp = nullptr;
+  if (SEED) {
+    mlp_seed<KIND>(A.mlp, M, active, uu, seed);
+    sp = seed;
+  }
+  if (!active) return;
+  int it = 0, sfail = 0;
+  int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail, alpha_imex * A.sc->dt);
+  if (SEED && sfail) atomicAdd(&A.sc->fallbacks, 1ull);
   if (err) {
     atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
     return;

@@ -162,7 +162,7 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
   A.mlp.par = c->d_mlp_par;
   if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  if (Traits<KIND>::MHD && !Traits<KIND>::RES && A.algo == ECHO_C2P_MLP)
+  if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP)
     ssp_combine_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
   else
     ssp_combine_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
@@ -196,10 +196,13 @@ void launch_ssp_stage1(EchoCtx* c) {
   A.algo = c->p.algo_solver;
   A.divclean = c->p.divclean;
   A.tol = c->p.c2p_tol;
-  A.mlp.frag = nullptr;
-  A.mlp.par = nullptr;
+  A.mlp.frag = c->d_mlp_frag;
+  A.mlp.par = c->d_mlp_par;
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  ssp_stage1_kernel<KIND><<<blocks, 128, 0, c->stream>>>(A);
+  if (A.algo == ECHO_C2P_MLP && c->d_mlp_frag)
+    ssp_stage1_kernel<KIND, true><<<blocks, 128, 0, c->stream>>>(A);
+  else
+    ssp_stage1_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
   }
 }
 

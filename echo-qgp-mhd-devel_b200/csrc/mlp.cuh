@@ -1,12 +1,15 @@
-// mlp.cuh -- the learned con2prim seed for ideal RMHD.
+// mlp.cuh -- the learned con2prim seed for ideal and resistive RMHD.
 //
-// A 4x64 tanh MLP maps five normalised invariants of the conserved state
-//   f0 = log U, f1 = D/U, f2 = S^2/U^2, f3 = B^2/U, f4 = (S.B)^2/U^3
-// (U = energy, D = density, S = momentum, B = field, all already divided by
-// sqrt(-g); the same quantities BRENTM's system sist3 is written in) to the
-// two unknowns x = v^2 and q = p/U.  The third unknown y = (e+p)gamma^2
-// follows from the EoS (sist3's third equation).  The seed is finished by
-// the FP64 Newton solve on sist3; it is never used on its own.
+// A 4x64 tanh MLP maps six normalised invariants of the conserved state
+//   f0 = log U, f1 = D/U, f2 = S^2/U^2, f3 = B^2/U, f4 = (S.B)^2/U^3,
+//   f5 = E^2/U (zero for ideal RMHD, where E is not a conserved variable)
+// (U = energy, D = density, S = momentum, B = field, E = electric field,
+// all already divided by sqrt(-g); the quantities BRENTM's system sist3 is
+// written in) to the two unknowns x = v^2 and q = p/U.  For ideal RMHD the
+// third unknown y = (e+p)gamma^2 follows from the EoS (sist3's third
+// equation) and the seed is finished by the FP64 Newton solve on sist3; for
+// resistive RMHD p starts the fixed point's inner Newton (cons2prim_res).
+// The seed is never used on its own.
 //
 // Inference runs per warp (32 cells) on the tensor cores: BF16 operands,
 // FP32 accumulation, mma.sync.m16n8k16.  The accumulator fragment of an
@@ -22,7 +25,7 @@
 
 namespace echo {
 
-enum { MLP_NIN = 5, MLP_H = 64, MLP_NOUT = 2, MLP_NHID = 4 };
+enum { MLP_NIN = 6, MLP_H = 64, MLP_NOUT = 2, MLP_NHID = 4 };
 
 // Weight fragments (u32 = two bf16) in the order the mma B operand needs:
 // layer 0: [k-tile 0][n-tile 0..7][lane][2]; layers 1..3: [kt 0..3][nt 0..7]
@@ -36,13 +39,13 @@ enum {
   MLP_FRAG_N = MLP_FRAG_L4 + 4 * 1 * 64
 };
 // biases and normalisation, FP32: b0..b3 (64 each), b4 (8, two used),
-// feature mean/std (5+5), target mean/std (2+2)
+// feature mean/std (6+6), target mean/std (2+2)
 enum {
   MLP_B0 = 0,
   MLP_B4 = 4 * 64,
   MLP_FMEAN = MLP_B4 + 8,
-  MLP_FSTD = MLP_FMEAN + 5,
-  MLP_TMEAN = MLP_FSTD + 5,
+  MLP_FSTD = MLP_FMEAN + MLP_NIN,
+  MLP_TMEAN = MLP_FSTD + MLP_NIN,
   MLP_TSTD = MLP_TMEAN + 2,
   MLP_PARAMS_N = MLP_TSTD + 2
 };
@@ -53,13 +56,15 @@ struct MlpDev {
 };
 
 // raw invariants of the cell (before standardisation)
-__device__ __forceinline__ void mlp_invariants(double D, double SS2, double U, double B2, double SB2, float f[5]) {
+__device__ __forceinline__ void mlp_invariants(double D, double SS2, double U, double B2, double SB2, double E2,
+                                               float f[MLP_NIN]) {
   double iu = 1.0 / U;
   f[0] = (float)log(U);
   f[1] = (float)(D * iu);
   f[2] = (float)(SS2 * iu * iu);
   f[3] = (float)(B2 * iu);
   f[4] = (float)(SB2 * iu * iu * iu);
+  f[5] = (float)(E2 * iu);
 }
 
 __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
@@ -88,31 +93,31 @@ __device__ __forceinline__ unsigned tanh_pack_bf16(float lo, float hi) {
 // invariants; out: (x, q) de-standardised.  The warp's 32 cells are two
 // m-tiles of 16 rows, run one after the other so that only one tile's
 // accumulators (32 registers) and A fragments (16) are live.
-__device__ __forceinline__ void mlp_warp(const MlpDev& M, const float f[5], float out[2]) {
+__device__ __forceinline__ void mlp_warp(const MlpDev& M, const float f[MLP_NIN], float out[2]) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  float fs[5];
+  float fs[MLP_NIN];
 #pragma unroll
-  for (int j = 0; j < 5; j++) fs[j] = (f[j] - __ldg(M.par + MLP_FMEAN + j)) / __ldg(M.par + MLP_FSTD + j);
+  for (int j = 0; j < MLP_NIN; j++) fs[j] = (f[j] - __ldg(M.par + MLP_FMEAN + j)) / __ldg(M.par + MLP_FSTD + j);
   // row r = mt*16 + h*8 + g' of the output sits in lane g'*4 (t = 0), element 2h / 2h+1
   const int mt_me = lane >> 4, h_me = (lane >> 3) & 1, src = (lane & 7) * 4;
   float y0 = 0.f, y1 = 0.f;
 #pragma unroll 1
   for (int mt = 0; mt < 2; mt++) {
-    // layer-0 A fragment (16 input columns, 5 used): rows g and g + 8 of this tile
+    // layer-0 A fragment (16 input columns, 6 used): rows g and g + 8 of this tile
     unsigned A[4][4];  // [k-tile][reg]
     {
-      float lo[5], hi[5];
+      float lo[MLP_NIN], hi[MLP_NIN];
 #pragma unroll
-      for (int j = 0; j < 5; j++) {
+      for (int j = 0; j < MLP_NIN; j++) {
         lo[j] = __shfl_sync(full, fs[j], mt * 16 + g);
         hi[j] = __shfl_sync(full, fs[j], mt * 16 + g + 8);
       }
       // columns 2t and 2t+1
       float l0 = t == 0 ? lo[0] : t == 1 ? lo[2] : t == 2 ? lo[4] : 0.f;
-      float l1 = t == 0 ? lo[1] : t == 1 ? lo[3] : 0.f;
+      float l1 = t == 0 ? lo[1] : t == 1 ? lo[3] : t == 2 ? lo[5] : 0.f;
       float h0 = t == 0 ? hi[0] : t == 1 ? hi[2] : t == 2 ? hi[4] : 0.f;
-      float h1 = t == 0 ? hi[1] : t == 1 ? hi[3] : 0.f;
+      float h1 = t == 0 ? hi[1] : t == 1 ? hi[3] : t == 2 ? hi[5] : 0.f;
       A[0][0] = pack_bf16(l0, l1);
       A[0][1] = pack_bf16(h0, h1);
       A[0][2] = 0u;

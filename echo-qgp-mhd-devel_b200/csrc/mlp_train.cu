@@ -4,7 +4,7 @@
 // FP32 forward pass, backward pass (weight and bias gradients, tanh
 // derivative), mean-squared loss on standardised targets and Adam.  The
 // weight vector layout (ECHO_MLP_NWEIGHTS floats) is, layer by layer,
-// W_l[K_l][N_l] row-major followed by b_l[N_l], with (K, N) = (5, 64),
+// W_l[K_l][N_l] row-major followed by b_l[N_l], with (K, N) = (6, 64),
 // (64, 64) x3, (64, 2).
 #include <cuda_runtime.h>
 
@@ -28,11 +28,13 @@
 
 namespace {
 
-const int NL = 5;
-const int LK[NL] = {5, 64, 64, 64, 64};
-const int LN[NL] = {64, 64, 64, 64, 2};
-const int WOFF[NL] = {0, 384, 4544, 8704, 12864};
-const int BOFF[NL] = {320, 4480, 8640, 12800, 12992};
+constexpr int NL = 5, NIN = echo::MLP_NIN;
+constexpr int LK[NL] = {NIN, 64, 64, 64, 64};
+constexpr int LN[NL] = {64, 64, 64, 64, 2};
+constexpr int WOFF[NL] = {0, 448, 4608, 8768, 12928};
+constexpr int BOFF[NL] = {384, 4544, 8704, 12864, 13056};
+static_assert(BOFF[NL - 1] + 2 == ECHO_MLP_NWEIGHTS, "weight vector layout");
+static_assert(echo::MLP_PARAMS_N - echo::MLP_FMEAN == ECHO_MLP_NNORM, "norm layout");
 
 // round-to-nearest-even float -> bf16 bits
 unsigned short bf16_bits(float f) {
@@ -64,7 +66,7 @@ void pack_layer(const float* W, int K, int N, int nkt, int nnt, unsigned* out) {
 void pack_network(const float* W, const float* norm, std::vector<unsigned>& frag, std::vector<float>& par) {
   frag.assign(echo::MLP_FRAG_N, 0u);
   par.assign(echo::MLP_PARAMS_N, 0.f);
-  pack_layer(W + WOFF[0], 5, 64, 1, 8, frag.data() + echo::MLP_FRAG_L0);
+  pack_layer(W + WOFF[0], NIN, 64, 1, 8, frag.data() + echo::MLP_FRAG_L0);
   pack_layer(W + WOFF[1], 64, 64, 4, 8, frag.data() + echo::MLP_FRAG_L1);
   pack_layer(W + WOFF[2], 64, 64, 4, 8, frag.data() + echo::MLP_FRAG_L2);
   pack_layer(W + WOFF[3], 64, 64, 4, 8, frag.data() + echo::MLP_FRAG_L3);
@@ -73,7 +75,7 @@ void pack_network(const float* W, const float* norm, std::vector<unsigned>& frag
     for (int n = 0; n < 64; n++) par[echo::MLP_B0 + l * 64 + n] = W[BOFF[l] + n];
   par[echo::MLP_B4 + 0] = W[BOFF[4] + 0];
   par[echo::MLP_B4 + 1] = W[BOFF[4] + 1];
-  for (int j = 0; j < 14; j++) par[echo::MLP_FMEAN + j] = norm[j];
+  for (int j = 0; j < ECHO_MLP_NNORM; j++) par[echo::MLP_FMEAN + j] = norm[j];
 }
 
 // ---------------------------------------------------------------------------
@@ -93,7 +95,7 @@ __global__ void k_gather(const float* Xs, const float* Ts, int n, int B, unsigne
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   unsigned i = hash32(seed * 0x9e3779b9u ^ hash32(step * 1000003u + (unsigned)b)) % (unsigned)n;
-  for (int j = 0; j < 5; j++) A0[b * 5 + j] = Xs[(size_t)i * 5 + j];
+  for (int j = 0; j < NIN; j++) A0[b * NIN + j] = Xs[(size_t)i * NIN + j];
   Y[b * 2 + 0] = Ts[(size_t)i * 2 + 0];
   Y[b * 2 + 1] = Ts[(size_t)i * 2 + 1];
 }
@@ -180,7 +182,7 @@ __global__ void k_adam(float* W, const float* G, float* m, float* v, int n, floa
 struct Trainer {
   int B = 0;
   float *W = nullptr, *G = nullptr, *m = nullptr, *v = nullptr;
-  float* act[NL + 1] = {nullptr};  // act[0] = input (B x 5), act[l+1] = layer l output
+  float* act[NL + 1] = {nullptr};  // act[0] = input (B x NIN), act[l+1] = layer l output
   float *dZ[NL] = {nullptr}, *Y = nullptr, *loss = nullptr;
   ~Trainer() {
     cudaFree(W);
@@ -200,7 +202,7 @@ struct Trainer {
     CK(cudaMalloc(&v, sizeof(float) * ECHO_MLP_NWEIGHTS));
     CK(cudaMemset(m, 0, sizeof(float) * ECHO_MLP_NWEIGHTS));
     CK(cudaMemset(v, 0, sizeof(float) * ECHO_MLP_NWEIGHTS));
-    CK(cudaMalloc(&act[0], sizeof(float) * B * 5));
+    CK(cudaMalloc(&act[0], sizeof(float) * B * NIN));
     for (int l = 0; l < NL; l++) {
       CK(cudaMalloc(&act[l + 1], sizeof(float) * B * LN[l]));
       CK(cudaMalloc(&dZ[l], sizeof(float) * B * LN[l]));
@@ -241,9 +243,9 @@ bool echo_mlp_pack(const float* W, const float* norm, std::vector<unsigned>& fra
 // ---------------------------------------------------------------------------
 static __global__ void k_infer(echo::MlpDev net, const float* X, int n, float* out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  float f[NIN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (i < n)
-    for (int j = 0; j < 5; j++) f[j] = X[(size_t)i * 5 + j];
+    for (int j = 0; j < NIN; j++) f[j] = X[(size_t)i * NIN + j];
   float o[2];
   echo::mlp_warp(net, f, o);
   if (i < n) {
@@ -279,11 +281,11 @@ int echo_gpu_mlp_infer(const float* weights, const float* norm, const float* X, 
   float *dpar, *dX, *dout;
   CK(cudaMalloc(&dfrag, sizeof(unsigned) * frag.size()));
   CK(cudaMalloc(&dpar, sizeof(float) * par.size()));
-  CK(cudaMalloc(&dX, sizeof(float) * 5 * (size_t)n));
+  CK(cudaMalloc(&dX, sizeof(float) * NIN * (size_t)n));
   CK(cudaMalloc(&dout, sizeof(float) * 2 * (size_t)n));
   CK(cudaMemcpy(dfrag, frag.data(), sizeof(unsigned) * frag.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dpar, par.data(), sizeof(float) * par.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dX, X, sizeof(float) * 5 * (size_t)n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dX, X, sizeof(float) * NIN * (size_t)n, cudaMemcpyHostToDevice));
   echo::MlpDev net{dfrag, dpar};
   k_infer<<<(n + 127) / 128, 128>>>(net, dX, n, dout);
   CK(cudaGetLastError());
@@ -302,7 +304,7 @@ int echo_gpu_mlp_grad(const float* weights, const float* Xs, const float* Ts, in
   int r = tr.alloc(n);
   if (r) return r;
   CK(cudaMemcpy(tr.W, weights, sizeof(float) * ECHO_MLP_NWEIGHTS, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(tr.act[0], Xs, sizeof(float) * 5 * (size_t)n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(tr.act[0], Xs, sizeof(float) * NIN * (size_t)n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(tr.Y, Ts, sizeof(float) * 2 * (size_t)n, cudaMemcpyHostToDevice));
   tr.fwd_bwd();
   CK(cudaGetLastError());
@@ -316,29 +318,32 @@ int echo_gpu_mlp_train(const float* X, const float* T, int n, int steps, int bat
   if (!X || !T || n < 2 || steps <= 0 || batch <= 0 || !weights_out || !norm_out) return ECHO_ERR_ARG;
   (void)cudaGetLastError();
   // standardisation of the raw invariants and targets
-  double mu[7] = {0}, sd[7] = {0};
+  // (a feature without spread -- E^2/U of ideal-RMHD pairs -- keeps std 1)
+  double mu[NIN + 2] = {0}, sd[NIN + 2] = {0};
   for (int i = 0; i < n; i++) {
-    for (int j = 0; j < 5; j++) mu[j] += X[(size_t)i * 5 + j];
-    for (int j = 0; j < 2; j++) mu[5 + j] += T[(size_t)i * 2 + j];
+    for (int j = 0; j < NIN; j++) mu[j] += X[(size_t)i * NIN + j];
+    for (int j = 0; j < 2; j++) mu[NIN + j] += T[(size_t)i * 2 + j];
   }
-  for (int j = 0; j < 7; j++) mu[j] /= n;
+  for (int j = 0; j < NIN + 2; j++) mu[j] /= n;
   for (int i = 0; i < n; i++) {
-    for (int j = 0; j < 5; j++) sd[j] += (X[(size_t)i * 5 + j] - mu[j]) * (X[(size_t)i * 5 + j] - mu[j]);
-    for (int j = 0; j < 2; j++) sd[5 + j] += (T[(size_t)i * 2 + j] - mu[5 + j]) * (T[(size_t)i * 2 + j] - mu[5 + j]);
+    for (int j = 0; j < NIN; j++) sd[j] += (X[(size_t)i * NIN + j] - mu[j]) * (X[(size_t)i * NIN + j] - mu[j]);
+    for (int j = 0; j < 2; j++)
+      sd[NIN + j] += (T[(size_t)i * 2 + j] - mu[NIN + j]) * (T[(size_t)i * 2 + j] - mu[NIN + j]);
   }
-  for (int j = 0; j < 7; j++) sd[j] = sqrt(sd[j] / n) > 1e-12 ? sqrt(sd[j] / n) : 1.0;
-  for (int j = 0; j < 5; j++) {
+  for (int j = 0; j < NIN + 2; j++) sd[j] = sqrt(sd[j] / n) > 1e-12 ? sqrt(sd[j] / n) : 1.0;
+  for (int j = 0; j < NIN; j++) {
     norm_out[j] = (float)mu[j];
-    norm_out[5 + j] = (float)sd[j];
+    norm_out[NIN + j] = (float)sd[j];
   }
   for (int j = 0; j < 2; j++) {
-    norm_out[10 + j] = (float)mu[5 + j];
-    norm_out[12 + j] = (float)sd[5 + j];
+    norm_out[2 * NIN + j] = (float)mu[NIN + j];
+    norm_out[2 * NIN + 2 + j] = (float)sd[NIN + j];
   }
-  std::vector<float> xs((size_t)n * 5), ts((size_t)n * 2);
+  std::vector<float> xs((size_t)n * NIN), ts((size_t)n * 2);
   for (int i = 0; i < n; i++) {
-    for (int j = 0; j < 5; j++) xs[(size_t)i * 5 + j] = (float)((X[(size_t)i * 5 + j] - mu[j]) / sd[j]);
-    for (int j = 0; j < 2; j++) ts[(size_t)i * 2 + j] = (float)((T[(size_t)i * 2 + j] - mu[5 + j]) / sd[5 + j]);
+    for (int j = 0; j < NIN; j++) xs[(size_t)i * NIN + j] = (float)((X[(size_t)i * NIN + j] - mu[j]) / sd[j]);
+    for (int j = 0; j < 2; j++)
+      ts[(size_t)i * 2 + j] = (float)((T[(size_t)i * 2 + j] - mu[NIN + j]) / sd[NIN + j]);
   }
   // Glorot-uniform initial weights from a fixed-seed generator
   std::vector<float> w0(ECHO_MLP_NWEIGHTS, 0.f);

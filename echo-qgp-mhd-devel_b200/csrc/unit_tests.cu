@@ -186,17 +186,7 @@ __global__ void c2p_seed_kernel(DevPhys P, Metric M, MlpDev net, int use_seed, d
   }
   float seed[2] = {0.f, 0.f};
   if (use_seed) {
-    float f[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-    if (active) {
-      double gm = M.gm, g3 = M.g3;
-      double D = gm * uu[KRH], sx = gm * uu[KVX], sy = gm * uu[KVY], sz = gm * uu[KVZ], U = gm * uu[KPR];
-      double bx = gm * uu[KBX], by = gm * uu[KBY], bz = gm * uu[KBZ];
-      double B2 = bx * bx + by * by + bz * bz * g3;
-      double SB = sx * bx + sy * by + sz * bz;
-      double SS2 = sx * sx + sy * sy + sz * sz / g3;
-      if (U > 0.) mlp_invariants(D, SS2, U, B2, SB * SB, f);
-    }
-    mlp_warp(net, f, seed);
+    mlp_seed<KIND>(net, M, active, uu, seed);
   }
   if (!active) return;
   int it = 0, sf = 0;

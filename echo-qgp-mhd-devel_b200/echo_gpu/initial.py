@@ -16,6 +16,8 @@ import math
 
 import numpy as np
 
+from . import params as P
+
 HC3 = 0.00768351  # (hbar c)^3 as written in eos.f90:275
 
 NUCLEI = {  # nuclear_data.dat: A, R (fm), a (fm), rho0 (fm^-3)
@@ -268,6 +270,36 @@ def primitives(cfg, tab: np.ndarray | None = None, seed: int = 7,
         if cfg.divclean:
             fields += [zero]
     return _pack(fields)
+
+
+def with_ideal_e(cfg, v: np.ndarray, ideal: float) -> np.ndarray:
+    """A resistive state (nv = 12) with its electric field set to `ideal`
+    times the ideal-MHD field E = -v x B: covariant E_i = -sqrt(-g) [ijk]
+    v^j B^k, raised with g_33 = tau^2 (tau = 1 in Minkowski coordinates)."""
+    v = np.array(v, dtype=np.float64).reshape(cfg.nv, -1)
+    tau = cfg.tstart if cfg.coordinates == P.BJORKEN else 1.0
+    vx, vy, vz, bx, by, bz = v[1], v[2], v[3], v[5], v[6], v[7]
+    e_cov = [-tau * (vy * bz - vz * by), -tau * (vz * bx - vx * bz), -tau * (vx * by - vy * bx)]
+    v[8], v[9], v[10] = ideal * e_cov[0], ideal * e_cov[1], ideal * e_cov[2] / tau**2
+    return v.reshape(-1)
+
+
+def resistive_flow(cfg, tab, amp: float = 0.2, ideal: float = 0.7) -> np.ndarray:
+    """The resistive workload's initial state (at rest, E = 0) given a
+    smooth flow along x, y and eta of amplitude `amp` and an electric field
+    that is `ideal` times the ideal -v x B: a state with Ohm currents and
+    charges from the first step."""
+    v = primitives(cfg, tab).reshape(cfg.nv, cfg.nz, cfg.ny, cfg.nx)
+    x = cell_centres(cfg.nx, cfg.x1, cfg.x2)
+    y = cell_centres(cfg.ny, cfg.y1, cfg.y2)
+    z = cell_centres(cfg.nz, cfg.z1, cfg.z2)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    Lx, Lz = cfg.x2 - cfg.x1, max(cfg.z2 - cfg.z1, 1e-300)
+    tau = cfg.tstart if cfg.coordinates == P.BJORKEN else 1.0
+    v[1] = amp * np.sin(np.pi * Y / Lx) * np.cos(np.pi * Z / Lz)
+    v[2] = amp * np.sin(np.pi * X / Lx)
+    v[3] = 0.5 * amp / tau * np.sin(np.pi * (X + Y) / Lx)
+    return with_ideal_e(cfg, v.reshape(-1), ideal)
 
 
 def bjorken_uniform(cfg, e0: float = 10.0) -> np.ndarray:

@@ -2,12 +2,15 @@
 loading into a run.
 
 Pairs are (conserved, primitive) states the GPU solver itself produces:
-ideal-RMHD runs of the 3+1D Milne workload at several energy scales and
-magnetisations, sampled every few steps.  The invariants and targets are
-computed here from u and v exactly as the device computes the invariants
-(csrc/kernels.cuh mlp_seed, csrc/mlp.cuh mlp_invariants):
-  U = u_E/tau, D = u_rho/tau, S_i = u_i/tau, B^i = u_B/tau (1/sqrt(-g) = 1/tau)
-  f = (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3), target = (v^2, p/U).
+ideal-RMHD runs of the 3+1D Milne workload (or resistive runs of the
+resistive workload) at several energy scales and magnetisations, sampled
+every few steps.  The invariants and targets are computed here from u and v
+exactly as the device computes the invariants (csrc/kernels.cuh mlp_seed,
+csrc/mlp.cuh mlp_invariants):
+  U = u_E/tau, D = u_rho/tau, S_i = u_i/tau, B^i = u_B/tau, E^i = u_E^i/tau
+  (1/sqrt(-g) = 1/tau)
+  f = (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3, E^2/U), target = (v^2, p/U),
+with E = 0 for ideal RMHD.
 """
 from __future__ import annotations
 
@@ -20,11 +23,14 @@ from . import initial as I
 from . import params as P
 from .lib import F, Evolve, load
 
-NW = 12994
+NW = 13058  # ECHO_MLP_NWEIGHTS
+NNORM = 16  # ECHO_MLP_NNORM
+NIN = 6  # ECHO_MLP_NIN
 
 
 def invariants_targets(u: np.ndarray, v: np.ndarray, t: float, nv: int):
-    """Invariants X (n x 5) and targets T (n x 2) of every cell of a state."""
+    """Invariants X (n x 6) and targets T (n x 2) of every cell of a state
+    (ideal RMHD: nv = 9, E^2/U = 0; resistive: nv = 12, E in u[8:11])."""
     uu = u.reshape(nv, -1) / t
     vv = v.reshape(nv, -1)
     g3 = t * t
@@ -33,44 +39,66 @@ def invariants_targets(u: np.ndarray, v: np.ndarray, t: float, nv: int):
     B2 = bx * bx + by * by + bz * bz * g3
     SB = sx * bx + sy * by + sz * bz
     SS2 = sx * sx + sy * sy + sz * sz / g3
-    X = np.stack([np.log(E), D / E, SS2 / E**2, B2 / E, SB * SB / E**3], 1)
+    if nv == 12:
+        E2 = uu[8] ** 2 + uu[9] ** 2 + g3 * uu[10] ** 2
+    else:
+        E2 = np.zeros_like(E)
+    X = np.stack([np.log(E), D / E, SS2 / E**2, B2 / E, SB * SB / E**3, E2 / E], 1)
     x2 = vv[1] ** 2 + vv[2] ** 2 + g3 * vv[3] ** 2
     T = np.stack([x2, vv[4] / E], 1)
     return X.astype(np.float32), T.astype(np.float32)
 
 
-def _magnetised(cfg, tab, peak_scale: float, mag: float, seed: int):
+def _magnetised(cfg, tab, peak_scale: float, mag: float, seed: int, flow: float = 0.0):
     """Primitives of the workload with the energy density scaled and the
-    field set to magnetisation B^2/(2e) = mag at the centre."""
-    v = I.primitives(cfg, tab, seed=seed).reshape(cfg.nv, -1).copy()
+    field set to magnetisation B^2/(2e) = mag at the centre (the workload's
+    own: 0.1 ideal, 0.3 resistive); resistive runs also get a smooth flow
+    of amplitude `flow` and 0.7 times the ideal E = -v x B."""
+    if cfg.mhd == 2:
+        v = I.resistive_flow(cfg, tab, amp=flow, ideal=0.0).reshape(cfg.nv, -1).copy()
+    else:
+        v = I.primitives(cfg, tab, seed=seed).reshape(cfg.nv, -1).copy()
     e_floor = cfg.enezero
     p = v[4]
     # rescale pressure through e: e -> e_floor + s (e - e_floor)
     e = np.interp(p, tab[:, 2], tab[:, 1])
     e2 = e_floor + peak_scale * (e - e_floor)
     v[4] = I.table_pressure(tab, e2)
-    v[5:8] *= math.sqrt(mag / 0.1 * peak_scale)
+    v[5:8] *= math.sqrt(mag / (0.3 if cfg.mhd == 2 else 0.1) * peak_scale)
+    if cfg.mhd == 2:
+        v = I.with_ideal_e(cfg, v.reshape(-1), 0.7).reshape(cfg.nv, -1)
     return v.reshape(-1)
 
 
 def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: int = 12, every: int = 3,
-                   rng_seed: int = 5, exact: bool = False):
+                   rng_seed: int = 5, exact: bool = False, resistive: bool = False):
     """Run the GPU solver on the RMHD workload (the full 97x97x81 grid, or a
     grid^3-sized version with the same spacing, EoS and scheme) at several
     energy scales and magnetisations and collect (invariants, targets)
     pairs.  The full grid covers the outer, dilute and strongly magnetised
-    region a central sub-grid never reaches."""
+    region a central sub-grid never reaches.  resistive: the resistive
+    workload instead (193x193x129 over the same extent at half the
+    resolution, or grid^3 at full resolution), at rest and with smooth flows
+    of amplitude 0.1 and 0.3 carrying 0.7 of the ideal E."""
     rng = np.random.default_rng(rng_seed)
     tab = I.eos_table_loaded()
-    base = P.config1() if grid is None else P.small(P.config1(), grid, nz=max(8, int(grid * 0.84)))
-    base = base.replace(algo_solver=P.C2P_NEWTON)
+    if resistive:
+        c4 = P.config4()
+        if grid is None:
+            base = c4.replace(nx=97, ny=97, nz=65, name=c4.name + "-half")
+        else:
+            base = P.small(c4, grid, nz=max(8, int(grid * 0.67)))
+        variants = [(s, m, f) for s in (0.3, 1.0, 3.0) for m in (0.1, 0.3) for f in (0.0, 0.1, 0.3)]
+    else:
+        base = P.config1() if grid is None else P.small(P.config1(), grid, nz=max(8, int(grid * 0.84)))
+        base = base.replace(algo_solver=P.C2P_NEWTON)
+        variants = [(s, m, 0.0) for s in (0.3, 1.0, 3.0) for m in (0.03, 0.1, 0.3)]
     przero = float(I.table_pressure(tab, np.array([base.enezero]))[0])
     Xs, Ts = [], []
-    variants = [(s, m) for s in (0.3, 1.0, 3.0) for m in (0.03, 0.1, 0.3)]
     per = max(1, n_target // (len(variants) * (steps // every)))
-    for k, (scale, mag) in enumerate(variants):
+    for k, (scale, mag, flow) in enumerate(variants):
         ev = Evolve(base.to_c(przero=przero), tab, exact=exact)
-        ev.upload(_magnetised(base, tab, scale, mag, seed=k), None, base.tstart)
+        ev.upload(_magnetised(base, tab, scale, mag, seed=k, flow=flow), None, base.tstart)
         for s in range(1, steps + 1):
             ev.run(1)
             if s % every == 0:
@@ -99,7 +127,7 @@ def train(X: np.ndarray, T: np.ndarray, steps: int = 3000, batch: int = 4096, lr
     X = np.ascontiguousarray(X, dtype=np.float32)
     T = np.ascontiguousarray(T, dtype=np.float32)
     w = np.zeros(NW, dtype=np.float32)
-    norm = np.zeros(14, dtype=np.float32)
+    norm = np.zeros(NNORM, dtype=np.float32)
     losses = np.zeros(max(1, steps // report_every), dtype=np.float32)
     rc = L.echo_gpu_mlp_train(X.ctypes.data_as(F), T.ctypes.data_as(F), len(X), steps, batch, lr, seed,
                               w.ctypes.data_as(F), norm.ctypes.data_as(F), losses.ctypes.data_as(F),

@@ -301,14 +301,17 @@ int echo_gpu_test_c2p_seeded(const EchoParams* p, const double* eos_table,
 
 /* ---- learned con2prim seed (ECHO_C2P_MLP) -------------------------------- */
 
-/* The seed network is a 4x64 tanh MLP from five invariants of the conserved
- * state (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3) to (v^2, p/U).  Weight
- * vector: per layer W[K][N] row-major then b[N], (K,N) = (5,64), (64,64) x3,
- * (64,2).  norm: feature mean[5], std[5], target mean[2], std[2]. */
-#define ECHO_MLP_NWEIGHTS 12994
+/* The seed network is a 4x64 tanh MLP from six invariants of the conserved
+ * state (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3, E^2/U; E = 0 for ideal
+ * RMHD) to (v^2, p/U).  Weight vector: per layer W[K][N] row-major then b[N],
+ * (K,N) = (6,64), (64,64) x3, (64,2).  norm: feature mean[6], std[6], target
+ * mean[2], std[2]. */
+#define ECHO_MLP_NIN 6
+#define ECHO_MLP_NWEIGHTS 13058
+#define ECHO_MLP_NNORM 16
 
 /* Trains the network with this library's own FP32 forward/backward kernels
- * and Adam on n raw (invariants X[n][5], targets T[n][2]) pairs.  A set-up
+ * and Adam on n raw (invariants X[n][6], targets T[n][2]) pairs.  A set-up
  * call: allocates device memory for the data and the optimiser.  loss_out
  * receives one value every report_every steps (may be NULL). */
 int echo_gpu_mlp_train(const float* X, const float* T, int n, int steps,

@@ -3267,15 +3267,15 @@ int orc_flux(const EchoParams* p, const double* tab, int n_eos, double g3,
 /* gradient w.r.t. the weight vector (layout of ECHO_MLP_NWEIGHTS).         */
 /* ------------------------------------------------------------------------ */
 void orc_mlp_grad(const float* W, const float* Xs, const float* Ts, int n, double* loss, double* grad) {
-  static const int LK[5] = {5, 64, 64, 64, 64}, LN[5] = {64, 64, 64, 64, 2};
-  static const int WO[5] = {0, 384, 4544, 8704, 12864}, BO[5] = {320, 4480, 8640, 12800, 12992};
-  const int NW = 12994;
+  static const int LK[5] = {6, 64, 64, 64, 64}, LN[5] = {64, 64, 64, 64, 2};
+  static const int WO[5] = {0, 448, 4608, 8768, 12928}, BO[5] = {384, 4544, 8704, 12864, 13056};
+  const int NW = 13058;
   double* g = grad;
   for (int i = 0; i < NW; i++) g[i] = 0.;
   double L = 0.;
   double act[6][64], dz[5][64];
   for (int r = 0; r < n; r++) {
-    for (int j = 0; j < 5; j++) act[0][j] = Xs[r * 5 + j];
+    for (int j = 0; j < 6; j++) act[0][j] = Xs[r * 6 + j];
     for (int l = 0; l < 5; l++)
       for (int o = 0; o < LN[l]; o++) {
         double z = W[BO[l] + o];
@@ -3304,17 +3304,17 @@ void orc_mlp_grad(const float* W, const float* Xs, const float* Ts, int n, doubl
 
 /* FP64 forward pass on raw invariants with normalisation (seed accuracy) */
 void orc_mlp_forward(const float* W, const float* norm, const float* X, int n, double* out) {
-  static const int LK[5] = {5, 64, 64, 64, 64}, LN[5] = {64, 64, 64, 64, 2};
-  static const int WO[5] = {0, 384, 4544, 8704, 12864}, BO[5] = {320, 4480, 8640, 12800, 12992};
+  static const int LK[5] = {6, 64, 64, 64, 64}, LN[5] = {64, 64, 64, 64, 2};
+  static const int WO[5] = {0, 448, 4608, 8768, 12928}, BO[5] = {384, 4544, 8704, 12864, 13056};
   double act[6][64];
   for (int r = 0; r < n; r++) {
-    for (int j = 0; j < 5; j++) act[0][j] = ((double)X[r * 5 + j] - norm[j]) / norm[5 + j];
+    for (int j = 0; j < 6; j++) act[0][j] = ((double)X[r * 6 + j] - norm[j]) / norm[6 + j];
     for (int l = 0; l < 5; l++)
       for (int o = 0; o < LN[l]; o++) {
         double z = W[BO[l] + o];
         for (int k = 0; k < LK[l]; k++) z += act[l][k] * (double)W[WO[l] + k * LN[l] + o];
         act[l + 1][o] = l < 4 ? tanh(z) : z;
       }
-    for (int o = 0; o < 2; o++) out[r * 2 + o] = act[5][o] * norm[12 + o] + norm[10 + o];
+    for (int o = 0; o < 2; o++) out[r * 2 + o] = act[5][o] * norm[14 + o] + norm[12 + o];
   }
 }

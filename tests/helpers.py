@@ -76,25 +76,9 @@ CASES = {
 
 
 def resistive_state(cfg, tab, amp: float = 0.2, ideal: float = 0.7) -> np.ndarray:
-    """The resistive workload's initial state (at rest, E = 0) given a
-    smooth flow along x, y and eta and an electric field that is `ideal`
-    times the ideal -v x B: a state with Ohm currents and charges from the
-    first step."""
-    v = I.primitives(cfg, tab).reshape(cfg.nv, cfg.nz, cfg.ny, cfg.nx)
-    x = I.cell_centres(cfg.nx, cfg.x1, cfg.x2)
-    y = I.cell_centres(cfg.ny, cfg.y1, cfg.y2)
-    z = I.cell_centres(cfg.nz, cfg.z1, cfg.z2)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    Lx, Lz = cfg.x2 - cfg.x1, max(cfg.z2 - cfg.z1, 1e-300)
-    tau = cfg.tstart if cfg.coordinates == P.BJORKEN else 1.0
-    v[1] = amp * np.sin(np.pi * Y / Lx) * np.cos(np.pi * Z / Lz)
-    v[2] = amp * np.sin(np.pi * X / Lx)
-    v[3] = 0.5 * amp / tau * np.sin(np.pi * (X + Y) / Lx)
-    vx, vy, vz, bx, by, bz = v[1], v[2], v[3], v[5], v[6], v[7]
-    # ideal covariant E_i = -sqrt(-g) [ijk] v^j B^k, raised with g_33 = tau^2
-    e_cov = [-tau * (vy * bz - vz * by), -tau * (vz * bx - vx * bz), -tau * (vx * by - vy * bx)]
-    v[8], v[9], v[10] = ideal * e_cov[0], ideal * e_cov[1], ideal * e_cov[2] / tau**2
-    return v.reshape(-1)
+    """The resistive workload's state with a smooth flow and 0.7 of the
+    ideal E (echo_gpu.initial.resistive_flow)."""
+    return I.resistive_flow(cfg, tab, amp, ideal)
 
 
 def gubser(tau, X, Y, q=1.0, T0=0.4):

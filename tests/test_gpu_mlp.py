@@ -23,8 +23,8 @@ pytestmark = pytest.mark.gpu
 
 def _random_weights(rng):
     w = np.zeros(S.NW, dtype=np.float32)
-    LK, LN = (5, 64, 64, 64, 64), (64, 64, 64, 64, 2)
-    WO, BO = (0, 384, 4544, 8704, 12864), (320, 4480, 8640, 12800, 12992)
+    LK, LN = (6, 64, 64, 64, 64), (64, 64, 64, 64, 2)
+    WO, BO = (0, 448, 4608, 8768, 12928), (384, 4544, 8704, 12864, 13056)
     for l in range(5):
         a = np.sqrt(6.0 / (LK[l] + LN[l]))
         w[WO[l]:WO[l] + LK[l] * LN[l]] = rng.uniform(-a, a, LK[l] * LN[l])
@@ -35,7 +35,7 @@ def _random_weights(rng):
 def test_training_gradient_matches_oracle():
     rng = np.random.default_rng(11)
     w = _random_weights(rng)
-    Xs = rng.standard_normal((256, 5)).astype(np.float32)
+    Xs = rng.standard_normal((256, 6)).astype(np.float32)
     Ts = rng.standard_normal((256, 2)).astype(np.float32)
     lg, gg = S.gradient(w, Xs, Ts)
     lo, go = O.mlp_grad(w, Xs, Ts)
@@ -46,8 +46,9 @@ def test_training_gradient_matches_oracle():
 def test_tensor_core_inference_matches_fp64():
     rng = np.random.default_rng(12)
     w = _random_weights(rng)
-    norm = np.array([0.5, 0.2, 0.1, 0.3, 0.05, 1.0, 0.3, 0.2, 0.4, 0.1, 0.2, 0.1, 0.3, 0.05], dtype=np.float32)
-    X = (rng.standard_normal((1000, 5)) * norm[5:10] + norm[:5]).astype(np.float32)
+    norm = np.array([0.5, 0.2, 0.1, 0.3, 0.05, 0.02, 1.0, 0.3, 0.2, 0.4, 0.1, 0.03, 0.2, 0.1, 0.3, 0.05],
+                    dtype=np.float32)
+    X = (rng.standard_normal((1000, 6)) * norm[6:12] + norm[:6]).astype(np.float32)
     out = S.infer(w, norm, X)
     ref = O.mlp_forward(w, norm, X)
     spread = ref.std(0)

@@ -71,7 +71,7 @@ def test_stiff_decay_parity(exact, tol):
 def test_rejected_combinations():
     base = CASES["res3d"]()
     _, tab, _ = setup(base)
-    for cfg in (base.replace(nrk=P.RK3), base.replace(divclean=0), base.replace(algo_solver=P.C2P_MLP)):
+    for cfg in (base.replace(nrk=P.RK3), base.replace(divclean=0)):
         with pytest.raises(RuntimeError, match="status -3"):
             Evolve(cfg.to_c(przero=przero_of(cfg)), tab)
 

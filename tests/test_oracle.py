@@ -97,11 +97,11 @@ def test_golden_vectors(name):
 def test_mlp_oracle_gradient_by_finite_differences():
     # pins the FP64 network gradient the GPU training kernels are checked against
     rng = np.random.default_rng(2)
-    w = (rng.standard_normal(12994) * 0.2).astype(np.float32)
-    X = rng.standard_normal((16, 5)).astype(np.float32)
+    w = (rng.standard_normal(13058) * 0.2).astype(np.float32)
+    X = rng.standard_normal((16, 6)).astype(np.float32)
     T = rng.standard_normal((16, 2)).astype(np.float32)
     _, g = O.mlp_grad(w, X, T)
-    for i in [0, 100, 330, 400, 5000, 9000, 12865, 12993]:
+    for i in [0, 100, 330, 383, 400, 5000, 9000, 12929, 13057]:
         h = 2e-3 * max(1.0, abs(float(w[i])))
         wp = w.astype(np.float64).copy()
         wm = w.astype(np.float64).copy()
