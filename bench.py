@@ -275,7 +275,8 @@ def run_resistive(args, torch, barrier, world, rank):
         "value": variants["mlp_seeded"]["value"], "unit": UNIT, "steps": steps,
         "ms_per_step": variants["mlp_seeded"]["ms_per_step"],
         "variants": variants, "seed_training": training,
-        "c2p_iters": "Newton steps per cell summed over the fixed point's passes, final combination only",
+        "c2p_iters": "Newton steps per cell summed over the fixed point's passes: the stage-4 solve and the "
+                     "final combination",
         "parity": "unpinned against the reference (no runnable resistive path); device = oracle at 1e-12",
     }
     if world == 1 and rank == 0:
