@@ -285,15 +285,94 @@ def run_resistive(args, torch, barrier, world, rank):
     return out
 
 
-def run_batched(args, torch, barrier, world, rank):
+def run_viscous(args, torch, barrier, world, rank, X1, T1):
+    """The 2+1D viscous workload: Israel-Stewart shear hydro on 201x201
+    (dx = 0.1 fm), eta/s = 0.12, tau_pi = 5 eta/(e+p), IMEX RK2, tabulated
+    EoS, MC-Glauber Pb+Pb at b = 8 fm; the plain (warm-started) nested
+    inversion and the MLP-seeded one, the network trained on pairs of the
+    ideal-RMHD workload (X1, T1) and of viscous runs of this one.  40 k
+    cells: the step is latency-bound, so it runs as captured step graphs."""
+    from echo_gpu import initial as I
+    from echo_gpu import params as P
+    from echo_gpu import seed as S
+    from echo_gpu.lib import Evolve
+
+    cfg = P.config2().replace(imex=1)
+    tab = I.eos_table_loaded()
+    przero = float(I.table_pressure(tab, np.array([cfg.enezero]))[0])
+    pcut = I.table_temperature_to_pressure(tab, cfg.smooth_temp)
+    v0 = I.primitives(cfg, tab)
+    t0 = time.perf_counter()
+    Xv, Tv = S.generate_pairs(n_target=args.pairs // 2, viscous=True)
+    X = np.concatenate([X1, Xv])
+    T = np.concatenate([T1, Tv])
+    t1 = time.perf_counter()
+    w, norm, losses = S.train(X, T, steps=args.train_steps)
+    t2 = time.perf_counter()
+    training = {"pairs": int(len(X)), "viscous_pairs": int(len(Xv)), "pair_generation_s": t1 - t0,
+                "train_steps": args.train_steps, "train_s": t2 - t1,
+                "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                "source": "the ideal-RMHD workload's pairs plus viscous runs of this workload "
+                          "(3 energy scales x b = 0, 5, 10 fm)"}
+    steps = max(20, min(args.steps * 4, 200))
+
+    def timed(algo):
+        c = cfg.replace(algo_solver=algo)
+        ev = Evolve(c.to_c(przero=przero, smooth_pressure=pcut), tab, exact=False)
+        if algo == P.C2P_MLP:
+            ev.set_seed_network(w, norm)
+        ev.upload(v0, None, cfg.tstart)
+        stream = torch.cuda.ExternalStream(ev.stream_handle())
+        ev.run(max(args.warmup, 3))
+        ev.sync()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ev.run(steps)
+        e1.record(stream)
+        ev.sync()
+        torch.cuda.synchronize()
+        barrier()
+        ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        st = ev.stats()
+        prof = ev.profile_step()
+        ev.sync()
+        ev.close()
+        return float(ms.item()), st, prof
+
+    variants = {}
+    for algo, name in ((P.C2P_NEWTON, "plain"), (P.C2P_MLP, "mlp_seeded")):
+        ms, st, prof = timed(algo)
+        variants[name] = {
+            "value": cfg.ncell * steps * world / (ms / 1e3), "ms_per_step": ms / steps,
+            "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()},
+            "c2p_iters_per_cell_last_stage": st.c2p_iters / max(cfg.ncell, 1),
+            "seed_fallbacks_total": int(st.seed_fallbacks), "errcode": int(st.errcode)}
+    return {
+        "workload": cfg.name, "grid": [cfg.nx, cfg.ny], "nv": cfg.nv, "scheme": "WENO5+HLL, IMEX RK2",
+        "value": variants["mlp_seeded"]["value"], "unit": UNIT, "steps": steps,
+        "ms_per_step": variants["mlp_seeded"]["ms_per_step"], "variants": variants, "seed_training": training,
+        "c2p_iters": "Newton steps per cell summed over the nested iteration's passes, last stage",
+    }, (w, norm)
+
+
+def run_batched(args, torch, barrier, world, rank, net=None):
     """The batched event-by-event workload: 512 Monte Carlo Glauber Pb+Pb
     events (viscous 2+1D, grids 61^2..161^2) from tau = 0.4 to 10 fm/c in
     one batch, beside the same events run one after another through the
-    single-grid path.  With N ranks the events are split across the GPUs by
-    cell count (no collective on the data path): the whole job's
+    single-grid path, and again with the MLP-seeded inversion (net: the
+    viscous seed network).  With N ranks the events are split across the
+    GPUs by cell count (no collective on the data path): the whole job's
     cell-updates over the slowest rank's time."""
     from echo_gpu import events as EV
     from echo_gpu import initial as I
+    from echo_gpu import params as P
     from echo_gpu import shard as SH
     from echo_gpu.batch import Batch, event_grid
     from echo_gpu.lib import Evolve
@@ -330,6 +409,33 @@ def run_batched(args, torch, barrier, world, rank):
     st_local = b.status()
     cu = SH.reduce_sum(b.cell_updates(), device="cuda")
     st = SH.gather_status(mine, st_local, full.nev)
+    seeded = None
+    if net is not None:
+        pcm = es.cfg.replace(algo_solver=P.C2P_MLP).to_c(przero=przero, smooth_pressure=pcut)
+        bm = Batch(pcm, tab, [event_grid(*es.grid(e)) for e in range(es.nev)])
+        bm.set_seed_network(*net)
+        bm.glauber(srcs, es.cfg.tstart, es.tmax)
+        bm.autotune(3)
+        bm.run(max(args.warmup, 3))
+        bm.glauber(srcs, es.cfg.tstart, es.tmax)
+        sm = torch.cuda.ExternalStream(bm.stream_handle())
+        barrier()
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(sm)
+        bm.run_to_end(chunk=16)
+        m1.record(sm)
+        bm.sync()
+        barrier()
+        ms_m = SH.reduce_max(m0.elapsed_time(m1), device="cuda")
+        cu_m = SH.reduce_sum(bm.cell_updates(), device="cuda")
+        stm = bm.status()
+        fb = SH.reduce_sum(sum(s["seed_fallbacks"] for s in stm), device="cuda")
+        crashed = SH.reduce_sum(sum(1 for s in stm if s["state"] == 2), device="cuda")
+        bm.close()
+        seeded = {"value": cu_m / (ms_m / 1e3), "ms": ms_m, "cell_updates": int(cu_m),
+                  "seed_fallbacks_total": int(fb), "events_crashed": int(crashed)}
     # the same events one at a time through the single-grid path (a sample)
     b.glauber(srcs, es.cfg.tstart, es.tmax)
     v0 = b.split(b.download()[0])
@@ -356,7 +462,8 @@ def run_batched(args, torch, barrier, world, rank):
     seq = seq_cu / (seq_ms / 1e3)
     if rank != 0:
         return None
-    value = cu / (ms / 1e3)
+    plain = cu / (ms / 1e3)
+    value = seeded["value"] if seeded else plain
     states = np.bincount([s["state"] for s in st], minlength=4)
     return {
         "workload": f"{full.nev} MC-Glauber Pb+Pb events (b in [0,12] fm), viscous 2+1D IS, grids "
@@ -365,17 +472,20 @@ def run_batched(args, torch, barrier, world, rank):
                     f"ENEZERO {full.cfg.enezero}",
         "cells": int(full.cells.sum()),
         "value": value, "unit": UNIT, "ms": ms, "batched_steps": nsteps,
+        "variants": {"plain": {"value": plain, "ms": ms}, "mlp_seeded": seeded},
         "scaling": "strong" if world > 1 else None,
         "sharding": f"events split over {world} GPU(s) by cell count, no data-path collective",
         "cell_updates": int(cu), "events_done": int(states[1]), "events_crashed": int(states[2]),
         "event_steps_min_max": [int(min(s["steps"] for s in st)), int(max(s["steps"] for s in st))],
         "sequential_single_grid": {"value": seq, "unit": UNIT,
                                    "sample": "every 16th event of rank 0's share, 20 steps each, one GPU"},
-        "speedup_vs_sequential": value / world / seq,
+        "speedup_vs_sequential": plain / world / seq,
+        "speedup_vs_sequential_note": "plain batched over plain single-grid, both on one GPU",
         "kernels_ms_per_step_at_start": {k: round(x, 4) for k, x in prof.items()},
         "autotuned_ms_per_launch": {k: round(x, 4) for k, x in tune_ms.items()},
         "ic": {"nucleon_sampling_s_host": sampling_s, "smearing_and_eos_s_device": ic_s},
-        "con2prim": "viscous nested Newton (system.f90:564-666); the learned seed covers ideal and resistive RMHD",
+        "con2prim": "viscous nested Newton (system.f90:564-666), plain and from the learned seed "
+                    "(the 2+1D viscous workload's network)",
     }
 
 
@@ -491,7 +601,8 @@ def run_b200(args):
         dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
     e2e_value = cfg0.ncell * e2e_steps * world / (float(e2e_ms.item()) / 1e3)
     st2 = ev.stats()
-    batched = run_batched(args, torch, barrier, world, rank) if args.batched else None
+    viscous, vnet = run_viscous(args, torch, barrier, world, rank, Xp, Tp) if args.viscous else (None, None)
+    batched = run_batched(args, torch, barrier, world, rank, vnet) if args.batched else None
     resistive = run_resistive(args, torch, barrier, world, rank) if args.resistive else None
 
     if world > 1:
@@ -552,6 +663,7 @@ def run_b200(args):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * nbytes, "d2h_bytes_per_step": 2 * nbytes,
                 "steps": e2e_steps},
+        "viscous": viscous,
         "batched": batched,
         "resistive": resistive,
         "gpu_launches": launches_per_step * args.steps,
@@ -574,6 +686,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--batched", type=int, default=1, help="also run the batched event-by-event workload")
     ap.add_argument("--resistive", type=int, default=1, help="also run the resistive RMHD workload")
+    ap.add_argument("--viscous", type=int, default=1, help="also run the 2+1D viscous workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -16,6 +16,9 @@
 
 using namespace echo;
 
+// the network's BF16 fragments and FP32 parameters (mlp_train.cu)
+bool echo_mlp_pack(const float* W, const float* norm, std::vector<unsigned>& frag, std::vector<float>& par);
+
 #define CK(x)                                                                                     \
   do {                                                                                            \
     cudaError_t e_ = (x);                                                                         \
@@ -124,7 +127,6 @@ int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos, int
   if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3) return ECHO_ERR_UNSUPPORTED;
   if (p->imex != 0 && p->imex != 1) return ECHO_ERR_ARG;
   if (p->mhd && c2p_alt_algo(p->algo_solver)) return ECHO_ERR_UNSUPPORTED;  // ALG_SOLV 2..6: single grid
-  if (p->algo_solver == ECHO_C2P_MLP) return ECHO_ERR_UNSUPPORTED;
   if (p->eqstate == ECHO_EOS_TABLE && (!eos_table || n_eos < 2)) return ECHO_ERR_ARG;
   for (int e = 0; e < nev; e++) {
     const EchoEventGrid& q = grids[e];
@@ -252,6 +254,8 @@ int echo_batch_free(EchoBatch* b) {
     cudaFree(b->d_WD[k]);
   }
   cudaFree(b->d_fail);
+  cudaFree(b->d_mlp_frag);
+  cudaFree(b->d_mlp_par);
   cudaFree(b->d_ev);
   cudaFree(b->d_sc);
   cudaFree(b->d_state);
@@ -387,9 +391,26 @@ int echo_batch_download(EchoBatch* b, double* v, double* u) {
   return ECHO_OK;
 }
 
+int echo_batch_mlp_set(EchoBatch* b, const float* weights, const float* norm) {
+  if (!b || !weights || !norm) return ECHO_ERR_ARG;
+  std::vector<unsigned> frag;
+  std::vector<float> par;
+  echo_mlp_pack(weights, norm, frag, par);
+  if (!b->d_mlp_frag) {
+    CK(cudaMalloc(&b->d_mlp_frag, sizeof(unsigned) * frag.size()));
+    CK(cudaMalloc(&b->d_mlp_par, sizeof(float) * par.size()));
+  }
+  CK(cudaMemcpyAsync(b->d_mlp_frag, frag.data(), sizeof(unsigned) * frag.size(), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->d_mlp_par, par.data(), sizeof(float) * par.size(), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  drop_graphs(b);  // step graphs captured before hold the unseeded update
+  return ECHO_OK;
+}
+
 int echo_batch_run(EchoBatch* b, int nsteps) {
   (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
   if (!b || nsteps < 0) return ECHO_ERR_ARG;
+  if (b->p.algo_solver == ECHO_C2P_MLP && !b->d_mlp_frag) return ECHO_ERR_ARG;  // no network loaded
   for (int s = 0; s < nsteps; s++) {
     int key = b->ucur | (b->vcur << 1) | (b->vn << 2);
     if (!b->graph_ok[key]) {
@@ -451,6 +472,7 @@ int echo_batch_status(EchoBatch* b, EchoEventStatus* st) {
     }
     o.c2p_iters = (long long)s.c2p_iters;
     o.repairs = (long long)s.repairs;
+    o.seed_fallbacks = (long long)s.fallbacks;
   }
   return ECHO_OK;
 }

@@ -461,6 +461,8 @@ struct EchoBatch {
   int nsm;
   int max_tiles[echo::PH_N];  // tiles with every event live
   int sched[echo::SL_N];      // CTAs per launch of each slot; 0 = one per tile
+  unsigned* d_mlp_frag;  // learned con2prim seed: BF16 weight fragments
+  float* d_mlp_par;      //   biases and normalisation
   cudaGraphExec_t graph[8];
   bool graph_ok[8];
   std::vector<std::pair<int, cudaEvent_t>>* marks;

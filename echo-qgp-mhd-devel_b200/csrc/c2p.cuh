@@ -988,7 +988,17 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     if (pr <= 0) errcode = 777;
     return errcode;
   } else if (T::VISC) {
-    // nested iteration (system.f90:564-666)
+    // nested iteration (system.f90:564-666).  The reference's outer loop
+    // ends after one pass: its test compares v^2 of the new velocities with
+    // the Newton's own v^2, the same number, so pi^{t mu} keep the guess's
+    // velocities (a relative residual ~1e-4 in S on the workload).
+    // ECHO_C2P_NEWTON and ECHO_C2P_MLP iterate the passes to the fixed
+    // point instead (max |dv| <= 1e-14, each pass's Newton from the last
+    // pass's p): the inversion's own root, at equal residual whatever the
+    // start.  With the learned seed (x = v^2, q = p/U) the first pass starts
+    // from v along S with |v|^2 = x and p = q U and its Newton gets 3
+    // steps; a seed that fails restarts from the warm start
+    // (*seed_failed = 1).
     double uin[T::NV], vprim[T::NV];
 #pragma unroll
     for (int k = 0; k < T::NV; k++) uin[k] = gm * u[k];
@@ -1001,6 +1011,24 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     for (int k = 0; k < T::NV; k++) vprim[k] = v[k];
     double rh = 0, pr = 0, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
     double et = gm * u[KPR];
+    const bool conv = algo == ECHO_C2P_NEWTON || algo == ECHO_C2P_MLP;
+    double p0 = v[KPR];  // where each pass's Newton starts
+    int cap = 1 << 30;   // Newton steps the current pass may take
+    if (seed) {
+      const double x = (double)seed[0], q = (double)seed[1];
+      if (x >= 0. && x < 1. && q > 0. && et > 0.) {
+        double sx = uin[KVX], sy = uin[KVY], sz = uin[KVZ] / g3;
+        double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
+        double a = s2 > 0. ? sqrt(x / s2) : 0.;
+        vx = a * sx;
+        vy = a * sy;
+        vz = a * sz;
+        p0 = q * et;
+        cap = 3;
+      } else if (seed_failed) {
+        *seed_failed = 1;
+      }
+    }
     int tot = 0;
     for (int iv = 1; iv <= 100; iv++) {
       vprim[KVX] = vx;
@@ -1014,14 +1042,12 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
       double sz_cov = uin[KVZ] - pi.tz * g3;
       double sx = sx_cov, sy = sy_cov, sz = sz_cov / g3;
       double s2 = sx * sx_cov + sy * sy_cov + sz * sz_cov;
-      pr = v[KPR];
+      pr = p0;
+      bool conv = false;
       for (int ip = 1; ip <= 100; ip++) {
         tot++;
         v2 = s2 / ((en1 + pr) * (en1 + pr));
-        if (v2 >= 1.) {
-          *iters = tot;
-          return 107;
-        }
+        if (v2 >= 1.) break;
         glf = 1. / sqrt(1. - v2);
         rh = d / glf;
         en = (en1 + pr) * (1. - v2) - pr - vprim[KPIBU];
@@ -1031,19 +1057,48 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
         f = pr_eos - pr;
         df = dprdrh * drhdpr + dprden * dendpr - 1.;
         dpr = -f / df;
-        if (fabs(dpr) < ntol * pr) break;
+        if (fabs(dpr) < ntol * pr) {
+          conv = true;
+          break;
+        }
+        if (ip >= cap) break;
         pr = pr + dpr;
       }
-      vx = sx / (en1 + pr);
-      if (fabs(vx) < eps) vx = 0.;
-      vy = sy / (en1 + pr);
-      if (fabs(vy) < eps) vy = 0.;
-      vz = sz / (en1 + pr);
-      if (fabs(vz) < eps) vz = 0.;
+      if (cap < 100 && (v2 >= 1. || !conv)) {
+        // the seed failed: the iteration from the warm start
+        if (seed_failed) *seed_failed = 1;
+        vx = v[KVX];
+        vy = v[KVY];
+        vz = v[KVZ];
+        p0 = v[KPR];
+        cap = 1 << 30;
+        iv = 0;
+        continue;
+      }
+      if (v2 >= 1.) {
+        *iters = tot;
+        return 107;
+      }
+      cap = 1 << 30;
+      double nvx = sx / (en1 + pr);
+      if (fabs(nvx) < eps) nvx = 0.;
+      double nvy = sy / (en1 + pr);
+      if (fabs(nvy) < eps) nvy = 0.;
+      double nvz = sz / (en1 + pr);
+      if (fabs(nvz) < eps) nvz = 0.;
+      const double dv = fmax3(fabs(nvx - vx), fabs(nvy - vy), fabs(nvz - vz) * M.gp);
+      vx = nvx;
+      vy = nvy;
+      vz = nvz;
       vprim[KVX] = vx;
       vprim[KVY] = vy;
       vprim[KVZ] = vz;
-      if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) break;
+      if (conv) {
+        p0 = pr;
+        if (dv <= 1.e-14) break;
+      } else if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) {
+        break;
+      }
     }
     *iters = tot;
     v[KRH] = rh;

@@ -137,10 +137,10 @@ __device__ __forceinline__ void map_ghost(int j, int n, int cl, int cr, int& q, 
 #define ECHO_SSP_MINB 8
 #endif
 #define ECHO_UPDATE_BOUNDS(KIND, SEED)                                       \
-  __launch_bounds__(128, (SEED)                 ? ECHO_UPDATE_MINB_SEED   \
-                         : (KIND) == KIND_VISC ? ECHO_UPDATE_MINB_VISC   \
-                         : (KIND) == KIND_RES  ? ECHO_UPDATE_MINB_RES    \
-                                               : ECHO_UPDATE_MINB)
+  __launch_bounds__(128, (KIND) == KIND_VISC ? ECHO_UPDATE_MINB_VISC     \
+                         : (SEED)             ? ECHO_UPDATE_MINB_SEED     \
+                         : (KIND) == KIND_RES ? ECHO_UPDATE_MINB_RES      \
+                                              : ECHO_UPDATE_MINB)
 
 struct FaceArgs {
   DevPhys P;
@@ -560,9 +560,12 @@ __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, boo
   if (active) {
     double gm = M.gm, g3 = M.g3;
     double D = gm * uu[KRH], sx = gm * uu[KVX], sy = gm * uu[KVY], sz = gm * uu[KVZ], U = gm * uu[KPR];
-    double bx = gm * uu[KBX], by = gm * uu[KBY], bz = gm * uu[KBZ];
-    double B2 = bx * bx + by * by + bz * bz * g3;
-    double SB = sx * bx + sy * by + sz * bz;
+    double B2 = 0., SB = 0.;
+    if (Traits<KIND>::MHD) {
+      double bx = gm * uu[KBX], by = gm * uu[KBY], bz = gm * uu[KBZ];
+      B2 = bx * bx + by * by + bz * bz * g3;
+      SB = sx * bx + sy * by + sz * bz;
+    }
     double SS2 = sx * sx + sy * sy + sz * sz / g3;
     double E2 = 0.;
     if (Traits<KIND>::RES) {

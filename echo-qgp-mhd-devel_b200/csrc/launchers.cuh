@@ -80,8 +80,12 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   A.vsnap = nullptr;
   if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;  // no network loaded
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP && mode == MODE_RK)
-    update_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
+  // the learned seed: RMHD (ideal, resistive) and viscous runs
+  constexpr bool CAN_SEED = Traits<KIND>::MHD || Traits<KIND>::VISC;
+  if (CAN_SEED && A.algo == ECHO_C2P_MLP && mode == MODE_RK && Traits<KIND>::VISC && c->p.imex)
+    update_kernel<KIND, CAN_SEED, Traits<KIND>::VISC><<<blocks, 128, 0, c->stream>>>(A);
+  else if (CAN_SEED && A.algo == ECHO_C2P_MLP && mode == MODE_RK)
+    update_kernel<KIND, CAN_SEED><<<blocks, 128, 0, c->stream>>>(A);
   else if (Traits<KIND>::VISC && c->p.imex && mode == MODE_RK)
     update_kernel<KIND, false, Traits<KIND>::VISC><<<blocks, 128, 0, c->stream>>>(A);
   else
@@ -162,8 +166,9 @@ void launch_ssp_combine(EchoCtx* c, int stage) {
   A.mlp.par = c->d_mlp_par;
   if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;
   unsigned blocks = (unsigned)((c->g.ncell + 127) / 128);
-  if (Traits<KIND>::MHD && A.algo == ECHO_C2P_MLP)
-    ssp_combine_kernel<KIND, Traits<KIND>::MHD><<<blocks, 128, 0, c->stream>>>(A);
+  constexpr bool CAN_SEED = Traits<KIND>::MHD || Traits<KIND>::VISC;
+  if (CAN_SEED && A.algo == ECHO_C2P_MLP)
+    ssp_combine_kernel<KIND, CAN_SEED><<<blocks, 128, 0, c->stream>>>(A);
   else
     ssp_combine_kernel<KIND, false><<<blocks, 128, 0, c->stream>>>(A);
   if (Traits<KIND>::MHD && !Traits<KIND>::RES && c2p_alt_algo(A.algo))
@@ -235,6 +240,12 @@ void launch_batch_faces(EchoBatch* b, int dir) {
   }
 }
 
+// the batch runs the learned seed: a network is loaded and the equations have one
+template <int KIND>
+inline bool batch_seeded(const EchoBatch* b) {
+  return (Traits<KIND>::MHD || Traits<KIND>::VISC) && b->p.algo_solver == ECHO_C2P_MLP && b->d_mlp_frag;
+}
+
 template <int KIND>
 void launch_batch_update(EchoBatch* b, int irk) {
   static const double crk[3][3][2] = {{{0., 1.}, {0., 0.}, {0., 0.}},
@@ -270,13 +281,20 @@ void launch_batch_update(EchoBatch* b, int irk) {
   A.algo = b->p.algo_solver;
   A.mode = MODE_RK;
   A.tol = b->p.c2p_tol;
-  A.mlp.frag = nullptr;
-  A.mlp.par = nullptr;
-  if (Traits<KIND>::VISC && b->p.imex)
-    batch_update_kernel<KIND, false, Traits<KIND>::VISC>
-        <<<batch_grid(b, SL_UPDATE, PH_CELL), 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
-  else
-    batch_update_kernel<KIND, false><<<batch_grid(b, SL_UPDATE, PH_CELL), 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+  A.mlp.frag = b->d_mlp_frag;
+  A.mlp.par = b->d_mlp_par;
+  const unsigned grid = batch_grid(b, SL_UPDATE, PH_CELL);
+  if (batch_seeded<KIND>(b)) {
+    constexpr bool CAN_SEED = Traits<KIND>::MHD || Traits<KIND>::VISC;
+    if (Traits<KIND>::VISC && b->p.imex)
+      batch_update_kernel<KIND, CAN_SEED, Traits<KIND>::VISC><<<grid, 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+    else
+      batch_update_kernel<KIND, CAN_SEED><<<grid, 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+  } else if (Traits<KIND>::VISC && b->p.imex) {
+    batch_update_kernel<KIND, false, Traits<KIND>::VISC><<<grid, 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+  } else {
+    batch_update_kernel<KIND, false><<<grid, 128, 0, b->stream>>>(A, batch_dev(b), b->nv);
+  }
 }
 
 template <int KIND>
@@ -325,7 +343,12 @@ void batch_occupancy(const EchoBatch* b, int* per_sm) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FY], batch_faces_kernel<KIND, 1, REC_RUNTIME>, 128, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_FZ], batch_faces_kernel<KIND, 2, REC_RUNTIME>, 128, 0);
   }
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_UPDATE], batch_update_kernel<KIND, false>, 128, 0);
+  if (batch_seeded<KIND>(b))
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_UPDATE],
+                                                  batch_update_kernel<KIND, Traits<KIND>::MHD || Traits<KIND>::VISC>,
+                                                  128, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_UPDATE], batch_update_kernel<KIND, false>, 128, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[SL_SMOOTH], batch_smooth_kernel<KIND>, 128, 0);
 }
 

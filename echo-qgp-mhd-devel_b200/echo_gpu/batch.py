@@ -13,7 +13,7 @@ import ctypes
 
 import numpy as np
 
-from .lib import LL, EchoEventGrid, EchoEventStatus, I, P, _dp, load
+from .lib import LL, EchoEventGrid, EchoEventStatus, F, I, P, _dp, load
 from .params import EchoParams
 
 LIVE, DONE, CRASHED, COOLED = 0, 1, 2, 3
@@ -105,6 +105,13 @@ class Batch:
         self._check(self.lib.echo_batch_download(self.h, _dp(v), _dp(u)), "download")
         return v, u
 
+    def set_seed_network(self, weights, norm) -> None:
+        """Load a trained con2prim seed (echo_gpu.seed.train); needed before
+        running with algo_solver = C2P_MLP."""
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        n = np.ascontiguousarray(norm, dtype=np.float32)
+        self._check(self.lib.echo_batch_mlp_set(self.h, w.ctypes.data_as(F), n.ctypes.data_as(F)), "mlp_set")
+
     # -- stepping --------------------------------------------------------------
     def run(self, nsteps: int) -> None:
         self._check(self.lib.echo_batch_run(self.h, nsteps), "run")
@@ -132,7 +139,7 @@ class Batch:
         st = (EchoEventStatus * self.nev)()
         self._check(self.lib.echo_batch_status(self.h, st), "status")
         return [dict(t=s.t, dt=s.dt, steps=s.steps, state=s.state, errcode=s.errcode, err_cell=s.err_cell,
-                     c2p_iters=s.c2p_iters, repairs=s.repairs) for s in st]
+                     c2p_iters=s.c2p_iters, repairs=s.repairs, seed_fallbacks=s.seed_fallbacks) for s in st]
 
     def cell_updates(self) -> int:
         """Cells times completed steps, summed over the events."""

@@ -44,7 +44,8 @@ class EchoEventGrid(ctypes.Structure):
 class EchoEventStatus(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("steps", ctypes.c_longlong),
                 ("state", ctypes.c_int), ("errcode", ctypes.c_int), ("err_cell", ctypes.c_int),
-                ("pad", ctypes.c_int), ("c2p_iters", ctypes.c_longlong), ("repairs", ctypes.c_longlong)]
+                ("pad", ctypes.c_int), ("c2p_iters", ctypes.c_longlong), ("repairs", ctypes.c_longlong),
+                ("seed_fallbacks", ctypes.c_longlong)]
 
 
 LL = ctypes.POINTER(ctypes.c_longlong)
@@ -101,6 +102,7 @@ FUNCTIONS = {
     "echo_batch_glauber": (ctypes.c_int, [P, D, LL, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double]),
     "echo_batch_run": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_batch_mlp_set": (ctypes.c_int, [P, F, F]),
     "echo_batch_live": (ctypes.c_int, [P, I]),
     "echo_batch_status": (ctypes.c_int, [P, ctypes.POINTER(EchoEventStatus)]),
     "echo_batch_sync": (ctypes.c_int, [P]),

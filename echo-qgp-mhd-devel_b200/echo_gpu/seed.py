@@ -3,14 +3,17 @@ loading into a run.
 
 Pairs are (conserved, primitive) states the GPU solver itself produces:
 ideal-RMHD runs of the 3+1D Milne workload (or resistive runs of the
-resistive workload) at several energy scales and magnetisations, sampled
-every few steps.  The invariants and targets are computed here from u and v
+resistive workload, or viscous runs of the 2+1D viscous workload) at
+several energy scales and magnetisations (impact parameters), sampled every
+few steps.  The invariants and targets are computed here from u and v
 exactly as the device computes the invariants (csrc/kernels.cuh mlp_seed,
 csrc/mlp.cuh mlp_invariants):
   U = u_E/tau, D = u_rho/tau, S_i = u_i/tau, B^i = u_B/tau, E^i = u_E^i/tau
   (1/sqrt(-g) = 1/tau)
   f = (log U, D/U, S^2/U^2, B^2/U, (S.B)^2/U^3, E^2/U), target = (v^2, p/U),
-with E = 0 for ideal RMHD.
+with E = 0 for ideal RMHD and B = E = 0 for viscous hydro (U, S then hold
+the viscous stresses' share as well; the seed's v^2 and p/U are the
+fluid's).
 """
 from __future__ import annotations
 
@@ -28,21 +31,27 @@ NNORM = 16  # ECHO_MLP_NNORM
 NIN = 6  # ECHO_MLP_NIN
 
 
-def invariants_targets(u: np.ndarray, v: np.ndarray, t: float, nv: int):
-    """Invariants X (n x 6) and targets T (n x 2) of every cell of a state
-    (ideal RMHD: nv = 9, E^2/U = 0; resistive: nv = 12, E in u[8:11])."""
+def invariants_targets(u: np.ndarray, v: np.ndarray, t: float, cfg):
+    """Invariants X (n x 6) and targets T (n x 2) of every cell of a state of
+    a run of `cfg` (ideal RMHD: E^2/U = 0; resistive: E in u[8:11]; viscous
+    hydro: B = E = 0)."""
+    nv = cfg.nv
     uu = u.reshape(nv, -1) / t
     vv = v.reshape(nv, -1)
     g3 = t * t
     D, sx, sy, sz, E = uu[0], uu[1], uu[2], uu[3], uu[4]
-    bx, by, bz = uu[5], uu[6], uu[7]
-    B2 = bx * bx + by * by + bz * bz * g3
-    SB = sx * bx + sy * by + sz * bz
+    zero = np.zeros_like(E)
+    if cfg.mhd:
+        bx, by, bz = uu[5], uu[6], uu[7]
+        B2 = bx * bx + by * by + bz * bz * g3
+        SB = sx * bx + sy * by + sz * bz
+    else:
+        B2, SB = zero, zero
     SS2 = sx * sx + sy * sy + sz * sz / g3
-    if nv == 12:
+    if cfg.mhd == 2:
         E2 = uu[8] ** 2 + uu[9] ** 2 + g3 * uu[10] ** 2
     else:
-        E2 = np.zeros_like(E)
+        E2 = zero
     X = np.stack([np.log(E), D / E, SS2 / E**2, B2 / E, SB * SB / E**3, E2 / E], 1)
     x2 = vv[1] ** 2 + vv[2] ** 2 + g3 * vv[3] ** 2
     T = np.stack([x2, vv[4] / E], 1)
@@ -70,8 +79,17 @@ def _magnetised(cfg, tab, peak_scale: float, mag: float, seed: int, flow: float 
     return v.reshape(-1)
 
 
+def _scaled(cfg, tab, peak_scale: float, b: float, seed: int):
+    """Primitives of the viscous workload (MC Glauber at impact parameter b)
+    with the energy density scaled as in _magnetised."""
+    v = I.primitives(cfg, tab, seed=seed, b=b).reshape(cfg.nv, -1).copy()
+    e = np.interp(v[4], tab[:, 2], tab[:, 1])
+    v[4] = I.table_pressure(tab, cfg.enezero + peak_scale * (e - cfg.enezero))
+    return v.reshape(-1)
+
+
 def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: int = 12, every: int = 3,
-                   rng_seed: int = 5, exact: bool = False, resistive: bool = False):
+                   rng_seed: int = 5, exact: bool = False, resistive: bool = False, viscous: bool = False):
     """Run the GPU solver on the RMHD workload (the full 97x97x81 grid, or a
     grid^3-sized version with the same spacing, EoS and scheme) at several
     energy scales and magnetisations and collect (invariants, targets)
@@ -79,7 +97,9 @@ def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: in
     region a central sub-grid never reaches.  resistive: the resistive
     workload instead (193x193x129 over the same extent at half the
     resolution, or grid^3 at full resolution), at rest and with smooth flows
-    of amplitude 0.1 and 0.3 carrying 0.7 of the ideal E."""
+    of amplitude 0.1 and 0.3 carrying 0.7 of the ideal E.  viscous: the
+    2+1D viscous workload (201x201, or grid^2), MC-Glauber events at 3
+    energy scales x impact parameters 0, 5 and 10 fm."""
     rng = np.random.default_rng(rng_seed)
     tab = I.eos_table_loaded()
     if resistive:
@@ -89,6 +109,9 @@ def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: in
         else:
             base = P.small(c4, grid, nz=max(8, int(grid * 0.67)))
         variants = [(s, m, f) for s in (0.3, 1.0, 3.0) for m in (0.1, 0.3) for f in (0.0, 0.1, 0.3)]
+    elif viscous:
+        base = P.config2() if grid is None else P.small(P.config2(), grid)
+        variants = [(s, b, 0.0) for s in (0.3, 1.0, 3.0) for b in (0.0, 5.0, 10.0)]
     else:
         base = P.config1() if grid is None else P.small(P.config1(), grid, nz=max(8, int(grid * 0.84)))
         base = base.replace(algo_solver=P.C2P_NEWTON)
@@ -98,7 +121,11 @@ def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: in
     per = max(1, n_target // (len(variants) * (steps // every)))
     for k, (scale, mag, flow) in enumerate(variants):
         ev = Evolve(base.to_c(przero=przero), tab, exact=exact)
-        ev.upload(_magnetised(base, tab, scale, mag, seed=k, flow=flow), None, base.tstart)
+        if viscous:
+            v0 = _scaled(base, tab, scale, mag, seed=k)
+        else:
+            v0 = _magnetised(base, tab, scale, mag, seed=k, flow=flow)
+        ev.upload(v0, None, base.tstart)
         for s in range(1, steps + 1):
             ev.run(1)
             if s % every == 0:
@@ -108,7 +135,7 @@ def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: in
                     break
                 v, u = ev.download()
                 # the step's last inversion used the metric of the step's start
-                X, T = invariants_targets(u, v, st.t - st.dt, base.nv)
+                X, T = invariants_targets(u, v, st.t - st.dt, base)
                 ok = np.isfinite(X).all(1) & np.isfinite(T).all(1)
                 idx = np.nonzero(ok)[0]
                 take = rng.choice(idx, size=min(per, len(idx)), replace=False)

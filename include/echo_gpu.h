@@ -395,6 +395,7 @@ typedef struct EchoEventStatus {
   int pad;
   long long c2p_iters;  /* con2prim iterations of the last stage */
   long long repairs;    /* con2prim repairs so far */
+  long long seed_fallbacks; /* learned seeds that needed the warm start so far */
 } EchoEventStatus;
 
 /* launch-shape slots (echo_batch_set_schedule) */
@@ -432,6 +433,10 @@ int echo_batch_download(EchoBatch* b, double* v, double* u);
 /* nsteps time steps of every live event, asynchronous (one CUDA graph per
  * step); finished and crashed events drop out on the device */
 int echo_batch_run(EchoBatch* b, int nsteps);
+/* Loads a trained con2prim seed network (echo_gpu_mlp_train layout) into
+ * the batch; required before running with algo_solver = ECHO_C2P_MLP.
+ * Allocates. */
+int echo_batch_mlp_set(EchoBatch* b, const float* weights, const float* norm);
 /* synchronises; number of live events */
 int echo_batch_live(EchoBatch* b, int* nlive);
 /* synchronises; status of every event (nev entries) */
