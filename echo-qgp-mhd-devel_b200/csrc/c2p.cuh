@@ -859,7 +859,7 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
     double et = U - 0.5 * (E2 + B2);
     double s2 = g1 * sx * sx + g2 * sy * sy + g3 * sz * sz;
     double w = 0, v2 = 0, glf, en, drhdpr, dendpr, pr_eos = 0, dprdrh = 0, dprden = 0, f, df, dpr;
-    bool conv = false;
+    bool newton_ok = false;
     int iter;
     for (iter = 1; iter <= 100; iter++) {
       w = et + pr;
@@ -875,14 +875,14 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
       df = dprdrh * drhdpr + dprden * dendpr - 1.;
       dpr = -f / df;
       if (fabs(dpr) < ntol * pr) {
-        conv = true;
+        newton_ok = true;
         break;
       }
       if (iter >= cap) break;
       pr = pr + dpr;
     }
     total += iter;
-    if (cap < 100 && (v2 >= 1. || !conv)) {
+    if (cap < 100 && (v2 >= 1. || !newton_ok)) {
       // the seed failed: the fixed point from the warm start
       if (seed_failed) *seed_failed = 1;
       vel[0] = v[KVX];
@@ -1043,7 +1043,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
       double sx = sx_cov, sy = sy_cov, sz = sz_cov / g3;
       double s2 = sx * sx_cov + sy * sy_cov + sz * sz_cov;
       pr = p0;
-      bool conv = false;
+      bool newton_ok = false;
       for (int ip = 1; ip <= 100; ip++) {
         tot++;
         v2 = s2 / ((en1 + pr) * (en1 + pr));
@@ -1058,13 +1058,13 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
         df = dprdrh * drhdpr + dprden * dendpr - 1.;
         dpr = -f / df;
         if (fabs(dpr) < ntol * pr) {
-          conv = true;
+          newton_ok = true;
           break;
         }
         if (ip >= cap) break;
         pr = pr + dpr;
       }
-      if (cap < 100 && (v2 >= 1. || !conv)) {
+      if (cap < 100 && (v2 >= 1. || !newton_ok)) {
         // the seed failed: the iteration from the warm start
         if (seed_failed) *seed_failed = 1;
         vx = v[KVX];
