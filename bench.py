@@ -359,7 +359,7 @@ def run_viscous(args, torch, barrier, world, rank, X1, T1):
         "value": variants["mlp_seeded"]["value"], "unit": UNIT, "steps": steps,
         "ms_per_step": variants["mlp_seeded"]["ms_per_step"], "variants": variants, "seed_training": training,
         "c2p_iters": "Newton steps per cell summed over the nested iteration's passes, last stage",
-    }, (w, norm)
+    }, (Xv, Tv)
 
 
 def run_batched(args, torch, barrier, world, rank, net=None):
@@ -367,12 +367,14 @@ def run_batched(args, torch, barrier, world, rank, net=None):
     events (viscous 2+1D, grids 61^2..161^2) from tau = 0.4 to 10 fm/c in
     one batch, beside the same events run one after another through the
     single-grid path, and again with the MLP-seeded inversion (net: the
-    viscous seed network).  With N ranks the events are split across the
+    2+1D viscous workload's training pairs, joined by pairs of this one's
+    events).  With N ranks the events are split across the
     GPUs by cell count (no collective on the data path): the whole job's
     cell-updates over the slowest rank's time."""
     from echo_gpu import events as EV
     from echo_gpu import initial as I
     from echo_gpu import params as P
+    from echo_gpu import seed as S
     from echo_gpu import shard as SH
     from echo_gpu.batch import Batch, event_grid
     from echo_gpu.lib import Evolve
@@ -411,9 +413,23 @@ def run_batched(args, torch, barrier, world, rank, net=None):
     st = SH.gather_status(mine, st_local, full.nev)
     seeded = None
     if net is not None:
+        # the seed for this workload: pairs from a sample of its own events run
+        # to the end time (dilute late stages, its EoS table) with the viscous
+        # workload's pairs, one network
+        t0 = time.perf_counter()
+        Xe, Te = S.generate_event_pairs(full, tab, przero, pcut, n_target=args.pairs // 2, sources=srcs_all)
+        Xb = np.concatenate([net[0], Xe])
+        Tb = np.concatenate([net[1], Te])
+        t1 = time.perf_counter()
+        wb, nb, lb = S.train(Xb, Tb, steps=args.train_steps)
+        t2 = time.perf_counter()
+        training = {"pairs": int(len(Xb)), "event_pairs": int(len(Xe)), "pair_generation_s": t1 - t0,
+                    "train_s": t2 - t1, "loss_first": float(lb[0]), "loss_last": float(lb[-1]),
+                    "source": "every 32nd event of the batch run alone to the end time (8 samples each) plus the "
+                              "2+1D viscous workload's pairs"}
         pcm = es.cfg.replace(algo_solver=P.C2P_MLP).to_c(przero=przero, smooth_pressure=pcut)
         bm = Batch(pcm, tab, [event_grid(*es.grid(e)) for e in range(es.nev)])
-        bm.set_seed_network(*net)
+        bm.set_seed_network(wb, nb)
         bm.glauber(srcs, es.cfg.tstart, es.tmax)
         bm.autotune(3)
         bm.run(max(args.warmup, 3))
@@ -435,7 +451,7 @@ def run_batched(args, torch, barrier, world, rank, net=None):
         crashed = SH.reduce_sum(sum(1 for s in stm if s["state"] == 2), device="cuda")
         bm.close()
         seeded = {"value": cu_m / (ms_m / 1e3), "ms": ms_m, "cell_updates": int(cu_m),
-                  "seed_fallbacks_total": int(fb), "events_crashed": int(crashed)}
+                  "seed_fallbacks_total": int(fb), "events_crashed": int(crashed), "seed_training": training}
     # the same events one at a time through the single-grid path (a sample)
     b.glauber(srcs, es.cfg.tstart, es.tmax)
     v0 = b.split(b.download()[0])
@@ -476,6 +492,8 @@ def run_batched(args, torch, barrier, world, rank, net=None):
         "scaling": "strong" if world > 1 else None,
         "sharding": f"events split over {world} GPU(s) by cell count, no data-path collective",
         "cell_updates": int(cu), "events_done": int(states[1]), "events_crashed": int(states[2]),
+        "crashed": [{"event": int(e), "b": float(full.b[e]), "n": int(full.n[e]), "errcode": int(x["errcode"]),
+                     "t": round(float(x["t"]), 4)} for e, x in enumerate(st) if x["state"] == 2],
         "event_steps_min_max": [int(min(s["steps"] for s in st)), int(max(s["steps"] for s in st))],
         "sequential_single_grid": {"value": seq, "unit": UNIT,
                                    "sample": "every 16th event of rank 0's share, 20 steps each, one GPU"},

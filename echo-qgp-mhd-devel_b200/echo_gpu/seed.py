@@ -147,6 +147,47 @@ def generate_pairs(n_target: int = 1_000_000, grid: int | None = None, steps: in
     return X, T
 
 
+def generate_event_pairs(es, tab, przero: float, smooth_pressure: float, n_target: int = 300_000,
+                         every_event: int = 32, samples: int = 8, rng_seed: int = 6, sources=None):
+    """Pairs from the batched event-by-event workload: every `every_event`-th
+    event of the EventSet `es` run alone (single grid, its own EoS table,
+    grid and end time) from its initial state to es.tmax, sampled at
+    `samples` times spread over the run, so that the dilute late stages the
+    batch reaches are in the training set."""
+    from . import events as EV
+
+    rng = np.random.default_rng(rng_seed)
+    picks = list(range(0, es.nev, every_event))
+    v0 = EV.event_primitives(EV.EventSet(cfg=es.cfg, b=es.b[picks], n=es.n[picks], dx=es.dx, tmax=es.tmax), tab,
+                             sources=None if sources is None else [sources[e] for e in picks])
+    per = max(1, n_target // (len(picks) * samples))
+    Xs, Ts = [], []
+    for k, e in enumerate(picks):
+        cfg = es.event_config(e)
+        ev = Evolve(cfg.to_c(przero=przero, smooth_pressure=smooth_pressure), tab)
+        ev.upload(v0[k], None, cfg.tstart)
+        ev.set_tout(es.tmax)
+        span = es.tmax - cfg.tstart
+        for j in range(1, samples + 1):
+            target = cfg.tstart + span * j / samples
+            for _ in range(20000):
+                st = ev.stats()
+                if st.errcode or st.t >= target - 1e-12:
+                    break
+                ev.run(4)
+                ev.sync()
+            if st.errcode:
+                break
+            v, u = ev.download()
+            X, T = invariants_targets(u, v, st.t - st.dt, cfg)
+            ok = np.nonzero(np.isfinite(X).all(1) & np.isfinite(T).all(1))[0]
+            take = rng.choice(ok, size=min(per, len(ok)), replace=False)
+            Xs.append(X[take])
+            Ts.append(T[take])
+        ev.close()
+    return np.concatenate(Xs), np.concatenate(Ts)
+
+
 def train(X: np.ndarray, T: np.ndarray, steps: int = 3000, batch: int = 4096, lr: float = 3e-3,
           seed: int = 1, report_every: int = 100):
     """Train the seed network on the GPU; returns (weights, norm, losses)."""
