@@ -76,7 +76,8 @@ def main():
     if a.c2p == "mlp":
         from . import seed as S
 
-        X, T = S.generate_pairs(n_target=a.pairs)
+        # pairs of the run's own equation set
+        X, T = S.generate_pairs(n_target=a.pairs, resistive=cfg.mhd == 2, viscous=bool(cfg.viscosity))
         w, norm, _ = S.train(X, T, steps=a.train_steps)
         ev.set_seed_network(w, norm)
     ev.upload(I.primitives(cfg, tab), None, cfg.tstart)
