@@ -810,9 +810,10 @@ __device__ __forceinline__ void ohm_solve(const DevPhys& P, const Metric& M, con
 // after 200 passes.  It starts from the previous primitives in v (the
 // reference's warm start) or, given the learned seed (x = v^2, q = p/U of
 // the total energy U), from p = q U and v along the fluid momentum S - E x B
-// (E of u) with |v|^2 = x; the seeded first pass gets 3 Newton steps, and a
-// seed that fails them restarts the fixed point from the warm start
-// (*seed_failed = 1).  v[KEX..KEZ] receives E and, when h > 0, u[KEX..KEZ]
+// (E of u) with |v|^2 = x; the seeded first pass gets 3 Newton steps, whose
+// last must be below 1e-10 of p (the seed's residual bar), and is always
+// followed by a pass at the full tolerance; a seed that fails restarts the
+// fixed point from the warm start (*seed_failed = 1).  v[KEX..KEZ] receives E and, when h > 0, u[KEX..KEZ]
 // sqrt(-g) E: the implicit solve changes the conserved E.
 inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u, double* v, int* iters,
                                     double h, const float* seed = nullptr, int* seed_failed = nullptr) {
@@ -878,7 +879,10 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
         newton_ok = true;
         break;
       }
-      if (iter >= cap) break;
+      if (iter >= cap) {  // the seed's budget, judged at a 1e-10 step
+        newton_ok = fabs(dpr) < 1.e-10 * pr;
+        break;
+      }
       pr = pr + dpr;
     }
     total += iter;
@@ -897,13 +901,14 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
       *iters = total;
       return 777;
     }
+    const bool seeded_pass = cap < 100;  // another pass at the full tolerance follows
     cap = 1 << 30;
     double vn0 = sx / w, vn1 = sy / w, vn2 = sz / w;
     double dv = fmax3(fabs(vn0 - vel[0]), fabs(vn1 - vel[1]), fabs(vn2 - vel[2]) * gp);
     vel[0] = vn0;
     vel[1] = vn1;
     vel[2] = vn2;
-    if (!(h > 0.) || dv <= vtol) break;
+    if (!seeded_pass && (!(h > 0.) || dv <= vtol)) break;
   }
   *iters = total;
   if (outer > 200) return 779;
@@ -997,7 +1002,8 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
     // pass's p): the inversion's own root, at equal residual whatever the
     // start.  With the learned seed (x = v^2, q = p/U) the first pass starts
     // from v along S with |v|^2 = x and p = q U and its Newton gets 3
-    // steps; a seed that fails restarts from the warm start
+    // steps, the last below 1e-10 of p, with a pass at the full tolerance
+    // after it; a seed that fails restarts from the warm start
     // (*seed_failed = 1).
     double uin[T::NV], vprim[T::NV];
 #pragma unroll
@@ -1061,7 +1067,10 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
           newton_ok = true;
           break;
         }
-        if (ip >= cap) break;
+        if (ip >= cap) {  // the seed's budget, judged at a 1e-10 step
+          newton_ok = fabs(dpr) < 1.e-10 * pr;
+          break;
+        }
         pr = pr + dpr;
       }
       if (cap < 100 && (v2 >= 1. || !newton_ok)) {
@@ -1079,6 +1088,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
         *iters = tot;
         return 107;
       }
+      const bool seeded_pass = cap < 100;  // another pass at the full tolerance follows
       cap = 1 << 30;
       double nvx = sx / (en1 + pr);
       if (fabs(nvx) < eps) nvx = 0.;
@@ -1095,7 +1105,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
       vprim[KVZ] = vz;
       if (conv) {
         p0 = pr;
-        if (dv <= 1.e-14) break;
+        if (dv <= 1.e-14 && !seeded_pass) break;
       } else if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) {
         break;
       }
