@@ -54,7 +54,12 @@ enum { ECHO_MINKOWSKI = 1, ECHO_BJORKEN = 2 };
 /* equations of state (EOS, eos.f90:158-188) */
 enum { ECHO_EOS_CONFORMAL = 1, ECHO_EOS_IDEALGAS = 2, ECHO_EOS_TABLE = 3 };
 
-/* con2prim solvers for ideal MHD (ALG_SOLV, common.f90:289) */
+/* con2prim solvers (ALG_SOLV, common.f90:289).  Ideal MHD as below.  The
+ * viscous inversion (system.f90:564-666) runs the reference's nested loop,
+ * which ends after one outer pass, under 1..6, and iterates it to its fixed
+ * point (max |dv| <= 1e-14) under ECHO_C2P_NEWTON and ECHO_C2P_MLP.  The
+ * resistive inversion (MHD = 2) is its own fixed point under every value;
+ * ECHO_C2P_MLP seeds it. */
 enum {
   ECHO_C2P_BRENT = 1,   /* reference default: BRENTM on (v^2, w*gamma^2, p);
                            2..6 are the reference's other ideal-MHD solvers
