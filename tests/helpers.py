@@ -107,3 +107,27 @@ def gubser_case(n=81, dx=0.1, dt=0.01, tau0=1.0):
     z = np.zeros_like(X)
     v = np.stack([np.ones_like(X), vr * X / rs, vr * Y / rs, z, p]).reshape(-1)
     return cfg, v, X, Y
+
+
+# the golden fixtures (tests/golden/<name>.npz): case, parameter changes,
+# steps, and whether the state carries the resistive flow and field
+GOLDEN_CASES = {
+    "hd2d": ("hd2d", {}, 10, False),
+    "rmhd3d": ("rmhd3d", {}, 3, False),
+    "visc2d": ("visc2d", {}, 5, False),
+    # the viscous inversion iterated to its fixed point, IMEX RK2
+    "visc2d_fixed_point": ("visc2d", {"imex": 1, "algo_solver": P.C2P_NEWTON}, 5, False),
+    # resistive RMHD, IMEX-SSP3(4,3,3) with the implicit Ohm's law
+    "res3d": ("res3d", {"sigma_el": 500.0}, 3, True),
+}
+
+
+def golden_setup(name):
+    """(cfg, params, eos table, initial primitives, steps) of a golden case."""
+    case, changes, steps, resistive = GOLDEN_CASES[name]
+    cfg = CASES[case]().replace(**changes)
+    pc, tab, v0 = setup(cfg)
+    if resistive:
+        v0 = resistive_state(cfg, tab)
+    return cfg, pc, tab, v0, steps
+

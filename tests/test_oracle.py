@@ -10,7 +10,7 @@ import pytest
 import pyoracle as O
 from echo_gpu import initial as I
 from echo_gpu import params as P
-from helpers import CASES, eos_table, gubser, gubser_case, rel_linf, setup
+from helpers import CASES, GOLDEN_CASES, eos_table, golden_setup, gubser, gubser_case, rel_linf, setup
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -75,15 +75,15 @@ def test_eos_table_file_round_trip(tmp_path):
     assert (np.diff(back[:, 2]) > 0).all() and (np.diff(back[:, 0]) > 0).all()
 
 
-@pytest.mark.parametrize("name", ["hd2d", "rmhd3d", "visc2d"])
+@pytest.mark.parametrize("name", list(GOLDEN_CASES))
 def test_golden_vectors(name):
     path = os.path.join(GOLDEN, f"{name}.npz")
     if not os.path.exists(path):
         pytest.skip("golden fixture missing")
     g = np.load(path)
     meta = json.loads(str(g["meta"]))
-    cfg = CASES[name]()
-    pc, tab, v = setup(cfg)
+    cfg, pc, tab, v, steps = golden_setup(name)
+    assert steps == meta["steps"]
     assert np.array_equal(v, g["v0"])
     o = O.Oracle(pc, tab)
     o.set_state(g["v0"], None, cfg.tstart)
