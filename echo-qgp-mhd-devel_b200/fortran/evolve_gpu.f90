@@ -73,6 +73,15 @@ module evolve_gpu
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
     end function
+
+    ! learned con2prim seed (ALG_SOLV = 101): weights(ECHO_MLP_NWEIGHTS) and
+    ! norm(ECHO_MLP_NNORM) as echo_gpu_mlp_train writes them; before the
+    ! first evolve_main
+    integer(c_int) function echo_gpu_mlp_set(ctx, weights, norm) bind(C, name="echo_gpu_mlp_set")
+      import :: c_int, c_ptr, c_float
+      type(c_ptr), value :: ctx
+      real(c_float), intent(in) :: weights(*), norm(*)
+    end function
   end interface
 
 contains
