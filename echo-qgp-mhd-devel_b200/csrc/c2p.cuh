@@ -841,7 +841,7 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
       pr = q * U;
       cap = 3;
     } else if (seed_failed) {
-      *seed_failed = 1;
+      *seed_failed |= 1;
     }
   }
   int errcode = 0, outer, total = 0;
@@ -881,6 +881,7 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
       }
       if (iter >= cap) {  // the seed's budget, judged at a 1e-10 step
         newton_ok = fabs(dpr) < 1.e-10 * pr;
+        if (newton_ok) pr = pr + dpr;  // the full-tolerance pass starts from the corrected p
         break;
       }
       pr = pr + dpr;
@@ -888,7 +889,7 @@ inline __device__ int cons2prim_res(const DevPhys& P, const Metric& M, double* u
     total += iter;
     if (cap < 100 && (v2 >= 1. || !newton_ok)) {
       // the seed failed: the fixed point from the warm start
-      if (seed_failed) *seed_failed = 1;
+      if (seed_failed) *seed_failed |= 1;
       vel[0] = v[KVX];
       vel[1] = v[KVY];
       vel[2] = v[KVZ];
@@ -1032,7 +1033,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
         p0 = q * et;
         cap = 3;
       } else if (seed_failed) {
-        *seed_failed = 1;
+        *seed_failed |= 1;
       }
     }
     int tot = 0;
@@ -1069,13 +1070,14 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
         }
         if (ip >= cap) {  // the seed's budget, judged at a 1e-10 step
           newton_ok = fabs(dpr) < 1.e-10 * pr;
+          if (newton_ok) pr = pr + dpr;  // the full-tolerance pass starts from the corrected p
           break;
         }
         pr = pr + dpr;
       }
       if (cap < 100 && (v2 >= 1. || !newton_ok)) {
         // the seed failed: the iteration from the warm start
-        if (seed_failed) *seed_failed = 1;
+        if (seed_failed) *seed_failed |= 1;
         vx = v[KVX];
         vy = v[KVY];
         vz = v[KVZ];
@@ -1169,7 +1171,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
             X[2] = Xs[2];
           }
         }
-        if (it <= 0 && seed_failed) *seed_failed = 1;
+        if (it <= 0 && seed_failed) *seed_failed |= 1;
       }
       if (it <= 0) {  // plain path: Newton from the previous primitives
         double Xn[3] = {X[0], X[1], X[2]};
@@ -1185,7 +1187,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
         nfev = it;
       } else {
         (void)brentm3(P, s, X, 1.e-14, 1.e-14, 300, 3, &nfev);
-        nfev += 1000;  // marks a bracketed fallback in the iteration statistics
+        if (seed_failed) *seed_failed |= 2;  // a bracketed fallback, counted on its own
       }
     } else {
       (void)brentm3(P, s, X, 1.e-14, 1.e-14, 300, 3, &nfev);

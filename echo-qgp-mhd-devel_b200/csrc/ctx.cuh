@@ -50,12 +50,16 @@ struct EchoCtx {
   void* d_out;              // output staging (echo_gpu_out_vars), grown on demand
   size_t out_bytes;
   unsigned long long* d_out_err;
+  // the fused stage kernel (stage.cuh): usable, on, tile, segment, launch
+  int st_ok, st_on, st_tx, st_ty, st_zseg, st_nt;
+  unsigned st_grid;
+  size_t st_smem;
 };
 void echo_out_free(EchoCtx* c);
 
 // kernel classes reported by echo_gpu_profile_step
 enum { PK_FACES_X = 0, PK_FACES_Y = 1, PK_FACES_Z = 2, PK_SCALARS = 3, PK_UPDATE = 4, PK_REPAIR = 5, PK_END = 6,
-       PK_N = 7 };
+       PK_STAGE = 7, PK_N = 8 };
 
 inline void mark(EchoCtx* c, int cls) {
   if (!c->marks) return;
@@ -66,6 +70,7 @@ inline void mark(EchoCtx* c, int cls) {
 }
 
 // shared by the single-grid and the batched contexts (echo_gpu.cu)
+int echo_check_params(const EchoParams* p, const double* eos_table, int n_eos);
 int echo_kind_of(const EchoParams* p);
 int echo_nv_of(int kind);
 void echo_setup_bc(const EchoParams* p, int nv, BcDir bc[3], int uniform[3], int sign[3]);
@@ -91,5 +96,9 @@ template <int KIND>
 void launch_ssp_combine(EchoCtx* c, int stage);
 template <int KIND>
 void launch_ssp_stage1(EchoCtx* c);
+template <int KIND>
+int setup_stage(EchoCtx* c, int tx, int ty, int zseg);
+template <int KIND>
+void launch_stage(EchoCtx* c, int irk, int mode, double* du_out);
 
 }  // namespace echo

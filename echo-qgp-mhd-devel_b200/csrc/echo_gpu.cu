@@ -205,11 +205,21 @@ static void enqueue_stage_ssp(EchoCtx* c, int irk) {
     mark(c, PK_REPAIR);
     c->vcur = 1 - c->vcur;
   }
-  enqueue_sweeps(c);
-  launch_scalars(c, irk, 2);
-  mark(c, PK_SCALARS);
-  DISPATCH(c, launch_update, c, irk, MODE_RHS, c->d_dussp[irk - 1]);
-  mark(c, PK_UPDATE);
+  if (c->st_ok && c->st_on) {
+    // sweeps + right-hand side in one kernel; the GLM scalars after it (the
+    // right-hand side reads none of them)
+    cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream);
+    DISPATCH(c, launch_stage, c, irk, MODE_RHS, c->d_dussp[irk - 1]);
+    mark(c, PK_STAGE);
+    launch_scalars(c, irk, 2);
+    mark(c, PK_SCALARS);
+  } else {
+    enqueue_sweeps(c);
+    launch_scalars(c, irk, 2);
+    mark(c, PK_SCALARS);
+    DISPATCH(c, launch_update, c, irk, MODE_RHS, c->d_dussp[irk - 1]);
+    mark(c, PK_UPDATE);
+  }
   if (irk == 1 && c->kind == KIND_RES) {
     DISPATCH(c, launch_ssp_stage1, c);
     mark(c, PK_UPDATE);
@@ -231,19 +241,32 @@ static void enqueue_stage(EchoCtx* c, int irk) {
     return;
   }
   cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream);
-  for (int d = 0; d < 3; d++) {
-    int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
-    if (n > 1) {
-      DISPATCH(c, launch_faces, c, d);
-      mark(c, PK_FACES_X + d);
+  // the fused stage needs dt before the faces: every stage but the first,
+  // and the first with divergence cleaning (dt = CFL, evolve.f90:734-735)
+  if (c->st_ok && c->st_on && (irk > 1 || c->p.divclean)) {
+    launch_scalars(c, irk, 3);
+    cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
+    cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
+    mark(c, PK_SCALARS);
+    DISPATCH(c, launch_stage, c, irk, MODE_RK, (double*)nullptr);
+    mark(c, PK_STAGE);
+    launch_scalars(c, irk, 4);
+    mark(c, PK_SCALARS);
+  } else {
+    for (int d = 0; d < 3; d++) {
+      int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
+      if (n > 1) {
+        DISPATCH(c, launch_faces, c, d);
+        mark(c, PK_FACES_X + d);
+      }
     }
+    launch_scalars(c, irk);
+    cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
+    cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
+    mark(c, PK_SCALARS);
+    DISPATCH(c, launch_update, c, irk, MODE_RK, (double*)nullptr);
+    mark(c, PK_UPDATE);
   }
-  launch_scalars(c, irk);
-  cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
-  cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
-  mark(c, PK_SCALARS);
-  DISPATCH(c, launch_update, c, irk, MODE_RK, (double*)nullptr);
-  mark(c, PK_UPDATE);
   // stage 1 wrote the new u into the other buffer: it becomes current before
   // the repair and the smoothing, which act on the new u
   if (irk == 1) c->ucur = 1 - c->ucur;
@@ -279,16 +302,10 @@ static void advance_roles(EchoCtx* c) {
   if (c->p.viscosity) c->vn = 1 - c->vn;
 }
 
-// ---------------------------------------------------------------------------
-// C-ABI
-// ---------------------------------------------------------------------------
-extern "C" {
-
-int echo_gpu_nv(const EchoCtx* c) { return c ? c->nv : 0; }
-
-int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoCtx** out) {
-  if (!p || !out) return ECHO_ERR_ARG;
-  *out = nullptr;
+// The parameter checks of a run, shared by every entry point that takes an
+// EchoParams: equation set, integrator, grid and EoS table.
+int echo_check_params(const EchoParams* p, const double* eos_table, int n_eos) {
+  if (!p) return ECHO_ERR_ARG;
   if (p->mhd > 2 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
   if (p->nrk != ECHO_RK2 && p->nrk != ECHO_RK3 && p->nrk != ECHO_SSP) return ECHO_ERR_UNSUPPORTED;
   // resistive runs: IMEX-SSP (common.f90:2114-2118), with GLM cleaning
@@ -299,6 +316,23 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return ECHO_ERR_ARG;
   if ((p->nx > 1 && p->nx < 3) || (p->ny > 1 && p->ny < 3) || (p->nz > 1 && p->nz < 3)) return ECHO_ERR_ARG;
   if (p->eqstate == ECHO_EOS_TABLE && (!eos_table || n_eos < 2)) return ECHO_ERR_ARG;
+  return ECHO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C-ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int echo_gpu_nv(const EchoCtx* c) { return c ? c->nv : 0; }
+
+int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoCtx** out) {
+  if (!p || !out) return ECHO_ERR_ARG;
+  *out = nullptr;
+  {
+    int r = echo_check_params(p, eos_table, n_eos);
+    if (r) return r;
+  }
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return ECHO_ERR_CUDA;
   EchoCtx* c = (EchoCtx*)calloc(1, sizeof(EchoCtx));
@@ -364,6 +398,10 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->d_out = nullptr;
   c->out_bytes = 0;
   c->d_out_err = nullptr;
+  // the fused stage kernel, when the run allows it (else the sweep kernels)
+  DISPATCH(c, setup_stage, c, 0, 0, 0);
+  c->st_on = 0;
+  (void)cudaGetLastError();
   *out = c;
   return ECHO_OK;
 }
@@ -684,6 +722,38 @@ int echo_gpu_profile_step(EchoCtx* c, double* ms, int* launches) {
   return ECHO_OK;
 }
 
+int echo_gpu_set_stage(EchoCtx* c, int fused, int tx, int ty, int zseg, int* info) {
+  (void)cudaGetLastError();
+  if (!c || (fused != 0 && fused != 1)) return ECHO_ERR_ARG;
+  if (fused) {
+    if (tx < 0 || ty < 0 || zseg < 0) return ECHO_ERR_ARG;
+    DISPATCH(c, setup_stage, c, tx, ty, zseg);
+    (void)cudaGetLastError();
+    if (!c->st_ok) {
+      c->st_on = 0;
+      return ECHO_ERR_UNSUPPORTED;
+    }
+  }
+  c->st_on = fused && c->st_ok;
+  // the cached step graphs hold the other kernels
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < 8; i++)
+    if (c->graph_ok[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph_ok[i] = false;
+    }
+  if (info) {
+    info[0] = c->st_on;
+    info[1] = c->st_tx;
+    info[2] = c->st_ty;
+    info[3] = c->st_zseg;
+    info[4] = c->st_nt;
+    info[5] = (int)c->st_grid;
+    info[6] = (int)c->st_smem;
+  }
+  return ECHO_OK;
+}
+
 int echo_gpu_sync(EchoCtx* c) {
   if (!c) return ECHO_ERR_ARG;
   CK(cudaStreamSynchronize(c->stream));
@@ -704,6 +774,7 @@ int echo_gpu_stats(EchoCtx* c, EchoStats* st) {
   st->repairs = (long long)s->repairs;
   st->seed_fallbacks = (long long)s->fallbacks;
   st->errcode = errcode_of(s, &st->err_cell);
+  st->bracket_fallbacks = (long long)s->brackets;
   return ECHO_OK;
 }
 

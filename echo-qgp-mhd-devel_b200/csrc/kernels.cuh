@@ -30,6 +30,7 @@ struct DevScalars {
   int nfail, pad;
   unsigned long long c2p_iters, c2p_cells, repairs, fallbacks;
   unsigned long long check_bits;  // check_temp maximum (bit pattern of a double >= 0)
+  unsigned long long brackets;    // con2prim solves that fell back to the bracketed BRENTM
 };
 
 struct Grid {
@@ -196,6 +197,87 @@ __host__ __device__ __forceinline__ size_t faces_of(const Grid& g) {
                     : (size_t)g.nx * g.ny * (g.nz + 1);
 }
 
+// The face after reconstruction (shared by the sweep kernels and the fused
+// stage kernel): the p <= 0 / v^2 >= 1 fix-ups (evolve.f90:334-369, w0 = the
+// cell left of the face), GLM upwinding (work_glm[xyz], work.f90:67-139)
+// with wave speed ch, the two system_flux calls and the HLL flux
+// (work.f90:195-229).  Writes F[NV] and the face's signal speed
+// max(a+, a-); returns a reference error code (F undefined then).
+template <int KIND, int DIR>
+__device__ __forceinline__ int face_tail(const DevPhys& P, const Metric& M, double ch, double* wl, double* wr,
+                                         double* w0, double* F, double& amax_local) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  amax_local = 0.0;
+  {
+    double v2;
+    if (wr[KPR] <= 0) wr[KPR] = w0[KPR];
+    v2 = 0;
+    v2 = v2 + wr[KVX] * wr[KVX] * M.g1;
+    v2 = v2 + wr[KVY] * wr[KVY] * M.g2;
+    v2 = v2 + wr[KVZ] * wr[KVZ] * M.g3;
+    if (v2 >= 1.) {
+      wr[KVX] = w0[KVX];
+      wr[KVY] = w0[KVY];
+      wr[KVZ] = w0[KVZ];
+      v2 = 0;
+      v2 = v2 + wr[KVX] * wr[KVX] * M.g1;
+      v2 = v2 + wr[KVY] * wr[KVY] * M.g2;
+      v2 = v2 + wr[KVZ] * wr[KVZ] * M.g3;
+      if (v2 >= 1) {
+#pragma unroll
+        for (int k = KVX; k <= KVZ; k++) {
+          w0[k] = w0[k] * P.maxspeed / (sqrt(v2));
+          wr[k] = w0[k];
+        }
+      }
+    }
+    if (wl[KPR] <= 0) wl[KPR] = w0[KPR];
+    v2 = 0;
+    v2 = v2 + wl[KVX] * wl[KVX] * M.g1;
+    v2 = v2 + wl[KVY] * wl[KVY] * M.g2;
+    v2 = v2 + wl[KVZ] * wl[KVZ] * M.g3;
+    if (v2 >= 1.) {
+      wl[KVX] = w0[KVX];
+      wl[KVY] = w0[KVY];
+      wl[KVZ] = w0[KVZ];
+      v2 = 0;
+      v2 = v2 + wl[KVX] * wl[KVX] * M.g1;
+      v2 = v2 + wl[KVY] * wl[KVY] * M.g2;
+      v2 = v2 + wl[KVZ] * wl[KVZ] * M.g3;
+      if (v2 >= 1) {
+#pragma unroll
+        for (int k = KVX; k <= KVZ; k++) {
+          w0[k] = w0[k] * P.maxspeed / (sqrt(v2));
+          wl[k] = w0[k];
+        }
+      }
+    }
+  }
+  if (T::GLM) {
+    const int kb = DIR == 0 ? KBX : DIR == 1 ? KBY : KBZ;
+    wl[T::KG] = 0.5 * (wl[T::KG] + wr[T::KG]) - (wr[kb] - wl[kb]) * ch / 2;
+    wr[T::KG] = wl[T::KG];
+    wl[kb] = 0.5 * (wl[kb] + wr[kb]) - (wr[T::KG] - wl[T::KG]) / (2 * ch);
+    wr[kb] = wl[kb];
+  }
+  double ul[NV], ur[NV], fl[NV], fr[NV];
+  double vflp, vflm, vfrp, vfrm;
+  int err = system_flux<KIND, DIR + 1>(P, M, wl, ul, fl, vflp, vflm);
+  if (!err) err = system_flux<KIND, DIR + 1>(P, M, wr, ur, fr, vfrp, vfrm);
+  if (err) return err;
+  double ap = 0., am = 0.;
+  if (vflp > ap) ap = vflp;
+  if (vfrp > ap) ap = vfrp;
+  if (-vflm > am) am = -vflm;
+  if (-vfrm > am) am = -vfrm;
+  amax_local = ap > am ? ap : am;
+  double a1 = (ap == 0.0 && am == 0.0) ? 1. : 1. / (ap + am);
+#pragma unroll
+  for (int k = 0; k < NV; k++) F[k] = a1 * (ap * fl[k] + am * fr[k] - ap * am * (ur[k] - ul[k]));
+  return 0;
+}
+
 // The flux through face `fid` (< faces_of<DIR>(A.g)): writes A.F (and A.WD)
 // and returns the face's signal speed max(a+, a-) for the CFL reduction.
 template <int KIND, int DIR, int REC>
@@ -298,82 +380,16 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
         A.WD[(size_t)(4 + c) * nfaces + fid] = r;
       }
     }
-    // fix-ups (evolve.f90:334-369); w0 = the cell left of the face
-    {
-      double v2;
-      if (wr[KPR] <= 0) wr[KPR] = w0[KPR];
-      v2 = 0;
-      v2 = v2 + wr[KVX] * wr[KVX] * M.g1;
-      v2 = v2 + wr[KVY] * wr[KVY] * M.g2;
-      v2 = v2 + wr[KVZ] * wr[KVZ] * M.g3;
-      if (v2 >= 1.) {
-        wr[KVX] = w0[KVX];
-        wr[KVY] = w0[KVY];
-        wr[KVZ] = w0[KVZ];
-        v2 = 0;
-        v2 = v2 + wr[KVX] * wr[KVX] * M.g1;
-        v2 = v2 + wr[KVY] * wr[KVY] * M.g2;
-        v2 = v2 + wr[KVZ] * wr[KVZ] * M.g3;
-        if (v2 >= 1) {
-#pragma unroll
-          for (int k = KVX; k <= KVZ; k++) {
-            w0[k] = w0[k] * A.P.maxspeed / (sqrt(v2));
-            wr[k] = w0[k];
-          }
-        }
-      }
-      if (wl[KPR] <= 0) wl[KPR] = w0[KPR];
-      v2 = 0;
-      v2 = v2 + wl[KVX] * wl[KVX] * M.g1;
-      v2 = v2 + wl[KVY] * wl[KVY] * M.g2;
-      v2 = v2 + wl[KVZ] * wl[KVZ] * M.g3;
-      if (v2 >= 1.) {
-        wl[KVX] = w0[KVX];
-        wl[KVY] = w0[KVY];
-        wl[KVZ] = w0[KVZ];
-        v2 = 0;
-        v2 = v2 + wl[KVX] * wl[KVX] * M.g1;
-        v2 = v2 + wl[KVY] * wl[KVY] * M.g2;
-        v2 = v2 + wl[KVZ] * wl[KVZ] * M.g3;
-        if (v2 >= 1) {
-#pragma unroll
-          for (int k = KVX; k <= KVZ; k++) {
-            w0[k] = w0[k] * A.P.maxspeed / (sqrt(v2));
-            wl[k] = w0[k];
-          }
-        }
-      }
-    }
-    // GLM upwinding (work_glm[xyz], work.f90:67-139)
-    if (T::GLM) {
-      const int kb = DIR == 0 ? KBX : DIR == 1 ? KBY : KBZ;
-      double ch = A.sc->glm_ch_old;
-      wl[T::KG] = 0.5 * (wl[T::KG] + wr[T::KG]) - (wr[kb] - wl[kb]) * ch / 2;
-      wr[T::KG] = wl[T::KG];
-      wl[kb] = 0.5 * (wl[kb] + wr[kb]) - (wr[T::KG] - wl[T::KG]) / (2 * ch);
-      wr[kb] = wl[kb];
-    }
-    // HLL (work.f90:195-229)
-    double ul[NV], ur[NV], fl[NV], fr[NV];
-    double vflp, vflm, vfrp, vfrm;
-    int err = system_flux<KIND, DIR + 1>(A.P, M, wl, ul, fl, vflp, vflm);
-    if (!err) err = system_flux<KIND, DIR + 1>(A.P, M, wr, ur, fr, vfrp, vfrm);
+    double fl_out[NV];
+    int err = face_tail<KIND, DIR>(A.P, M, A.sc->glm_ch_old, wl, wr, w0, fl_out, amax_local);
     if (err) {
       size_t cell = base + (size_t)((i >= 1 ? i : 1) - 1) * stride;
       atomicMin(&A.sc->err_key, ((unsigned long long)cell << 20) | (unsigned long long)err);
 #pragma unroll
       for (int k = 0; k < NV; k++) A.F[(size_t)k * nfaces + fid] = 0.0;
     } else {
-      double ap = 0., am = 0.;
-      if (vflp > ap) ap = vflp;
-      if (vfrp > ap) ap = vfrp;
-      if (-vflm > am) am = -vflm;
-      if (-vfrm > am) am = -vfrm;
-      amax_local = ap > am ? ap : am;
-      double a1 = (ap == 0.0 && am == 0.0) ? 1. : 1. / (ap + am);
 #pragma unroll
-      for (int k = 0; k < NV; k++)
-        A.F[(size_t)k * nfaces + fid] = a1 * (ap * fl[k] + am * fr[k] - ap * am * (ur[k] - ul[k]));
+      for (int k = 0; k < NV; k++) A.F[(size_t)k * nfaces + fid] = fl_out[k];
       // GLM speed of the reference: the last face of the last pencil (work.f90:217,310,401)
       int na = DIR == 0 ? g.ny : g.nx;
       int nb = DIR == 2 ? g.ny : g.nz;
@@ -419,18 +435,30 @@ struct ScalarArgs {
   double cfl, maxdt, glm_alpha;
   int irk, nrk, divclean;
   int mode;  // 0: explicit RK stage (after the sweeps); 1: IMEX-SSP dt (before the
-             // sweeps of stage 1, from the previous stage's speeds); 2: IMEX-SSP GLM
+             // sweeps of stage 1, from the previous stage's speeds); 2: IMEX-SSP GLM;
+             // 3, 4: the fused stage kernel's halves of mode 0 -- 3 before it
+             // (glm_ch, dt, GLM damping: none of them depends on this stage's
+             // faces when the host fuses the stage), 4 after it (glm_ch_old)
 };
 
 __device__ __forceinline__ void stage_scalars(const ScalarArgs& A) {
   DevScalars* sc = A.sc;
-  if (A.mode != 1) {
-    // glm_ch = glm_ch_old (start of stage); glm_ch_old = maxval(aflux) (end of sweeps)
-    sc->glm_ch = sc->glm_ch_old;
+  if (A.mode == 4) {
     double m = sc->aflux[0];
     if (sc->aflux[1] > m) m = sc->aflux[1];
     if (sc->aflux[2] > m) m = sc->aflux[2];
     sc->glm_ch_old = m;
+    return;
+  }
+  if (A.mode != 1) {
+    // glm_ch = glm_ch_old (start of stage); glm_ch_old = maxval(aflux) (end of sweeps)
+    sc->glm_ch = sc->glm_ch_old;
+    if (A.mode != 3) {
+      double m = sc->aflux[0];
+      if (sc->aflux[1] > m) m = sc->aflux[1];
+      if (sc->aflux[2] > m) m = sc->aflux[2];
+      sc->glm_ch_old = m;
+    }
   }
   if (A.irk == 1 && A.mode != 2) {
     double amax;
@@ -581,67 +609,27 @@ __device__ __forceinline__ void mlp_seed(const MlpDev& net, const Metric& M, boo
 // The update of cell c (flux divergence, sources, RK combination,
 // con2prim).  Called by every thread of a warp together (the learned seed
 // and the counters are warp-collective); threads without a cell pass
-// active = false.
+// active = false.  update_finish takes the flux divergence du[NV] (summed
+// in the reference's order: du = 0; += x; += y; += z) and, for viscous
+// runs, the spatial derivatives of u^mu in dv[NDER] (the rest zero); it
+// adds the lagged time derivatives, the sources, and does the RK
+// combination or writes du (MODE_RHS), then con2prim.  update_cell reads
+// the face fluxes of the three sweep kernels; the fused stage kernel
+// computes them itself (stage.cuh).
 template <int KIND, bool SEED, bool IMEX = false>
-__device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool active) {
+__device__ __forceinline__ void update_finish(const UpdateArgs& A, size_t c, bool active, int ix, int iy, int iz,
+                                              double* du, double* dv) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const Grid& g = A.g;
-  unsigned long long my_iters = 0, my_fallbacks = 0;
+  unsigned long long my_iters = 0, my_fallbacks = 0, my_brackets = 0;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
   double vv[NV], uu[NV];
   if (active) {
-    int ix = (int)(c % g.nx);
-    size_t r = c / g.nx;
-    int iy = (int)(r % g.ny);
-    int iz = (int)(r / g.ny);
-    const size_t nfx = (size_t)(g.nx + 1) * g.ny * g.nz;
-    const size_t nfy = (size_t)g.nx * (g.ny + 1) * g.nz;
-    const size_t nfz = (size_t)g.nx * g.ny * (g.nz + 1);
-    const size_t fx = ((size_t)iz * g.ny + iy) * (g.nx + 1) + ix;       // face ix-1/2 -> index ix
-    const size_t fy = ((size_t)iz * (g.ny + 1) + iy) * g.nx + ix;
-    const size_t fz = ((size_t)iz * g.ny + iy) * g.nx + ix;
-    double src[NV], du[NV], kap[2] = {0., 0.};
+    double src[NV], kap[2] = {0., 0.};
 #pragma unroll
     for (int k = 0; k < NV; k++) vv[k] = A.vin[(size_t)k * g.ncell + c];
-    // flux divergence in the reference's order: du = 0; += x; += y; += z
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-      double d = 0.;
-      if (g.nx > 1) d = d + g.ddx * (A.Fx[(size_t)k * nfx + fx + 1] - A.Fx[(size_t)k * nfx + fx]);
-      if (g.ny > 1) d = d + g.ddy * (A.Fy[(size_t)k * nfy + fy + g.nx] - A.Fy[(size_t)k * nfy + fy]);
-      if (g.nz > 1)
-        d = d + g.ddz * (A.Fz[(size_t)k * nfz + fz + (size_t)g.nx * g.ny] - A.Fz[(size_t)k * nfz + fz]);
-      du[k] = d;
-    }
-    // sources (evolve_src, evolve.f90:689-718)
-    double dv[NDER];
     if (T::VISC) {
-#pragma unroll
-      for (int q = 0; q < NDER; q++) dv[q] = 0.;
-      const int dk[3][4] = {{DTX, DXX, DYX, DZX}, {DTY, DXY, DYY, DZY}, {DTZ, DXZ, DYZ, DZZ}};
-      if (g.nx > 1) {
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          dv[dk[0][q]] = g.ddx * 0.5 *
-                         (A.WDx[(size_t)q * nfx + fx + 1] + A.WDx[(size_t)(4 + q) * nfx + fx + 1] -
-                          A.WDx[(size_t)q * nfx + fx] - A.WDx[(size_t)(4 + q) * nfx + fx]);
-      }
-      if (g.ny > 1) {
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          dv[dk[1][q]] = g.ddy * 0.5 *
-                         (A.WDy[(size_t)q * nfy + fy + g.nx] + A.WDy[(size_t)(4 + q) * nfy + fy + g.nx] -
-                          A.WDy[(size_t)q * nfy + fy] - A.WDy[(size_t)(4 + q) * nfy + fy]);
-      }
-      if (g.nz > 1) {
-        size_t s = (size_t)g.nx * g.ny;
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          dv[dk[2][q]] = g.ddz * 0.5 *
-                         (A.WDz[(size_t)q * nfz + fz + s] + A.WDz[(size_t)(4 + q) * nfz + fz + s] -
-                          A.WDz[(size_t)q * nfz + fz] - A.WDz[(size_t)(4 + q) * nfz + fz]);
-      }
       if (A.vsnap) {
 #pragma unroll
         for (int k = 0; k < 4; k++) A.vsnap[(size_t)k * g.ncell + c] = vv[k];
@@ -749,7 +737,8 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
       int it = 0, sfail = 0;
       int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail);
       my_iters = (unsigned long long)it;
-      my_fallbacks = (unsigned long long)sfail;
+      my_fallbacks = (unsigned long long)(sfail & 1);
+      my_brackets = (unsigned long long)(sfail >> 1);
       if (err) {
         A.fail[c] = 1;
         atomicAdd(&A.sc->nfail, 1);
@@ -759,15 +748,77 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
         for (int k = 0; k < NV; k++) A.vout[(size_t)k * g.ncell + c] = vv[k];
       }
     }
-    // per-warp sums of iteration counts and seed fallbacks
+    // per-warp sums of iteration counts, seed and bracketed fallbacks
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       my_iters += __shfl_xor_sync(0xffffffffu, my_iters, o);
       my_fallbacks += __shfl_xor_sync(0xffffffffu, my_fallbacks, o);
+      my_brackets += __shfl_xor_sync(0xffffffffu, my_brackets, o);
     }
     if ((threadIdx.x & 31) == 0 && my_iters) atomicAdd(&A.sc->c2p_iters, my_iters);
     if ((threadIdx.x & 31) == 0 && my_fallbacks) atomicAdd(&A.sc->fallbacks, my_fallbacks);
+    if ((threadIdx.x & 31) == 0 && my_brackets) atomicAdd(&A.sc->brackets, my_brackets);
   }
+}
+
+
+template <int KIND, bool SEED, bool IMEX = false>
+__device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool active) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  const Grid& g = A.g;
+  int ix = 0, iy = 0, iz = 0;
+  double du[NV], dv[NDER];
+  if (active) {
+    ix = (int)(c % g.nx);
+    size_t r = c / g.nx;
+    iy = (int)(r % g.ny);
+    iz = (int)(r / g.ny);
+    const size_t nfx = (size_t)(g.nx + 1) * g.ny * g.nz;
+    const size_t nfy = (size_t)g.nx * (g.ny + 1) * g.nz;
+    const size_t nfz = (size_t)g.nx * g.ny * (g.nz + 1);
+    const size_t fx = ((size_t)iz * g.ny + iy) * (g.nx + 1) + ix;       // face ix-1/2 -> index ix
+    const size_t fy = ((size_t)iz * (g.ny + 1) + iy) * g.nx + ix;
+    const size_t fz = ((size_t)iz * g.ny + iy) * g.nx + ix;
+    // flux divergence in the reference's order: du = 0; += x; += y; += z
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double d = 0.;
+      if (g.nx > 1) d = d + g.ddx * (A.Fx[(size_t)k * nfx + fx + 1] - A.Fx[(size_t)k * nfx + fx]);
+      if (g.ny > 1) d = d + g.ddy * (A.Fy[(size_t)k * nfy + fy + g.nx] - A.Fy[(size_t)k * nfy + fy]);
+      if (g.nz > 1)
+        d = d + g.ddz * (A.Fz[(size_t)k * nfz + fz + (size_t)g.nx * g.ny] - A.Fz[(size_t)k * nfz + fz]);
+      du[k] = d;
+    }
+    if (T::VISC) {
+#pragma unroll
+      for (int q = 0; q < NDER; q++) dv[q] = 0.;
+      const int dk[3][4] = {{DTX, DXX, DYX, DZX}, {DTY, DXY, DYY, DZY}, {DTZ, DXZ, DYZ, DZZ}};
+      if (g.nx > 1) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dv[dk[0][q]] = g.ddx * 0.5 *
+                         (A.WDx[(size_t)q * nfx + fx + 1] + A.WDx[(size_t)(4 + q) * nfx + fx + 1] -
+                          A.WDx[(size_t)q * nfx + fx] - A.WDx[(size_t)(4 + q) * nfx + fx]);
+      }
+      if (g.ny > 1) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dv[dk[1][q]] = g.ddy * 0.5 *
+                         (A.WDy[(size_t)q * nfy + fy + g.nx] + A.WDy[(size_t)(4 + q) * nfy + fy + g.nx] -
+                          A.WDy[(size_t)q * nfy + fy] - A.WDy[(size_t)(4 + q) * nfy + fy]);
+      }
+      if (g.nz > 1) {
+        size_t s = (size_t)g.nx * g.ny;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          dv[dk[2][q]] = g.ddz * 0.5 *
+                         (A.WDz[(size_t)q * nfz + fz + s] + A.WDz[(size_t)(4 + q) * nfz + fz + s] -
+                          A.WDz[(size_t)q * nfz + fz] - A.WDz[(size_t)(4 + q) * nfz + fz]);
+      }
+    }
+  }
+  update_finish<KIND, SEED, IMEX>(A, c, active, ix, iy, iz, du, dv);
 }
 
 template <int KIND, bool SEED, bool IMEX = false>
@@ -862,7 +913,7 @@ __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_combine_kernel(SspArgs
     const double h = (T::RES && A.stage < 5) ? alpha_imex * dt : 0.;
     int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail, h);
     my_iters = (unsigned long long)it;
-    my_fallbacks = (unsigned long long)sfail;
+    my_fallbacks = (unsigned long long)(sfail & 1);
     if (err) {
       A.fail[c] = 1;
       atomicAdd(&A.sc->nfail, 1);
@@ -917,7 +968,7 @@ __global__ void __launch_bounds__(128, ECHO_SSP_MINB) ssp_stage1_kernel(SspArgs 
   if (!active) return;
   int it = 0, sfail = 0;
   int err = cons2prim<KIND>(A.P, M, A.algo, A.tol, uu, vv, &it, sp, &sfail, alpha_imex * A.sc->dt);
-  if (SEED && sfail) atomicAdd(&A.sc->fallbacks, 1ull);
+  if (SEED && (sfail & 1)) atomicAdd(&A.sc->fallbacks, 1ull);
   if (err) {
     atomicMin(&A.sc->err_key, ((unsigned long long)c << 20) | (unsigned long long)err);
     return;

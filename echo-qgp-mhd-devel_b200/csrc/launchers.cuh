@@ -3,6 +3,7 @@
 #pragma once
 
 #include "batch.cuh"
+#include "stage.cuh"
 
 namespace echo {
 
@@ -93,6 +94,168 @@ void launch_update(EchoCtx* c, int irk, int mode, double* du_out) {
   if (Traits<KIND>::MHD && !Traits<KIND>::RES && mode == MODE_RK && c2p_alt_algo(A.algo))
     c2p_alt_kernel<KIND><<<blocks, 128, 0, c->stream>>>(c->P, c->g, c->p.coordinates, A.algo, A.tol, c->d_sc, A.uout,
                                                          A.vin, A.vout, c->d_fail);
+}
+
+// The fused stage kernel (stage.cuh): the UpdateArgs of launch_update with
+// no face arrays, plus the tile decomposition chosen by setup_stage.
+template <int KIND>
+static UpdateArgs update_args(EchoCtx* c, int irk, int mode, double* du_out) {
+  static const double crk[3][3][2] = {{{0., 1.}, {0., 0.}, {0., 0.}},
+                                      {{0., 1.}, {1. / 2., 1. / 2.}, {0., 0.}},
+                                      {{0., 1.}, {3. / 4., 1. / 4.}, {1. / 3., 2. / 3.}}};
+  UpdateArgs A;
+  memset(&A, 0, sizeof(A));
+  A.P = c->P;
+  A.g = c->g;
+  A.vin = c->d_v[c->vcur];
+  A.vout = c->d_v[1 - c->vcur];
+  A.uin = c->d_u[c->ucur];
+  A.uout = irk == 1 ? c->d_u[1 - c->ucur] : c->d_u[c->ucur];
+  A.u0 = irk == 1 ? c->d_u[c->ucur] : c->d_u[1 - c->ucur];
+  A.vnew = c->d_vh[c->vn];
+  A.vold = c->d_vh[1 - c->vn];
+  A.du_out = du_out;
+  A.fail = c->d_fail;
+  A.sc = c->d_sc;
+  int nrk = c->p.nrk;
+  A.c1 = nrk <= 3 ? crk[nrk - 1][irk - 1][0] : 0.;
+  A.c2 = nrk <= 3 ? crk[nrk - 1][irk - 1][1] : 0.;
+  A.irk = irk;
+  A.nrk = nrk;
+  A.divclean = c->p.divclean;
+  A.coordinates = c->p.coordinates;
+  A.algo = c->p.algo_solver;
+  A.mode = mode;
+  A.tol = c->p.c2p_tol;
+  A.dus_out = nullptr;
+  if (Traits<KIND>::RES) {
+    if (mode == MODE_RHS) A.dus_out = c->d_dss[irk - 1];
+    const int ke[3] = {KEX, KEY, KEZ};
+    for (int d = 0; d < 3; d++)
+      for (int q = 0; q < 2; q++) A.ebc[d][q] = c->bc[d].c[ke[d]][q];
+  }
+  A.mlp.frag = c->d_mlp_frag;
+  A.mlp.par = c->d_mlp_par;
+  A.vsnap = nullptr;
+  if (A.algo == ECHO_C2P_MLP && !c->d_mlp_frag) A.algo = ECHO_C2P_NEWTON;  // no network loaded
+  return A;
+}
+
+// the instantiation of stage_kernel a run uses
+template <int KIND>
+static void* stage_variant(int algo_mlp, int imex) {
+  constexpr bool CAN_SEED = Traits<KIND>::MHD || Traits<KIND>::VISC;
+  constexpr bool VISC = Traits<KIND>::VISC;
+  if (CAN_SEED && algo_mlp && VISC && imex) return (void*)stage_kernel<KIND, CAN_SEED, VISC>;
+  if (CAN_SEED && algo_mlp) return (void*)stage_kernel<KIND, CAN_SEED, false>;
+  if (VISC && imex) return (void*)stage_kernel<KIND, false, VISC>;
+  return (void*)stage_kernel<KIND, false, false>;
+}
+
+// Tile, segment and grid of the fused stage for this run: the tile whose
+// faces and cells fill a CTA in one pass each and that needs the fewest
+// tiles (ties: the fewest CTA threads), then the eta segment length that
+// minimises waves x (planes + the extra lower eta face of a segment).
+// tx, ty, zseg > 0 force a choice.  Returns 0 and leaves st_ok = 0 when the
+// run cannot use the fused stage (the sweep kernels then run).
+template <int KIND>
+int setup_stage(EchoCtx* c, int tx, int ty, int zseg) {
+  typedef Traits<KIND> T;
+  const int nw = T::VISC ? 8 : 0;
+  c->st_ok = 0;
+  const Grid& g = c->g;
+  if (c->p.recal != ECHO_REC_WENO5 || g.nx < 3 || g.ny < 3) return 0;
+  if (T::MHD && !T::RES && c2p_alt_algo(c->p.algo_solver)) return 0;
+  const bool three_d = g.nz > 1;
+  int dev = 0, nsm = 148;
+  size_t smem_optin = 0;
+  {
+    int v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    smem_optin = (size_t)v;
+  }
+  auto threads_of = [](int a, int b) {
+    int m = (a + 1) * b;
+    if (a * (b + 1) > m) m = a * (b + 1);
+    return (m + 31) / 32 * 32;
+  };
+  if (tx <= 0 || ty <= 0) {
+    long long best = -1;
+    int bt = 1 << 30;
+    for (int a = 6; a <= 32; a++)
+      for (int b = 6; b <= 32; b++) {
+        int nt = threads_of(a, b);
+        if (nt > ECHO_STAGE_NT) continue;
+        if (8 * stage_smem_doubles(T::NV, nw, a, b, three_d) > smem_optin / 2) continue;
+        long long tiles = (long long)((g.nx + a - 1) / a) * ((g.ny + b - 1) / b);
+        if (best < 0 || tiles < best || (tiles == best && nt < bt)) {
+          best = tiles;
+          bt = nt;
+          tx = a;
+          ty = b;
+        }
+      }
+    if (best < 0) return 0;
+  }
+  const int nt = threads_of(tx, ty);
+  if (nt > ECHO_STAGE_NT || tx * ty > nt) return 0;
+  const size_t smem = 8 * stage_smem_doubles(T::NV, nw, tx, ty, three_d);
+  if (smem > smem_optin) return 0;
+  int occ = 1 << 30;
+  for (int mlp = 0; mlp < 2; mlp++)
+    for (int im = 0; im < 2; im++) {
+      void* fn = stage_variant<KIND>(mlp, im);
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+      int o = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, nt, smem) != cudaSuccess) return 0;
+      occ = o < occ ? o : occ;
+    }
+  if (occ < 1) return 0;
+  const long long tiles = (long long)((g.nx + tx - 1) / tx) * ((g.ny + ty - 1) / ty);
+  const long long slots = (long long)occ * nsm;
+  if (zseg <= 0) {
+    double best = 1e300;
+    zseg = g.nz;
+    for (int s = 1; s <= g.nz; s++) {
+      int zl = (g.nz + s - 1) / s;
+      int nseg = (g.nz + zl - 1) / zl;
+      long long waves = (tiles * nseg + slots - 1) / slots;
+      double cost = (double)waves * (zl + (three_d ? 0.34 : 0.0));
+      if (cost < best - 1e-9) {
+        best = cost;
+        zseg = zl;
+      }
+    }
+  }
+  if (zseg > g.nz) zseg = g.nz;
+  const long long nunits = tiles * ((g.nz + zseg - 1) / zseg);
+  c->st_tx = tx;
+  c->st_ty = ty;
+  c->st_zseg = zseg;
+  c->st_nt = nt;
+  c->st_smem = smem;
+  c->st_grid = (unsigned)(nunits < slots ? nunits : slots);
+  c->st_ok = 1;
+  return 1;
+}
+
+template <int KIND>
+void launch_stage(EchoCtx* c, int irk, int mode, double* du_out) {
+  StageArgs S;
+  memset(&S, 0, sizeof(S));
+  S.U = update_args<KIND>(c, irk, mode, du_out);
+  for (int d = 0; d < 3; d++) S.bc[d] = c->bc[d];
+  S.tx = c->st_tx;
+  S.ty = c->st_ty;
+  S.ntx = (c->g.nx + S.tx - 1) / S.tx;
+  S.nty = (c->g.ny + S.ty - 1) / S.ty;
+  S.zseg = c->st_zseg;
+  S.nunits = (long long)S.ntx * S.nty * ((c->g.nz + S.zseg - 1) / S.zseg);
+  void* fn = stage_variant<KIND>(S.U.algo == ECHO_C2P_MLP && mode == MODE_RK, c->p.imex && mode == MODE_RK);
+  void* args[] = {&S};
+  cudaLaunchKernel(fn, dim3(c->st_grid), dim3(c->st_nt), args, c->st_smem, c->stream);
 }
 
 template <int KIND>
@@ -356,6 +519,8 @@ void batch_occupancy(const EchoBatch* b, int* per_sm) {
 
 #define ECHO_INSTANTIATE_GRID(K)                                              \
   template void echo::launch_faces<K>(EchoCtx*, int);                         \
+  template int echo::setup_stage<K>(EchoCtx*, int, int, int);                 \
+  template void echo::launch_stage<K>(EchoCtx*, int, int, double*);           \
   template void echo::launch_update<K>(EchoCtx*, int, int, double*);          \
   template void echo::launch_repair_smooth<K>(EchoCtx*, int);                 \
   template void echo::launch_p2c<K>(EchoCtx*);                                \

@@ -51,10 +51,19 @@ static __global__ void noalloc_reset_scalars(DevScalars* sc, double t, double t3
 extern "C" int echo_gpu_rhs_noalloc(const EchoParams* p, const double* d_eos_cols, int n_eos, double t,
                                     const double* d_v, double* d_du, void* stream, int* errcode) {
   if (!p || !d_v || !d_du) return ECHO_ERR_ARG;
-  if (p->mhd > 1 || (p->mhd && p->viscosity)) return ECHO_ERR_UNSUPPORTED;
-  if (p->nx < 1 || p->ny < 1 || p->nz < 1) return ECHO_ERR_ARG;
-  if ((p->nx > 1 && p->nx < 3) || (p->ny > 1 && p->ny < 3) || (p->nz > 1 && p->nz < 3)) return ECHO_ERR_ARG;
-  if (p->eqstate == ECHO_EOS_TABLE && (!d_eos_cols || n_eos < 2)) return ECHO_ERR_ARG;
+  {
+    // the checks echo_gpu_init makes (equation set, integrator, grid, table)
+    int r = echo_check_params(p, d_eos_cols, n_eos);
+    if (r) return r;
+  }
+  if (p->mhd == 2) return ECHO_ERR_UNSUPPORTED;  // resistive runs: stage right-hand sides need the SSP state
+  if (errcode) {
+    // reading the error code back synchronises the stream, which a stream
+    // being captured into a graph does not allow
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing((cudaStream_t)stream, &cs) != cudaSuccess) return ECHO_ERR_CUDA;
+    if (cs != cudaStreamCaptureStatusNone) return ECHO_ERR_ARG;
+  }
   int kind = p->viscosity ? KIND_VISC : p->mhd ? (p->divclean ? KIND_MHDGLM : KIND_MHD) : KIND_HD;
   int nv = kind == KIND_VISC ? 12 : kind == KIND_MHD ? 8 : kind == KIND_MHDGLM ? 9 : 5;
   size_t nf[3] = {(size_t)(p->nx + 1) * p->ny * p->nz, (size_t)p->nx * (p->ny + 1) * p->nz,

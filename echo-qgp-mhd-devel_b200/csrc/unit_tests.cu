@@ -280,3 +280,64 @@ extern "C" int echo_gpu_test_c2p_seeded(const EchoParams* p, const double* eos_t
   cudaFree(dpar);
   return ECHO_OK;
 }
+
+// ---------------------------------------------------------------------------
+// FP64 peak of this GPU: the roofline the step kernels' FP64 work is
+// measured against.  Every thread runs 8 independent multiply-add chains
+// (x = x * a + b, a fixed point at 1, so no value leaves the normal range)
+// for `iters` rounds; one round is 8 DFMA = 16 FLOP per thread.
+// ---------------------------------------------------------------------------
+namespace echo {
+__global__ void __launch_bounds__(256) fp64_peak_kernel(int iters, double a, double b, double* out) {
+  double x0 = 1.0 + threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;
+  double x4 = x0 + 4e-9, x5 = x0 + 5e-9, x6 = x0 + 6e-9, x7 = x0 + 7e-9;
+#pragma unroll 4
+  for (int i = 0; i < iters; i++) {
+    x0 = fma(x0, a, b);
+    x1 = fma(x1, a, b);
+    x2 = fma(x2, a, b);
+    x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b);
+    x5 = fma(x5, a, b);
+    x6 = fma(x6, a, b);
+    x7 = fma(x7, a, b);
+  }
+  double s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == 12345.0) out[0] = s;  // never true: keeps the chains live
+}
+}  // namespace echo
+
+extern "C" int echo_gpu_fp64_peak(double* gflops, double* ms) {
+  if (!gflops) return ECHO_ERR_ARG;
+  int dev = 0, nsm = 0, per_sm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, echo::fp64_peak_kernel, 256, 0));
+  if (per_sm < 1) per_sm = 1;
+  const int iters = 1 << 11;
+  const unsigned blocks = (unsigned)(nsm * per_sm);
+  double* d_out = nullptr;
+  CK(cudaMalloc(&d_out, sizeof(double)));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  echo::fp64_peak_kernel<<<blocks, 256>>>(iters, 0.999999, 1e-6, d_out);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; r++) {
+    CK(cudaEventRecord(e0));
+    echo::fp64_peak_kernel<<<blocks, 256>>>(iters, 0.999999, 1e-6, d_out);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    if (t < best) best = t;
+  }
+  CK(cudaGetLastError());
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_out);
+  double flop = 16.0 * (double)iters * (double)blocks * 256.0;
+  *gflops = flop / (best * 1e-3) / 1e9;
+  if (ms) *ms = best;
+  return ECHO_OK;
+}

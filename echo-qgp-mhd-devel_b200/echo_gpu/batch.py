@@ -18,7 +18,8 @@ from .params import EchoParams
 
 LIVE, DONE, CRASHED, COOLED = 0, 1, 2, 3
 SLOTS = ("faces_x", "faces_y", "faces_z", "update", "smooth")
-KERNEL_CLASSES = ("faces_x", "faces_y", "faces_z", "scalars", "update_c2p", "repair_smooth", "end_step")
+KERNEL_CLASSES = ("faces_x", "faces_y", "faces_z", "scalars", "update_c2p", "repair_smooth", "end_step",
+                  "stage_fused")
 
 
 def event_grid(nx: int, ny: int, nz: int, x1: float, x2: float, y1: float, y2: float,

@@ -32,6 +32,7 @@ class EchoStats(ctypes.Structure):
         ("c2p_iters", ctypes.c_longlong), ("c2p_cells", ctypes.c_longlong),
         ("repairs", ctypes.c_longlong), ("seed_fallbacks", ctypes.c_longlong),
         ("errcode", ctypes.c_int), ("err_cell", ctypes.c_int),
+        ("bracket_fallbacks", ctypes.c_longlong),
     ]
 
 
@@ -69,6 +70,7 @@ FUNCTIONS = {
     "echo_gpu_stream": (ctypes.c_int, [P, ctypes.POINTER(P)]),
     "echo_gpu_put_state": (ctypes.c_int, [P, P, P]),
     "echo_gpu_rhs_noalloc": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double, P, P, P, I]),
+    "echo_gpu_fp64_peak": (ctypes.c_int, [D, D]),
     "echo_gpu_mlp_train": (ctypes.c_int, [F, F, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                           ctypes.c_uint, F, F, F, ctypes.c_int]),
     "echo_gpu_mlp_grad": (ctypes.c_int, [F, F, F, ctypes.c_int, F, F]),
@@ -78,6 +80,7 @@ FUNCTIONS = {
                                                 F, F, D, D, I, I, I]),
     "echo_gpu_get_state": (ctypes.c_int, [P, P, P]),
     "echo_gpu_profile_step": (ctypes.c_int, [P, D, I]),
+    "echo_gpu_set_stage": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, I]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
@@ -246,13 +249,22 @@ class Evolve:
         self._check(self.lib.echo_gpu_stream(self.h, ctypes.byref(s)), "stream")
         return s.value or 0
 
-    KERNEL_CLASSES = ("faces_x", "faces_y", "faces_z", "stage_scalars", "update_c2p", "repair", "end_step")
+    KERNEL_CLASSES = ("faces_x", "faces_y", "faces_z", "stage_scalars", "update_c2p", "repair", "end_step",
+                      "stage_fused")
 
     def profile_step(self):
-        ms = np.zeros(7)
-        n = np.zeros(7, dtype=np.int32)
+        ms = np.zeros(len(self.KERNEL_CLASSES))
+        n = np.zeros(len(self.KERNEL_CLASSES), dtype=np.int32)
         self._check(self.lib.echo_gpu_profile_step(self.h, _dp(ms), _ip(n)), "profile_step")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def set_stage(self, fused: bool = True, tx: int = 0, ty: int = 0, zseg: int = 0) -> dict:
+        """Fused stage kernel on or off (and its tile); returns the choice."""
+        info = np.zeros(7, dtype=np.int32)
+        rc = self.lib.echo_gpu_set_stage(self.h, int(fused), tx, ty, zseg, _ip(info))
+        if rc not in (0, -3) or (rc == -3 and fused):
+            raise RuntimeError(f"set_stage failed with status {rc}")
+        return dict(zip(("fused", "tx", "ty", "zseg", "threads", "ctas", "smem_bytes"), info.tolist()))
 
     def hyp_init(self, freeze_type: int, freeze_value: float) -> None:
         """Freeze-out hypersurface on T (0) or e (1) = freeze_value."""
@@ -358,3 +370,14 @@ def unit_c2p_seeded(params, eos_table, g3, gp, u, vguess, weights=None, norm=Non
     if rc:
         raise RuntimeError(f"test_c2p_seeded status {rc}")
     return v, err, it, sf
+
+
+def fp64_peak() -> tuple[float, float]:
+    """Measured FP64 GFLOP/s of the current GPU and the timed launch's ms."""
+    L = load(False)
+    g = ctypes.c_double(0)
+    ms = ctypes.c_double(0)
+    rc = L.echo_gpu_fp64_peak(ctypes.byref(g), ctypes.byref(ms))
+    if rc:
+        raise RuntimeError(f"fp64_peak status {rc}")
+    return g.value, ms.value

@@ -1,7 +1,8 @@
 ! evolve_gpu.f90 -- ISO_C_BINDING interface of libechogpu.so for the
 ! ECHO-QGP Fortran host.  With -DECHO_GPU the bodies of evolve_main,
-! evolve_alloc and the state hand-over around output call these bindings
-! (see INTEGRATION.md for the exact edits of evolve.f90 and echo.f90).
+! evolve_alloc and the state hand-over around output call these bindings;
+! the per-step work of echo.f90 around them (check_temp, out_vars, out_hyp,
+! out_dump/out_restart) has device counterparts bound below as well.
 !
 ! All arrays are passed as they are: v(ix1:ix2,iy1:iy2,iz1:iz2,nv) and u(...)
 ! are column-major with x fastest and the variable index slowest, the layout
@@ -72,6 +73,82 @@ module evolve_gpu
     integer(c_int) function echo_gpu_free(ctx) bind(C, name="echo_gpu_free")
       import :: c_int, c_ptr
       type(c_ptr), value :: ctx
+    end function
+
+    ! check_temp (out.f90:1487-1557) on the device: max_value = the grid
+    ! maximum of T (freeze_type 0) or e (1); stop = 1 when it is below temp_end
+    integer(c_int) function echo_gpu_check_temp(ctx, freeze_type, temp_end, max_value, stop_flag) &
+        bind(C, name="echo_gpu_check_temp")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: freeze_type
+      real(c_double), value :: temp_end
+      real(c_double), intent(out) :: max_value
+      integer(c_int), intent(out) :: stop_flag
+    end function
+
+    ! out_vars (out.f90:232-591): the bytes of one outNNNN.dat (t, then the
+    ! selected fields), precision 8 or 4; sel is a mask of ECHO_OUT_* bits
+    integer(c_int) function echo_gpu_out_vars_size(ctx, sel, precision, nbytes) &
+        bind(C, name="echo_gpu_out_vars_size")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: sel          ! C unsigned: the low 27 bits are used
+      integer(c_int), value :: precision
+      integer(c_size_t), intent(out) :: nbytes
+    end function
+
+    integer(c_int) function echo_gpu_out_vars(ctx, sel, precision, buf, nbytes, errcode) &
+        bind(C, name="echo_gpu_out_vars")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: sel
+      integer(c_int), value :: precision
+      type(c_ptr), value :: buf             ! c_loc of an integer(1) buffer of nbytes
+      integer(c_size_t), value :: nbytes
+      integer(c_int), intent(out) :: errcode
+    end function
+
+    ! out_hyp (out.f90:1569-1650): hyp_init once, hyp_step at every
+    ! hypersurface time, hyp_get for the n_elements rows of 8 + nv doubles
+    integer(c_int) function echo_gpu_hyp_init(ctx, freeze_type, freeze_value) bind(C, name="echo_gpu_hyp_init")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: freeze_type
+      real(c_double), value :: freeze_value
+    end function
+
+    integer(c_int) function echo_gpu_hyp_step(ctx, n_elements, errcode) bind(C, name="echo_gpu_hyp_step")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), intent(out) :: n_elements
+      integer(c_int), intent(out) :: errcode
+    end function
+
+    integer(c_int) function echo_gpu_hyp_get(ctx, elements) bind(C, name="echo_gpu_hyp_get")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: elements(*)   ! (8 + nv) * n_elements
+    end function
+
+    ! out_dump / out_restart (out.f90:1313-1483): the run state at a step
+    ! boundary as one blob of checkpoint_size bytes
+    integer(c_int) function echo_gpu_checkpoint_size(ctx, nbytes) bind(C, name="echo_gpu_checkpoint_size")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx
+      integer(c_size_t), intent(out) :: nbytes
+    end function
+
+    integer(c_int) function echo_gpu_checkpoint(ctx, blob) bind(C, name="echo_gpu_checkpoint")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: blob            ! c_loc of an integer(1) buffer
+    end function
+
+    integer(c_int) function echo_gpu_restart(ctx, blob) bind(C, name="echo_gpu_restart")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: blob
     end function
 
     ! learned con2prim seed (ALG_SOLV = 101): weights(ECHO_MLP_NWEIGHTS) and

@@ -128,9 +128,10 @@ typedef struct EchoStats {
   long long c2p_iters;  /* sum of con2prim iterations over cells, last stage */
   long long c2p_cells;  /* cells inverted in the last stage */
   long long repairs;    /* cells that went through the neighbour-average repair */
-  long long seed_fallbacks; /* MLP seeds that needed the bracketed fallback */
+  long long seed_fallbacks; /* learned seeds that missed (the warm-start solve took over), so far */
   int errcode;          /* first reference error code, 0 if none */
   int err_cell;         /* linear Fortran index of the first failing cell */
+  long long bracket_fallbacks; /* Newton solves that fell back to the bracketed BRENTM, so far */
 } EchoStats;
 
 /* ---- context ----------------------------------------------------------- */
@@ -268,16 +269,40 @@ int echo_gpu_hyp_step(EchoCtx* ctx, int* n_elements, int* errcode);
 int echo_gpu_hyp_get(EchoCtx* ctx, double* out);
 
 /* Runs one full step with a CUDA event after every launch group and returns
- * the device time per kernel class (ms[7]: faces x, faces y, faces z, stage
- * scalars, update+con2prim, repair(+smoothing), end of step) and the number
- * of launches of each class.  The step is a real step of the run. */
+ * the device time per kernel class (ms[8]: faces x, faces y, faces z, stage
+ * scalars, update+con2prim, repair(+smoothing), end of step, fused stage)
+ * and the number of launches of each class.  The step is a real step of the
+ * run. */
 int echo_gpu_profile_step(EchoCtx* ctx, double* ms, int* launches);
+
+/* No counterpart in the reference (an execution option).  How a stage runs:
+ * fused = 1 (the default wherever the run allows it) runs the three sweeps,
+ * the flux divergence, the sources, the update and con2prim of a stage in
+ * one kernel over x-y tiles of tx x ty cells marching through eta segments
+ * of zseg planes, with no face flux in global memory; fused = 0 runs the
+ * sweep kernels and the update kernel.  The first stage of an explicit RK
+ * step without divergence cleaning always runs the sweeps (its dt needs
+ * every face's signal speed before any update).  tx, ty, zseg = 0 choose
+ * the tile and segment for this grid.  Both give the same results within
+ * the parity tolerance.  info (may be NULL) receives 7 ints: fused, tx, ty,
+ * zseg, threads per CTA, CTAs, shared-memory bytes per CTA.  Returns
+ * ECHO_ERR_UNSUPPORTED (and runs the sweeps) where the run cannot fuse:
+ * reconstruction other than WENO5, nx or ny below 3, ALG_SOLV 2-6.
+ * Synchronises the stream and drops the cached step graphs. */
+int echo_gpu_set_stage(EchoCtx* ctx, int fused, int tx, int ty, int zseg, int* info);
 
 /* ---- pieces of the step, for parity tests against the oracle ----------- */
 
 /* evolve_dfx/dfy/dfz + evolve_src of one stage (evolve.f90:302-718) into
  * du (nx*ny*nz*nv, Fortran order, host memory), with ax/ay/az maxima. */
 int echo_gpu_rhs(EchoCtx* ctx, double* du, double* amax3);
+
+/* No counterpart in the reference (measurement).  The FP64 peak of the
+ * current GPU: independent DFMA chains on every SM, best of five timed
+ * launches; *gflops = FP64 GFLOP/s (a DFMA counts 2), *ms = that launch's
+ * time.  The denominator of the FP64 roofline the step kernels report.
+ * Allocates 8 bytes and synchronises the device. */
+int echo_gpu_fp64_peak(double* gflops, double* ms);
 
 /* Reconstruction of m pencils of length n (+ghosts) with REC_ALGO.
  * f is m rows of (n + 8) values, f[row*(n+8) + (i+4)] = f(i), i=-4..n+3;
@@ -339,8 +364,9 @@ int echo_gpu_mlp_infer(const float* weights, const float* norm, const float* X,
 /* ---- allocation-free stage right-hand side ------------------------------ */
 
 /* No counterpart in the reference.  The du of one explicit stage -- what
- * echo_gpu_rhs returns: the three flux sweeps plus the sources, at time t,
- * from primitives d_v -- for callers that cannot allocate device memory:
+ * echo_gpu_rhs returns right after echo_gpu_upload of d_v at time t: the
+ * three flux sweeps plus the sources -- for callers that cannot allocate
+ * device memory:
  * a code coupled to this library inside a GPU application whose memory
  * belongs to another allocator (a framework pool, or a solver that reserves
  * HBM up front), or a driver that must not allocate between graph captures.
@@ -358,9 +384,20 @@ int echo_gpu_mlp_infer(const float* weights, const float* norm, const float* X,
  * device current; make that first call before any stream capture.  All
  * calls share the array, which keeps the last call's contents, so calls
  * that overlap on the GPU (other streams, other host threads) race.
+ *
+ * The call carries no run state: like a context just uploaded, it takes the
+ * GLM wave speed of the face upwinding as 0.5 (common.f90:283) and the
+ * viscous lagged time derivatives (dts) as zero (timeinterval = 0).  In the
+ * middle of a divergence-cleaning or viscous run its du therefore differs
+ * from echo_gpu_rhs on the running context; it equals echo_gpu_rhs on a
+ * context that uploads the same primitives at the same t.  Resistive runs
+ * (mhd = 2) return ECHO_ERR_UNSUPPORTED; every parameter check of
+ * echo_gpu_init applies.
  * Launches go to `stream` (a cudaStream_t, may be NULL).  If errcode is not
  * NULL the call synchronises the stream and returns the first reference
- * error code found (0 = none). */
+ * error code found (0 = none); a stream being captured cannot be
+ * synchronised, so with errcode set on a capturing stream the call returns
+ * ECHO_ERR_ARG before any launch: pass errcode = NULL there. */
 #define ECHO_NOALLOC_SCRATCH_DOUBLES (4 * 1024 * 1024)
 int echo_gpu_rhs_noalloc(const EchoParams* p, const double* d_eos_cols,
                          int n_eos, double t, const double* d_v, double* d_du,

@@ -58,7 +58,8 @@ def test_struct_layouts_match_the_header(tmp_path):
 
     if not shutil.which("gcc"):
         pytest.skip("no C compiler")
-    structs = {"EchoParams": EchoParams, "EchoEventGrid": LB.EchoEventGrid, "EchoEventStatus": LB.EchoEventStatus}
+    structs = {"EchoParams": EchoParams, "EchoEventGrid": LB.EchoEventGrid, "EchoEventStatus": LB.EchoEventStatus,
+               "EchoStats": LB.EchoStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
