@@ -56,6 +56,9 @@ def main():
     ap.add_argument("--events", type=int, default=64, help="events of the batched workload")
     ap.add_argument("--pairs", type=int, default=100_000, help="training pairs for --c2p mlp")
     ap.add_argument("--train-steps", type=int, default=500)
+    ap.add_argument("--stage", default="auto", choices=["auto", "fused", "sweeps"],
+                    help="fused stage kernel or the sweep kernels (auto: the library's default)")
+    ap.add_argument("--tile", default="", help="fused stage tile tx,ty,zseg (0 = chosen for the grid)")
     a = ap.parse_args()
     if a.config == "batch":
         run_batch(a)
@@ -80,6 +83,10 @@ def main():
         X, T = S.generate_pairs(n_target=a.pairs, resistive=cfg.mhd == 2, viscous=bool(cfg.viscosity))
         w, norm, _ = S.train(X, T, steps=a.train_steps)
         ev.set_seed_network(w, norm)
+    if a.stage != "auto" or a.tile:
+        tx, ty, zs = (int(x) for x in a.tile.split(",")) if a.tile else (0, 0, 0)
+        info = ev.set_stage(a.stage != "sweeps", tx, ty, zs)
+        print(f"stage: {info}")
     ev.upload(I.primitives(cfg, tab), None, cfg.tstart)
     t0 = time.perf_counter()
     ev.run(a.steps)
