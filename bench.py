@@ -9,7 +9,10 @@ time step of the grid (three RK stages, con2prim included).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 value:   cell-updates/s with the state resident in HBM (the library's CUDA
-         graph per step), timed with CUDA events on the library's stream.
+         graph per step), timed with CUDA events on the library's stream,
+         for the faster of the con2prim paths (Newton from the previous
+         stage's primitives); the BRENTM and MLP-seeded variants are timed
+         beside it in `variants`.
 e2e:     the same metric through the C-ABI with host buffers: every step
          copies v and u from page-locked host memory to the device, runs one
          step and copies v back.
@@ -38,6 +41,16 @@ import numpy as np  # noqa: E402
 METRIC = "cell-updates/s on 1 B200: MLP-seeded vs plain con2prim at equal 1e-10 residual"
 UNIT = "cell-updates/s"
 B_ALG_STEP = 1008  # algorithmic HBM bytes per cell-update of a stage-fused RK3 step, nv = 9
+
+
+COUNTERS = os.path.join(ROOT, "profiles", "roofline_counters_rmhd_97x97x81.json")
+
+
+def config_of(cfg) -> dict:
+    """The `config` object of both arms (the headline workload)."""
+    return {"workload": cfg.name, "grid": [cfg.nx, cfg.ny, cfg.nz], "nv": cfg.nv,
+            "scheme": "WENO5+HLL+GLM, RK3, tabulated EoS (2048 pts)",
+            "l2": "working set per step (2x v, 2x u, 3 face-flux arrays ~ 440 MB) exceeds the 126 MB L2"}
 
 
 def peaks() -> dict:
@@ -128,14 +141,17 @@ def cpu_rate(cfg, tab, przero, threads: int, target_s: float, steps: int | None 
         return cfg.replace(nz=nz, z1=z1, z2=z2)
 
     state = state or (lambda c: I.primitives(c, tab))
-    probe = slab(6)
-    o = O.Oracle(probe.to_c(przero=przero), tab, threads=threads)
-    o.set_state(state(probe), None, probe.tstart)
-    t0 = time.perf_counter()
-    o.step()
-    rate = probe.ncell / (time.perf_counter() - t0)
-    nz = int(max(6, min(cfg.nz, round(target_s * rate / (cfg.nx * cfg.ny)))))
-    c = slab(nz)
+    if cfg.nz == 1:
+        c = cfg  # a 2+1D grid: the whole grid
+    else:
+        probe = slab(6)
+        o = O.Oracle(probe.to_c(przero=przero), tab, threads=threads)
+        o.set_state(state(probe), None, probe.tstart)
+        t0 = time.perf_counter()
+        o.step()
+        rate = probe.ncell / (time.perf_counter() - t0)
+        nz = int(max(6, min(cfg.nz, round(target_s * rate / (cfg.nx * cfg.ny)))))
+        c = slab(nz)
     o = O.Oracle(c.to_c(przero=przero), tab, threads=threads)
     o.set_state(state(c), None, c.tstart)
     for _ in range(warmup):
@@ -145,7 +161,8 @@ def cpu_rate(cfg, tab, przero, threads: int, target_s: float, steps: int | None 
     for _ in range(n):
         o.step()
     el = time.perf_counter() - t0
-    sample = (f"{n} full steps of a {c.nx}x{c.ny}x{c.nz} slab of the workload "
+    what = "the whole grid" if c.nz == cfg.nz else "a slab"
+    sample = (f"{n} full steps of {what} ({c.nx}x{c.ny}x{c.nz}) of the workload "
               f"(same spacing, EoS, scheme), after {warmup} untimed steps")
     return c.ncell * n / el, el, sample
 
@@ -156,7 +173,6 @@ def run_reference(args):
         return
     cfg, tab, przero = workload()
     threads = os.cpu_count() or 1
-    cfg_name = cfg.name
     # each step is one time step of a slab sized to ~1 s of work on all cores
     rate, el, sample = cpu_rate(cfg, tab, przero, threads, target_s=1.0, steps=args.steps,
                                 warmup=args.warmup)
@@ -166,8 +182,8 @@ def run_reference(args):
         "ms_per_step": 1e3 * el / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (optical-Glauber Au+Au b=7 fm x Gaussian eta profile, B_y ~ exp(-x^2/2/2.5^2))",
-        "config": {"workload": cfg_name + " (slab sample)", "grid": [cfg.nx, cfg.ny, cfg.nz], "nv": cfg.nv,
-                   "scheme": "WENO5+HLL+GLM, RK3, BRENTM con2prim, tabulated EoS"},
+        "config": dict(config_of(cfg), con2prim="BRENTM (the reference's ALG_SOLV=1)",
+                       build="oracle/liboracle_echo.so (gcc -O2, OpenMP over pencils and cells)"),
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -192,6 +208,50 @@ def algorithmic_bytes(kclass: str, cfg) -> float:
 
 
 B_ALG_RES = 1896  # bytes per cell-update of a stage-fused IMEX-SSP3(4,3,3) resistive step, nv = 12
+
+
+def run_ideal_hd(args, torch, barrier, world, rank):
+    """The 2+1D ideal-hydro workload: p = e/3, 101x101 (dx = 0.2 fm),
+    optical-Glauber Au+Au at b = 7 fm, WENO5 + HLL, RK2 at CFL 0.4, its 100
+    steps from tau = 0.4 fm/c (10 k cells: the step is launch-bound and runs
+    as captured step graphs), beside the CPU restatement on one core."""
+    from echo_gpu import params as P
+    from echo_gpu.lib import Evolve
+    from echo_gpu import initial as I
+
+    cfg = P.config0()
+    przero = cfg.enezero / 3.0
+    v0 = I.primitives(cfg, None)
+    ev = Evolve(cfg.to_c(przero=przero), None, exact=False)
+    ev.upload(v0, None, cfg.tstart)
+    stream = torch.cuda.ExternalStream(ev.stream_handle())
+    ev.run(max(args.warmup, 3))
+    ev.sync()
+    ev.upload(v0, None, cfg.tstart)
+    ev.run(1)  # the step graphs exist; time the workload's own 100 steps from tau0
+    ev.upload(v0, None, cfg.tstart)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ev.run(cfg.steps)
+    e1.record(stream)
+    ev.sync()
+    barrier()
+    ms = float(e0.elapsed_time(e1))
+    st = ev.stats()
+    prof = ev.profile_step()
+    ev.close()
+    out = {"workload": cfg.name, "grid": [cfg.nx, cfg.ny], "nv": cfg.nv, "scheme": "WENO5+HLL, RK2, p = e/3",
+           "value": cfg.ncell * cfg.steps * world / (ms / 1e3), "unit": UNIT, "steps": cfg.steps,
+           "ms_per_step": ms / cfg.steps, "t_end": st.t, "errcode": int(st.errcode),
+           "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items() if v[1]}}
+    if world == 1 and rank == 0:
+        rate, el, sample = cpu_rate(cfg, None, przero, threads=1, target_s=2.0, steps=20,
+                                    state=lambda c: I.primitives(c, None))
+        out["cpu_oracle"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample}
+    return out
 
 
 def run_resistive(args, torch, barrier, world, rank):
@@ -266,14 +326,15 @@ def run_resistive(args, torch, barrier, world, rank):
                               "peak_src": pk["src"] + " (hbm_gbs)"},
             "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()},
             "c2p_iters_per_cell_last_stage": st.c2p_iters / max(cfg.ncell, 1),
-            "seed_fallbacks_total": int(st.seed_fallbacks),
+            "seed_fallbacks_total": int(st.seed_fallbacks), "bracket_fallbacks_total": int(st.bracket_fallbacks),
             "errcode": int(st.errcode), "repairs": int(st.repairs)}
     out = {
         "workload": cfg.name, "grid": [cfg.nx, cfg.ny, cfg.nz], "nv": cfg.nv,
         "scheme": "WENO5+HLL (light-cone speeds)+GLM, IMEX-SSP3(4,3,3), implicit Ohm's law, tabulated EoS",
         "sigma_el": cfg.sigma_el, "sigma_chiral": cfg.sigma_chiral,
-        "value": variants["mlp_seeded"]["value"], "unit": UNIT, "steps": steps,
-        "ms_per_step": variants["mlp_seeded"]["ms_per_step"],
+        "value": variants["plain"]["value"], "unit": UNIT, "steps": steps,
+        "ms_per_step": variants["plain"]["ms_per_step"],
+        "value_variant": "plain (faster than mlp_seeded)",
         "variants": variants, "seed_training": training,
         "c2p_iters": "Newton steps per cell summed over the fixed point's passes: the stage-4 solve and the "
                      "final combination",
@@ -353,11 +414,13 @@ def run_viscous(args, torch, barrier, world, rank, X1, T1):
             "value": cfg.ncell * steps * world / (ms / 1e3), "ms_per_step": ms / steps,
             "kernels_ms_per_step": {k: round(v[0], 4) for k, v in prof.items()},
             "c2p_iters_per_cell_last_stage": st.c2p_iters / max(cfg.ncell, 1),
-            "seed_fallbacks_total": int(st.seed_fallbacks), "errcode": int(st.errcode)}
+            "seed_fallbacks_total": int(st.seed_fallbacks), "bracket_fallbacks_total": int(st.bracket_fallbacks),
+            "errcode": int(st.errcode)}
     return {
         "workload": cfg.name, "grid": [cfg.nx, cfg.ny], "nv": cfg.nv, "scheme": "WENO5+HLL, IMEX RK2",
-        "value": variants["mlp_seeded"]["value"], "unit": UNIT, "steps": steps,
-        "ms_per_step": variants["mlp_seeded"]["ms_per_step"], "variants": variants, "seed_training": training,
+        "value": variants["plain"]["value"], "unit": UNIT, "steps": steps,
+        "ms_per_step": variants["plain"]["ms_per_step"], "value_variant": "plain (faster than mlp_seeded)",
+        "variants": variants, "seed_training": training,
         "c2p_iters": "Newton steps per cell summed over the nested iteration's passes, last stage",
     }, (Xv, Tv)
 
@@ -479,12 +542,12 @@ def run_batched(args, torch, barrier, world, rank, net=None):
     if rank != 0:
         return None
     plain = cu / (ms / 1e3)
-    value = seeded["value"] if seeded else plain
+    value = plain
     states = np.bincount([s["state"] for s in st], minlength=4)
     return {
         "workload": f"{full.nev} MC-Glauber Pb+Pb events (b in [0,12] fm), viscous 2+1D IS, grids "
                     f"{int(full.n.min())}^2..{int(full.n.max())}^2 at dx={full.dx}, tau {full.cfg.tstart} -> "
-                    f"{full.tmax} fm/c, CFL dt per event, RK2, WENO5+HLL, crossover EoS to 1e-7 GeV/fm^3, "
+                    f"{full.tmax} fm/c, CFL dt per event, IMEX RK2, WENO5+HLL, crossover EoS to 1e-7 GeV/fm^3, "
                     f"ENEZERO {full.cfg.enezero}",
         "cells": int(full.cells.sum()),
         "value": value, "unit": UNIT, "ms": ms, "batched_steps": nsteps,
@@ -583,15 +646,17 @@ def run_b200(args):
         it = st.c2p_iters / max(cfg0.ncell, 1)
         variants[names[algo]] = {
             "value": cfg0.ncell * args.steps * world / (ms / 1e3), "ms_per_step": ms / args.steps,
-            "c2p_iters_per_cell_last_stage": it if algo == P.C2P_BRENT else (it % 1000),
-            "seed_fallbacks_total": int(st.seed_fallbacks), "errcode": int(st.errcode)}
-        if algo == P.C2P_MLP:
+            "c2p_iters_per_cell_last_stage": it,
+            "c2p_iters": "BRENTM function evaluations" if algo == P.C2P_BRENT else "Newton steps",
+            "seed_fallbacks_total": int(st.seed_fallbacks), "bracket_fallbacks_total": int(st.bracket_fallbacks),
+            "errcode": int(st.errcode)}
+        if algo == P.C2P_NEWTON:
             keep = (ev, stream, ms, st)
         else:
             ev.close()
     clocks = clk.stop()
     ev, stream, ms_max, st = keep
-    value = variants["mlp_seeded"]["value"]
+    value = variants["plain_newton"]["value"]
     prof = ev.profile_step()  # one real step, per-kernel device times
     ev.sync()
 
@@ -622,6 +687,7 @@ def run_b200(args):
     viscous, vnet = run_viscous(args, torch, barrier, world, rank, Xp, Tp) if args.viscous else (None, None)
     batched = run_batched(args, torch, barrier, world, rank, vnet) if args.batched else None
     resistive = run_resistive(args, torch, barrier, world, rank) if args.resistive else None
+    ideal_hd = run_ideal_hd(args, torch, barrier, world, rank) if args.ideal_hd else None
 
     if world > 1:
         dist.barrier()
@@ -630,24 +696,29 @@ def run_b200(args):
             dist.destroy_process_group()
         return
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel: HBM (its own compulsory bytes, and the
+    # stage-fused B_alg of one stage) and FP64 (ncu FLOPs over the measured
+    # FP64 peak of this GPU)
     pk = peaks()
     dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
     dom_ms, dom_n = prof[dom]
     per_launch_s = dom_ms / dom_n / 1e3
     alg = algorithmic_bytes(dom, cfg0)
     achieved = alg / per_launch_s / 1e9
-    traffic, pipes = None, None
-    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                rec = json.load(f).get(dom)
-            if isinstance(rec, dict):
-                traffic = rec.get("dram_bytes")
-                pipes = {k: rec[k] for k in ("fp64_pipe_pct", "tensor_pipe_pct") if k in rec}
-        except Exception:
-            traffic = None
+    stage_bytes = B_ALG_STEP / cfg0.nrk * cfg0.ncell  # one RK3 stage of a stage-fused implementation
+    from echo_gpu import counters as CT
+    from echo_gpu.lib import fp64_peak
+
+    fp64_gflops, _ = fp64_peak()
+    cnt, fresh = (CT.load(COUNTERS) if os.path.exists(COUNTERS) else ({}, False))
+    krec = cnt.get("kernels", {})
+    traffic = krec.get(dom, {}).get("dram_bytes")
+    flop_dom = krec.get(dom, {}).get("fp64_flop")
+    flop_step = None
+    if all(k in krec for k, (_, n) in prof.items() if n and k in ("faces_x", "faces_y", "faces_z", "update_c2p")):
+        flop_step = sum(krec[k]["fp64_flop"] * n for k, (_, n) in prof.items() if k in krec and n)
+    counters_src = {"file": os.path.relpath(COUNTERS, ROOT), "build_hash": cnt.get("build_hash"),
+                    "this_build": CT.build_hash(), "same_build": fresh}
     launches_per_step = sum(n for (_, n) in prof.values())
 
     cpu = None
@@ -660,20 +731,32 @@ def run_b200(args):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (optical-Glauber Au+Au b=7 fm x Gaussian eta profile, B_y ~ exp(-x^2/2/2.5^2))",
-        "config": {
-            "workload": cfg0.name, "grid": [cfg0.nx, cfg0.ny, cfg0.nz], "nv": cfg0.nv,
-            "scheme": "WENO5+HLL+GLM, RK3, tabulated EoS (2048 pts)",
-            "con2prim": "MLP-seeded Newton (4x64 tanh, BF16 tensor-core inference), residual 1e-10",
-            "build": "libechogpu.so (--fmad=true)",
-            "l2": "working set per step (2x v, 2x u, 3 face-flux arrays ~ 440 MB) exceeds the 126 MB L2",
-            "parallelism": f"replicas x{world}",
-        },
+        "config": dict(config_of(cfg0),
+                       con2prim="Newton from the previous stage's primitives, residual 1e-10 (BRENTM fallback)",
+                       build="libechogpu.so (--fmad=true)", parallelism=f"replicas x{world}"),
         "variants": variants,
         "training": training,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg, "launch_ms": dom_ms / dom_n,
-                     "peak_src": pk["src"] + " (hbm_gbs)", "ncu_pipes": pipes},
+                     "algorithmic_bytes_per_launch": alg,
+                     "algorithmic_bytes": "the kernel's own compulsory bytes: read v once, write its face fluxes "
+                                          "(faces), or read 3 face arrays, v, u, u0 and write u, v (update)",
+                     "launch_ms": dom_ms / dom_n, "peak_src": pk["src"] + " (hbm_gbs)",
+                     "traffic_src": counters_src,
+                     "stage_b_alg": {"bytes_per_stage": stage_bytes,
+                                     "note": "336 B per cell per RK3 stage of a stage-fused implementation (nv = 9)",
+                                     "achieved_gbs_over_dominant_launch": stage_bytes / per_launch_s / 1e9,
+                                     "frac": stage_bytes / per_launch_s / 1e9 / pk["hbm_gbs"]}},
+        "fp64_roofline": {"bound": "fp64", "kernel": dom, "peak_gflops": fp64_gflops,
+                          "peak_src": "measured on this GPU by echo_gpu_fp64_peak (independent DFMA chains)",
+                          "flop_per_launch": flop_dom,
+                          "achieved_gflops": (flop_dom / per_launch_s / 1e9) if flop_dom else None,
+                          "frac": (flop_dom / per_launch_s / 1e9 / fp64_gflops) if flop_dom else None,
+                          "step_flop_per_cell_update": (flop_step / cfg0.ncell) if flop_step else None,
+                          "step_achieved_gflops": (flop_step / cfg0.ncell * value / world / 1e9) if flop_step else None,
+                          "step_frac": (flop_step / cfg0.ncell * value / world / 1e9 / fp64_gflops) if flop_step
+                          else None,
+                          "flop_src": counters_src},
         "step_roofline": {"bytes_per_cell_update": B_ALG_STEP,
                           "achieved_gbs": value / world * B_ALG_STEP / 1e9,
                           "frac": value / world * B_ALG_STEP / 1e9 / pk["hbm_gbs"]},
@@ -684,6 +767,7 @@ def run_b200(args):
         "viscous": viscous,
         "batched": batched,
         "resistive": resistive,
+        "ideal_hd": ideal_hd,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clocks,
         "stats": {"errcode": st.errcode, "repairs": st.repairs, "t": st2.t, "dt": st.dt},
@@ -705,6 +789,7 @@ def main():
     ap.add_argument("--batched", type=int, default=1, help="also run the batched event-by-event workload")
     ap.add_argument("--resistive", type=int, default=1, help="also run the resistive RMHD workload")
     ap.add_argument("--viscous", type=int, default=1, help="also run the 2+1D viscous workload")
+    ap.add_argument("--ideal-hd", type=int, default=1, help="also run the 2+1D ideal-hydro workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

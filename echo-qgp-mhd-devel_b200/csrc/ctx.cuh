@@ -42,14 +42,20 @@ struct EchoCtx {
   unsigned char* d_fail;
   DevScalars* d_sc;
   DevScalars* h_sc;         // pinned mirror
-  cudaGraphExec_t graph[8];  // one per buffer-role key at step start
-  bool graph_ok[8];
+  cudaGraphExec_t graph[16];  // one per buffer-role key at step start
+  bool graph_ok[16];
   // per-kernel timing (echo_gpu_profile_step): events recorded after each launch group
   std::vector<std::pair<int, cudaEvent_t>>* marks;
   EchoHyp* hyp;             // set up by echo_gpu_hyp_init
   void* d_out;              // output staging (echo_gpu_out_vars), grown on demand
   size_t out_bytes;
   unsigned long long* d_out_err;
+  // the reference's vnewstep/unewstep -> vold/uold of components
+  // krh..kvold_end (echo.f90:192-202, 240-241), kept only for dump.dat
+  // (echo_gpu_keep_old): d_oldv[on] / d_oldu[on] = the step-start copies,
+  // [1 - on] = vold / uold
+  int keep_old, kold, on;
+  double *d_oldv[2], *d_oldu[2];
   // the fused stage kernel (stage.cuh): usable, on, tile, segment, launch
   int st_ok, st_on, st_tx, st_ty, st_zseg, st_nt;
   unsigned st_grid;

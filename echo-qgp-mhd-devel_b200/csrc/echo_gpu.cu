@@ -4,6 +4,7 @@
 // captured into a CUDA graph (echo_gpu_run).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -280,13 +281,19 @@ static void snapshot_vnewstep(EchoCtx* c) {
   if (c->p.viscosity)
     cudaMemcpyAsync(c->d_vh[c->vn], c->d_v[c->vcur], sizeof(double) * c->g.ncell * 4, cudaMemcpyDeviceToDevice,
                     c->stream);
+  if (c->keep_old) {  // the full vnewstep / unewstep of the reference, for dump.dat
+    size_t b = sizeof(double) * c->g.ncell * c->kold;
+    cudaMemcpyAsync(c->d_oldv[c->on], c->d_v[c->vcur], b, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(c->d_oldu[c->on], c->d_u[c->ucur], b, cudaMemcpyDeviceToDevice, c->stream);
+  }
 }
 
-// end of step: vold = vnewstep (echo.f90:240) is a role swap
+// end of step: vold = vnewstep, uold = unewstep (echo.f90:240-241) are role swaps
 static void end_step(EchoCtx* c) {
   end_step_kernel<<<1, 1, 0, c->stream>>>(c->d_sc, c->p.coordinates);
   mark(c, PK_END);
   if (c->p.viscosity) c->vn = 1 - c->vn;
+  if (c->keep_old) c->on = 1 - c->on;
 }
 
 static void enqueue_step(EchoCtx* c) {
@@ -300,6 +307,7 @@ static void advance_roles(EchoCtx* c) {
   c->ucur = 1 - c->ucur;
   c->vcur = c->vcur ^ (c->p.nrk & 1);
   if (c->p.viscosity) c->vn = 1 - c->vn;
+  if (c->keep_old) c->on = 1 - c->on;
 }
 
 // The parameter checks of a run, shared by every entry point that takes an
@@ -398,6 +406,7 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->d_out = nullptr;
   c->out_bytes = 0;
   c->d_out_err = nullptr;
+  c->kold = p->mhd ? 8 : 5;  // krh..kvold_end: kbz with MHD, kpr without (common.f90:378-386)
   // the fused stage kernel, when the run allows it (else the sweep kernels)
   DISPATCH(c, setup_stage, c, 0, 0, 0);
   c->st_on = 0;
@@ -409,7 +418,7 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
 int echo_gpu_free(EchoCtx* c) {
   if (!c) return ECHO_OK;
   cudaStreamSynchronize(c->stream);
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < 16; i++)
     if (c->graph_ok[i]) cudaGraphExecDestroy(c->graph[i]);
   for (int i = 0; i < 2; i++) {
     cudaFree(c->d_v[i]);
@@ -431,6 +440,10 @@ int echo_gpu_free(EchoCtx* c) {
   cudaFree(c->d_du);
   cudaFree(c->d_mlp_frag);
   cudaFree(c->d_mlp_par);
+  for (int i = 0; i < 2; i++) {
+    cudaFree(c->d_oldv[i]);
+    cudaFree(c->d_oldu[i]);
+  }
   cudaFreeHost(c->h_sc);
   echo_hyp_free(c->hyp);
   echo_out_free(c);
@@ -460,6 +473,15 @@ static int reset_scalars(EchoCtx* c, double t) {
   return ECHO_OK;
 }
 
+// vold = v, uold = u of the uploaded state (init.f90:3271-3272)
+static int init_old(EchoCtx* c) {
+  if (!c->keep_old) return ECHO_OK;
+  size_t b = sizeof(double) * c->g.ncell * c->kold;
+  CK(cudaMemcpyAsync(c->d_oldv[1 - c->on], c->d_v[c->vcur], b, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_oldu[1 - c->on], c->d_u[c->ucur], b, cudaMemcpyDeviceToDevice, c->stream));
+  return ECHO_OK;
+}
+
 static int upload_impl(EchoCtx* c, const double* v, const double* u, double t, cudaMemcpyKind kind) {
   (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
   if (!c || !v) return ECHO_ERR_ARG;
@@ -467,6 +489,7 @@ static int upload_impl(EchoCtx* c, const double* v, const double* u, double t, c
   c->vcur = 0;
   c->ucur = 0;
   c->vn = 0;
+  c->on = 0;
   int r = reset_scalars(c, t);
   if (r) return r;
   CK(cudaMemcpyAsync(c->d_v[0], v, bytes, kind, c->stream));
@@ -475,6 +498,8 @@ static int upload_impl(EchoCtx* c, const double* v, const double* u, double t, c
   } else {
     DISPATCH(c, launch_p2c, c);
   }
+  r = init_old(c);
+  if (r) return r;
   CK(cudaStreamSynchronize(c->stream));
   CK(cudaGetLastError());
   return ECHO_OK;
@@ -580,7 +605,7 @@ int echo_gpu_run(EchoCtx* c, int nsteps) {
   for (int s = 0; s < nsteps; s++) {
     // buffer roles at step start: which u/v buffer is current and which
     // vnewstep/vold buffer is which; they repeat, so graphs are cached per key
-    int key = c->ucur | (c->vcur << 1) | (c->vn << 2);
+    int key = c->ucur | (c->vcur << 1) | (c->vn << 2) | (c->on << 3);
     if (!c->graph_ok[key]) {
       cudaGraph_t gr;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -676,7 +701,7 @@ int echo_gpu_restart(EchoCtx* c, const void* blob) {
   }
   size_t nvc = (size_t)c->nv * c->g.ncell;
   const char* p = (const char*)blob + sizeof(h);
-  c->vcur = c->ucur = c->vn = 0;
+  c->vcur = c->ucur = c->vn = c->on = 0;
   CK(cudaMemcpyAsync(c->d_sc, &h.sc, sizeof(DevScalars), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_v[0], p, sizeof(double) * nvc, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_u[0], p + sizeof(double) * nvc, sizeof(double) * nvc, cudaMemcpyHostToDevice,
@@ -684,6 +709,137 @@ int echo_gpu_restart(EchoCtx* c, const void* blob) {
   CK(cudaMemcpyAsync(c->d_vh[1], p + sizeof(double) * 2 * nvc, sizeof(double) * 4 * c->g.ncell,
                      cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return ECHO_OK;
+}
+
+// dump.dat (out_dump / out_restart, out.f90:1313-1483, restart_type /= 0,
+// out_freeze off): stream-access records, no markers -- iout (int32), t,
+// timeold, timeinterval, vall (nv fields), uall (nv), vallold and uallold
+// (krh..kvold_end), g_cov_3_old.
+static size_t dump_bytes(const EchoCtx* c) {
+  return 4 + 3 * sizeof(double) + sizeof(double) * c->g.ncell * (2 * (size_t)c->nv + 2 * (size_t)c->kold) +
+         sizeof(double);
+}
+
+int echo_gpu_keep_old(EchoCtx* c, int on) {
+  if (!c || (on != 0 && on != 1)) return ECHO_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  if (on && !c->keep_old) {
+    size_t b = sizeof(double) * c->g.ncell * c->kold;
+    for (int i = 0; i < 2; i++) {
+      if (!c->d_oldv[i]) CK(cudaMalloc(&c->d_oldv[i], b));
+      if (!c->d_oldu[i]) CK(cudaMalloc(&c->d_oldu[i], b));
+    }
+    c->keep_old = 1;
+    c->on = 0;
+    int r = init_old(c);  // from the current state, as init() leaves them
+    if (r) return r;
+  } else if (!on) {
+    c->keep_old = 0;
+  }
+  for (int i = 0; i < 16; i++)
+    if (c->graph_ok[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph_ok[i] = false;
+    }
+  CK(cudaStreamSynchronize(c->stream));
+  return ECHO_OK;
+}
+
+int echo_gpu_dump_size(const EchoCtx* c, size_t* bytes) {
+  if (!c || !bytes) return ECHO_ERR_ARG;
+  *bytes = dump_bytes(c);
+  return ECHO_OK;
+}
+
+int echo_gpu_dump(EchoCtx* c, int iout, void* buf, size_t bytes) {
+  (void)cudaGetLastError();
+  if (!c || !buf || bytes != dump_bytes(c)) return ECHO_ERR_ARG;
+  const size_t nc = c->g.ncell, nvc = (size_t)c->nv * nc, nold = (size_t)c->kold * nc;
+  DevScalars s;
+  CK(cudaMemcpyAsync(&s, c->d_sc, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
+  char* p = (char*)buf;
+  const int32_t io = iout;
+  memcpy(p, &io, 4);
+  p += 4;
+  double* vall = (double*)malloc(sizeof(double) * (2 * nvc + 2 * nold));
+  if (!vall) return ECHO_ERR_ARG;
+  double* uall = vall + nvc;
+  double* vold = uall + nvc;
+  double* uold = vold + nold;
+  memset(vold, 0, sizeof(double) * 2 * nold);
+  cudaError_t e = cudaMemcpyAsync(vall, c->d_v[c->vcur], sizeof(double) * nvc, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(uall, c->d_u[c->ucur], sizeof(double) * nvc, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && c->keep_old) {
+    e = cudaMemcpyAsync(vold, c->d_oldv[1 - c->on], sizeof(double) * nold, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(uold, c->d_oldu[1 - c->on], sizeof(double) * nold, cudaMemcpyDeviceToHost, c->stream);
+  } else if (e == cudaSuccess && c->p.viscosity) {
+    // without keep_old the device holds the viscous vold's rho and velocity
+    e = cudaMemcpyAsync(vold, c->d_vh[1 - c->vn], sizeof(double) * 4 * nc, cudaMemcpyDeviceToHost, c->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    free(vall);
+    fprintf(stderr, "echo_gpu: CUDA error %s in echo_gpu_dump\n", cudaGetErrorString(e));
+    return ECHO_ERR_CUDA;
+  }
+  const double hdr[3] = {s.t, s.timeold, s.timeinterval};
+  memcpy(p, hdr, sizeof(hdr));
+  p += sizeof(hdr);
+  memcpy(p, vall, sizeof(double) * (2 * nvc + 2 * nold));
+  p += sizeof(double) * (2 * nvc + 2 * nold);
+  memcpy(p, &s.g3old, sizeof(double));
+  free(vall);
+  return ECHO_OK;
+}
+
+int echo_gpu_restart_dump(EchoCtx* c, const void* buf, size_t bytes, int* iout) {
+  (void)cudaGetLastError();
+  if (!c || !buf || bytes != dump_bytes(c)) return ECHO_ERR_ARG;
+  const size_t nc = c->g.ncell, nvc = (size_t)c->nv * nc, nold = (size_t)c->kold * nc;
+  const char* p = (const char*)buf;
+  int32_t io;
+  memcpy(&io, p, 4);
+  p += 4;
+  double hdr[3];
+  memcpy(hdr, p, sizeof(hdr));
+  p += sizeof(hdr);
+  const char* arrays = p;
+  double g3old;
+  memcpy(&g3old, p + sizeof(double) * (2 * nvc + 2 * nold), sizeof(double));
+  // the host copy is not necessarily aligned for doubles (iout is 4 bytes)
+  double* tmp = (double*)malloc(sizeof(double) * (2 * nvc + 2 * nold));
+  if (!tmp) return ECHO_ERR_ARG;
+  memcpy(tmp, arrays, sizeof(double) * (2 * nvc + 2 * nold));
+  c->vcur = c->ucur = c->vn = c->on = 0;
+  int r = reset_scalars(c, hdr[0]);
+  if (r) {
+    free(tmp);
+    return r;
+  }
+  DevScalars s;
+  cudaError_t e = cudaMemcpy(&s, c->d_sc, sizeof(s), cudaMemcpyDeviceToHost);
+  s.timeold = hdr[1];
+  s.timeinterval = hdr[2];
+  s.g3old = g3old;
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_sc, &s, sizeof(s), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_v[0], tmp, sizeof(double) * nvc, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(c->d_u[0], tmp + nvc, sizeof(double) * nvc, cudaMemcpyHostToDevice);
+  // vold: the viscous time derivatives read its velocities (d_vh[1 - vn])
+  if (e == cudaSuccess && c->p.viscosity)
+    e = cudaMemcpy(c->d_vh[1], tmp + 2 * nvc, sizeof(double) * 4 * nc, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && c->keep_old) {
+    e = cudaMemcpy(c->d_oldv[1], tmp + 2 * nvc, sizeof(double) * nold, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->d_oldu[1], tmp + 2 * nvc + nold, sizeof(double) * nold, cudaMemcpyHostToDevice);
+  }
+  free(tmp);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "echo_gpu: CUDA error %s in echo_gpu_restart_dump\n", cudaGetErrorString(e));
+    return ECHO_ERR_CUDA;
+  }
+  if (iout) *iout = io;
   return ECHO_OK;
 }
 
@@ -737,7 +893,7 @@ int echo_gpu_set_stage(EchoCtx* c, int fused, int tx, int ty, int zseg, int* inf
   c->st_on = fused && c->st_ok;
   // the cached step graphs hold the other kernels
   CK(cudaStreamSynchronize(c->stream));
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < 16; i++)
     if (c->graph_ok[i]) {
       cudaGraphExecDestroy(c->graph[i]);
       c->graph_ok[i] = false;

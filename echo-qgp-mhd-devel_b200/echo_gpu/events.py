@@ -68,8 +68,10 @@ def batched_viscous(nev: int = 512, seed: int = 2024, dx: float = 0.15, nmin: in
     n = np.rint(nmax - (nmax - nmin) * b / bmax).astype(np.int64)
     base = P.config2()
     h = 0.5 * int(n[0]) * dx
+    # IMEX RK2, the viscous workload's scheme (the Israel-Stewart relaxation
+    # linearly implicit per stage)
     cfg = base.replace(name="batched-viscous-2d", nx=int(n[0]), ny=int(n[0]), x1=-h, x2=h, y1=-h, y2=h,
-                       maxdt=maxdt, enezero=enezero)
+                       maxdt=maxdt, enezero=enezero, imex=1)
     return EventSet(cfg=cfg, b=b, n=n, dx=dx, tmax=tmax)
 
 

@@ -90,6 +90,10 @@ FUNCTIONS = {
     "echo_gpu_checkpoint_size": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
     "echo_gpu_checkpoint": (ctypes.c_int, [P, P]),
     "echo_gpu_restart": (ctypes.c_int, [P, P]),
+    "echo_gpu_keep_old": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_gpu_dump_size": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
+    "echo_gpu_dump": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_size_t]),
+    "echo_gpu_restart_dump": (ctypes.c_int, [P, P, ctypes.c_size_t, I]),
     "echo_gpu_check_temp": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, D, I]),
     "echo_gpu_out_vars_size": (ctypes.c_int, [P, ctypes.c_uint, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]),
     "echo_gpu_out_vars": (ctypes.c_int, [P, ctypes.c_uint, ctypes.c_int, P, ctypes.c_size_t, I]),
@@ -281,6 +285,26 @@ class Evolve:
         if n.value:
             self._check(self.lib.echo_gpu_hyp_get(self.h, _dp(out)), "hyp_get")
         return out
+
+    def keep_old(self, on: bool = True):
+        """Keep the reference's vold/uold (for a complete dump.dat)."""
+        self._check(self.lib.echo_gpu_keep_old(self.h, int(on)), "keep_old")
+
+    def dump(self, iout: int) -> bytes:
+        """The bytes of dump.dat (out_dump, out.f90:1313-1392)."""
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.echo_gpu_dump_size(self.h, ctypes.byref(n)), "dump_size")
+        buf = ctypes.create_string_buffer(n.value)
+        self._check(self.lib.echo_gpu_dump(self.h, iout, ctypes.cast(buf, P), n.value), "dump")
+        return buf.raw
+
+    def restart_dump(self, data: bytes) -> int:
+        """Restart from the bytes of a dump.dat (out_restart); returns iout."""
+        buf = ctypes.create_string_buffer(data, len(data))
+        io = ctypes.c_int(0)
+        self._check(self.lib.echo_gpu_restart_dump(self.h, ctypes.cast(buf, P), len(data), ctypes.byref(io)),
+                    "restart_dump")
+        return io.value
 
     def checkpoint(self) -> bytes:
         """The run state at this step boundary (out_dump's role)."""

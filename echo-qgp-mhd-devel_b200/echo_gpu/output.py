@@ -78,3 +78,34 @@ def read(data: bytes, cfg, sel: int, precision: int = 8):
         raise ValueError(f"{arr.size} values for {len(names)} fields of {n} cells")
     shape = (cfg.nz, cfg.ny, cfg.nx)
     return float(arr[0]), {name: arr[1 + i * n:1 + (i + 1) * n].reshape(shape) for i, name in enumerate(names)}
+
+
+def write_dump(root: str, id_of_the_run: int, blob: bytes) -> str:
+    """Write the bytes of echo_gpu_dump to outrNNNN/dump.dat (out_dump,
+    out.f90:1349-1381); returns the path."""
+    d = os.path.join(root, run_dir(id_of_the_run))
+    os.makedirs(d, exist_ok=True)
+    path = os.path.join(d, "dump.dat")
+    with open(path, "wb") as f:
+        f.write(blob)
+    return path
+
+
+def read_dump(data: bytes, cfg) -> dict:
+    """Parse dump.dat as out_restart reads it (out.f90:1422-1432):
+    iout, t, timeold, timeinterval, vall, uall, vallold, uallold (the fields
+    krh..kvold_end: 8 with MHD, else 5), g_cov_3_old."""
+    nc = cfg.nx * cfg.ny * cfg.nz
+    kold = 8 if cfg.mhd else 5
+    iout = int(np.frombuffer(data, dtype="<i4", count=1)[0])
+    rest = np.frombuffer(data, dtype="<f8", offset=4)
+    want = 3 + nc * (2 * cfg.nv + 2 * kold) + 1
+    if rest.size != want:
+        raise ValueError(f"dump.dat holds {rest.size} doubles after iout, a run of this shape writes {want}")
+    o = 3
+    out = {"iout": iout, "t": float(rest[0]), "timeold": float(rest[1]), "timeinterval": float(rest[2])}
+    for name, n in (("vall", cfg.nv), ("uall", cfg.nv), ("vallold", kold), ("uallold", kold)):
+        out[name] = rest[o:o + n * nc].copy()
+        o += n * nc
+    out["g_cov_3_old"] = float(rest[o])
+    return out

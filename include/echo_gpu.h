@@ -249,6 +249,28 @@ int echo_gpu_checkpoint_size(const EchoCtx* ctx, size_t* bytes);
 int echo_gpu_checkpoint(EchoCtx* ctx, void* blob);
 int echo_gpu_restart(EchoCtx* ctx, const void* blob);
 
+/* dump.dat in the reference's layout (out_dump / out_restart,
+ * out.f90:1313-1483, with out_freeze off): stream access, no record
+ * markers -- iout (int32), t, timeold, timeinterval (double), vall and uall
+ * (nv fields each, Fortran order), vallold and uallold (the fields krh..
+ * kvold_end: 5, or 8 with MHD, common.f90:378-386), g_cov_3_old.
+ * dump_size gives the bytes; dump fills `buf` with exactly that many (the
+ * caller writes them to outrNNNN/dump.dat); restart_dump reads such a file
+ * of a run of the same shape into the context at a step boundary and
+ * returns its iout, as out_restart does (t, timeold, timeinterval,
+ * g_cov_3_old, v, u, vold; dt and the GLM speed start as after an upload, as
+ * the reference's restart leaves them).  vold / uold are the reference's
+ * step-start copies of the previous step (echo.f90:192-202, 240-241); the
+ * device keeps them only after echo_gpu_keep_old(ctx, 1) (two more copies
+ * of kvold_end fields per step; set at upload as init() does, init.f90:
+ * 3271-3272).  Without it the dump holds the viscous vold's rho and
+ * velocities (the only part the evolution reads, dts in viscous.f90:56-97)
+ * and zeros elsewhere.  All three synchronise the stream. */
+int echo_gpu_keep_old(EchoCtx* ctx, int on);
+int echo_gpu_dump_size(const EchoCtx* ctx, size_t* bytes);
+int echo_gpu_dump(EchoCtx* ctx, int iout, void* buf, size_t bytes);
+int echo_gpu_restart_dump(EchoCtx* ctx, const void* buf, size_t bytes, int* iout);
+
 /* Freeze-out hypersurface (out_hyp, out.f90:1569-1650, with
  * find_hypersurface_ideal/_visco/_mhd and set_fo_ide/_vis,
  * hypersurface.f90:172-460, 775-1117), on the device.  hyp_init sets the
