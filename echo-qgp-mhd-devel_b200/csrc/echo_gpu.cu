@@ -795,6 +795,10 @@ int echo_gpu_dump(EchoCtx* c, int iout, void* buf, size_t bytes) {
   return ECHO_OK;
 }
 
+// t^3 as the step's end computes it on the device (end_step_scalars): a
+// restarted run must hold the bits the uninterrupted one holds
+static __global__ void t3_kernel(DevScalars* sc) { sc->t3 = pow(sc->t, 3.); }
+
 int echo_gpu_restart_dump(EchoCtx* c, const void* buf, size_t bytes, int* iout) {
   (void)cudaGetLastError();
   if (!c || !buf || bytes != dump_bytes(c)) return ECHO_ERR_ARG;
@@ -825,6 +829,11 @@ int echo_gpu_restart_dump(EchoCtx* c, const void* buf, size_t bytes, int* iout) 
   s.timeinterval = hdr[2];
   s.g3old = g3old;
   if (e == cudaSuccess) e = cudaMemcpy(c->d_sc, &s, sizeof(s), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    t3_kernel<<<1, 1, 0, c->stream>>>(c->d_sc);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_v[0], tmp, sizeof(double) * nvc, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_u[0], tmp + nvc, sizeof(double) * nvc, cudaMemcpyHostToDevice);
   // vold: the viscous time derivatives read its velocities (d_vh[1 - vn])

@@ -31,7 +31,7 @@ VARIANTS = {
 
 # one translation unit per equation set, compiled in parallel
 SOURCES = ["echo_gpu.cu", "unit_tests.cu", "kind_hd.cu", "kind_visc.cu", "kind_mhd.cu", "kind_mhdglm.cu", "kind_res.cu",
-           "noalloc.cu", "mlp_train.cu", "batch.cu", "hyper.cu", "output.cu"]
+           "noalloc.cu", "mlp_train.cu", "batch.cu", "hyper.cu", "output.cu", "glauber.cu"]
 
 
 def nvcc() -> str:

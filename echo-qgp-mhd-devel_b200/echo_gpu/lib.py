@@ -51,6 +51,28 @@ class EchoEventStatus(ctypes.Structure):
 
 LL = ctypes.POINTER(ctypes.c_longlong)
 
+
+class EchoOpticalGlauber(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "mass_number", "radius", "delta", "roze", "sigma_in", "ah", "bimpact", "ecenter", "rhocenter",
+        "dr", "dz1", "acc", "deta", "sigeta", "sqrt_s", "nucleon_mass")]
+
+
+def optical_glauber_params(nucleus: str = "Au", b: float = 7.0, sigma_in_mb: float = 42.0, ah: float = 0.15,
+                           ecenter: float = 1.0, rhocenter: float = 0.1, dr: float = 0.001, dz1: float = 0.001,
+                           acc: float = 1e-7, deta: float = 2.0, sigeta: float = 1.5, sqrt_s: float = 200.0,
+                           nucleon_mass: float = 0.938) -> EchoOpticalGlauber:
+    """The GLAUBER_GEOMETRIC parameters: nucleus from nuclear_data.dat
+    (projmass, radius, delta, roze), SIGMA_IN in mb (stored in fm^2,
+    common.f90:2259), AH, impact parameter, ECENTER, the thickness table's
+    r and z steps and accuracy (the reference's printed defaults 0.001,
+    0.001, 1e-7), the eta plateau and Gaussian width and the collision's
+    sqrt(s) for 3+1D."""
+    A, R, a, rho0 = {"Au": (197.0, 6.38, 0.535, 0.1693), "Pb": (208.0, 6.62, 0.546, 0.1604)}[nucleus]
+    return EchoOpticalGlauber(mass_number=A, radius=R, delta=a, roze=rho0, sigma_in=sigma_in_mb / 10.0, ah=ah,
+                              bimpact=b, ecenter=ecenter, rhocenter=rhocenter, dr=dr, dz1=dz1, acc=acc, deta=deta,
+                              sigeta=sigeta, sqrt_s=sqrt_s, nucleon_mass=nucleon_mass)
+
 FUNCTIONS = {
     "echo_gpu_init": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.POINTER(P)]),
     "echo_gpu_free": (ctypes.c_int, [P]),
@@ -91,6 +113,7 @@ FUNCTIONS = {
     "echo_gpu_checkpoint": (ctypes.c_int, [P, P]),
     "echo_gpu_restart": (ctypes.c_int, [P, P]),
     "echo_gpu_keep_old": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_gpu_optical_glauber": (ctypes.c_int, [P, ctypes.POINTER(EchoOpticalGlauber), ctypes.c_double, D, D]),
     "echo_gpu_dump_size": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_size_t)]),
     "echo_gpu_dump": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_size_t]),
     "echo_gpu_restart_dump": (ctypes.c_int, [P, P, ctypes.c_size_t, I]),
@@ -285,6 +308,21 @@ class Evolve:
         if n.value:
             self._check(self.lib.echo_gpu_hyp_get(self.h, _dp(out)), "hyp_get")
         return out
+
+    def optical_glauber(self, g: EchoOpticalGlauber, t: float, peak: float | None = None) -> tuple[float, float]:
+        """The optical Glauber initial state on the device, uploaded at time
+        t; with `peak`, ecenter is rescaled so that the grid's largest e is
+        `peak` (a second device pass).  Returns (check mass, max e)."""
+        chk = ctypes.c_double(0)
+        mx = ctypes.c_double(0)
+        self._check(self.lib.echo_gpu_optical_glauber(self.h, ctypes.byref(g), t, ctypes.byref(chk),
+                                                      ctypes.byref(mx)), "optical_glauber")
+        if peak is not None:
+            g2 = EchoOpticalGlauber.from_buffer_copy(g)
+            g2.ecenter = g.ecenter * peak / mx.value
+            self._check(self.lib.echo_gpu_optical_glauber(self.h, ctypes.byref(g2), t, ctypes.byref(chk),
+                                                          ctypes.byref(mx)), "optical_glauber")
+        return chk.value, mx.value
 
     def keep_old(self, on: bool = True):
         """Keep the reference's vold/uold (for a complete dump.dat)."""

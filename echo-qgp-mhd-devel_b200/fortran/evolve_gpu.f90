@@ -151,6 +151,37 @@ module evolve_gpu
       type(c_ptr), value :: blob
     end function
 
+    ! dump.dat in the reference's own layout (out_dump / out_restart):
+    ! keep_old(1) once after the upload makes vold/uold complete; dump fills
+    ! a buffer of dump_size bytes that the host writes to outrNNNN/dump.dat
+    integer(c_int) function echo_gpu_keep_old(ctx, on) bind(C, name="echo_gpu_keep_old")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: on
+    end function
+
+    integer(c_int) function echo_gpu_dump_size(ctx, nbytes) bind(C, name="echo_gpu_dump_size")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx
+      integer(c_size_t), intent(out) :: nbytes
+    end function
+
+    integer(c_int) function echo_gpu_dump(ctx, iout, buf, nbytes) bind(C, name="echo_gpu_dump")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: iout
+      type(c_ptr), value :: buf
+      integer(c_size_t), value :: nbytes
+    end function
+
+    integer(c_int) function echo_gpu_restart_dump(ctx, buf, nbytes, iout) bind(C, name="echo_gpu_restart_dump")
+      import :: c_int, c_ptr, c_size_t
+      type(c_ptr), value :: ctx
+      type(c_ptr), value :: buf
+      integer(c_size_t), value :: nbytes
+      integer(c_int), intent(out) :: iout
+    end function
+
     ! learned con2prim seed (ALG_SOLV = 101): weights(ECHO_MLP_NWEIGHTS) and
     ! norm(ECHO_MLP_NNORM) as echo_gpu_mlp_train writes them; before the
     ! first evolve_main

@@ -237,6 +237,42 @@ enum {
 int echo_gpu_out_vars_size(const EchoCtx* ctx, unsigned sel, int precision, size_t* bytes);
 int echo_gpu_out_vars(EchoCtx* ctx, unsigned sel, int precision, void* buf, size_t bytes, int* errcode);
 
+/* Optical Glauber initial state on the device (init.f90:852-1242, the
+ * reference's GLAUBER_GEOMETRIC initial conditions; glaubermc.f90 is the
+ * Monte Carlo mode, echo_batch_glauber).  The nucleus' Woods-Saxon
+ * thickness is integrated by the reference's own rule (thickness,
+ * init.f90:1164-1219: radii r = (nc-1) dr out to the grid's reach plus the
+ * impact parameter, |z| <= 2 radius, dz halved from 2 dz1 until the two
+ * end-point sums agree to acc), the numbers of binary collisions and wounded
+ * nucleons at each cell centre use the nearest radius nint(r/dr + 1) (bincoll,
+ * wound, init.f90:971-1032), normalised by those of a b = 0 collision at the
+ * origin (init.f90:1805-1812), and calc_enedens (init.f90:902-929, no
+ * tilting; with nz > 1 times the plateau-plus-Gaussian H(eta) around the
+ * local eta0 of the two thicknesses) gives e; initio (init.f90:852-893)
+ * then sets rho = rhocenter, v = 0 and p = p(e) + przero, and the state is
+ * uploaded as by echo_gpu_upload(v, NULL, t).  *check_mass = the
+ * reference's printed "check nucleus mass" (sum over the table of
+ * r T(r) dr times 2 x 3.1415927); *max_e = the largest e of the grid (with
+ * ecenter = 1 it is the factor a caller divides a target peak by).
+ * Allocates the thickness table (8 bytes per 0.001 fm of reach) on the
+ * first call; synchronises.  Returns ECHO_ERR_ARG (nothing uploaded) when
+ * the table does not converge within 8 halvings of dz. */
+typedef struct EchoOpticalGlauber {
+  double mass_number;   /* projmass (nuclear_data.dat) */
+  double radius, delta; /* Woods-Saxon radius and width (fm) */
+  double roze;          /* normal nuclear density (fm^-3) */
+  double sigma_in;      /* inelastic NN cross section in fm^2 (SIGMA_IN/10, common.f90:2259) */
+  double ah;            /* hardness: weight of binary collisions (AH) */
+  double bimpact;       /* impact parameter (fm) */
+  double ecenter;       /* e at the centre of a b = 0 collision (GeV/fm^3) */
+  double rhocenter;     /* the density primitive */
+  double dr, dz1, acc;  /* thickness table step, first z step, integration accuracy */
+  double deta, sigeta;  /* 3+1D: plateau width and Gaussian width of H(eta) */
+  double sqrt_s, nucleon_mass; /* gamma_col = sqrt_s / (2 m) (common.f90:2261) for eta0 */
+} EchoOpticalGlauber;
+int echo_gpu_optical_glauber(EchoCtx* ctx, const EchoOpticalGlauber* g, double t, double* check_mass,
+                             double* max_e);
+
 /* Checkpoint / restart of a run at a step boundary (the role of out_dump and
  * out_restart, out.f90:1313-1483, which the reference turns off for MHD and
  * Monte Carlo runs; here every equation set).  The blob (checkpoint_size

@@ -3335,3 +3335,165 @@ void orc_mlp_forward(const float* W, const float* norm, const float* X, int n, d
     for (int o = 0; o < 2; o++) out[r * 2 + o] = act[5][o] * norm[14 + o] + norm[12 + o];
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* tabulated EoS at one point: get_energy (eos.f90:468-523)                  */
+/* ------------------------------------------------------------------------ */
+int orc_eos_energy(const EchoParams* p, const double* tab, int n_eos, double pr, double* en) {
+  Phys ph;
+  double* bufs[4] = {0, 0, 0, 0};
+  unit_phys(&ph, p, 1., 1., tab, n_eos, bufs);
+  int e = eos_energy(&ph, 0., en, pr);
+  for (int i = 0; i < 4; i++) free(bufs[i]);
+  return e;
+}
+
+/* ------------------------------------------------------------------------ */
+/* optical Glauber initial state (init.f90:852-1242)                        */
+/* ------------------------------------------------------------------------ */
+
+/* Fortran nint: nearest integer, halves away from zero */
+static long orc_nint(double x) { return x >= 0. ? (long)floor(x + 0.5) : -(long)floor(-x + 0.5); }
+
+/* thickness (init.f90:1164-1219): the Woods-Saxon thickness at nmax radii
+ * r = (nc-1) dr, each the sum over |z| <= 2 radius of the density at
+ * z1 = -zmax, -zmax + dz, ... with dz halved from 2 dz1 until the two
+ * end-point sums agree to acc (at most ORC_THICK_RUNS halvings; the
+ * reference has no limit); thick[nc-1] = sum1 dz.  Returns the reference's
+ * "check nucleus mass", check * 2 * 3.1415927 * dr with
+ * check = sum_nc r sum1 dz (init.f90:1211-1219), or -1 when a radius did not
+ * converge. */
+#define ORC_THICK_RUNS 8
+double orc_thickness(double radius, double delta, double roze, double dr, double dz1, double acc, int nmax,
+                     double* thick) {
+  const double delta_inv = 1. / delta;
+  const double zmax = 2. * radius;
+  double check = 0.;
+  int bad = 0;
+  /* radii are independent: computed in parallel, summed below in the
+   * reference's order */
+  double* term = (double*)malloc(sizeof(double) * (size_t)nmax);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+  for (int nc = 1; nc <= nmax; nc++) {
+    double dz = 2. * dz1;
+    const double r = (nc - 1) * dr;
+    const double r2 = r * r;
+    double ratio = 1000., sum1 = 0., sum2 = 0.;
+    int nrun = 0;
+    while (ratio > acc) {
+      if (nrun == ORC_THICK_RUNS) {
+        bad = 1;
+        break;
+      }
+      dz = dz * 0.5;
+      const long nstep = orc_nint(2. * zmax / dz);
+      nrun = nrun + 1;
+      double z1 = -zmax, z2 = z1 + dz;
+      sum1 = 0.;
+      sum2 = 0.;
+      for (long n = 1; n <= nstep; n++) {
+        double z = z1;
+        double erre = sqrt(r2 + z * z);
+        double espo = exp((erre - radius) * delta_inv);
+        double rho1 = roze / (espo + 1.);
+        z = z2;
+        erre = sqrt(r2 + z * z);
+        espo = exp((erre - radius) * delta_inv);
+        double rho2 = roze / (espo + 1.);
+        sum1 = sum1 + rho1;
+        sum2 = sum2 + rho2;
+        z1 = z2;
+        z2 = z2 + dz;
+      }
+      ratio = fabs(2. * (sum2 - sum1) / (sum1 + sum2));
+    }
+    term[nc - 1] = r * sum1 * dz;
+    thick[nc - 1] = sum1 * dz;
+  }
+  for (int nc = 1; nc <= nmax; nc++) check = check + term[nc - 1];
+  free(term);
+  return bad ? -1. : check * 2 * 3.1415927 * dr;
+}
+
+/* wound (init.f90:1001-1032) and bincoll (:971-997) at (xx, yy) with impact
+ * parameter b1: the thickness of each nucleus by the nearest table point
+ * nint(r/dr + 1) */
+static void orc_wound(const double* thick, int nmax, double dr, double amassa, double sigma_in, double xx, double yy,
+                      double b1, double* tA, double* tB, double* thplus, double* thminus, int* bad) {
+  double xs = xx + b1 * 0.5;
+  double radius = sqrt(xs * xs + yy * yy);
+  long ip = orc_nint(radius / dr + 1);
+  xs = xx - b1 * 0.5;
+  radius = sqrt(xs * xs + yy * yy);
+  long im = orc_nint(radius / dr + 1);
+  if (ip < 1 || ip > nmax || im < 1 || im > nmax) {
+    *bad = 1;
+    ip = ip < 1 ? 1 : (ip > nmax ? nmax : ip);
+    im = im < 1 ? 1 : (im > nmax ? nmax : im);
+  }
+  *thplus = thick[ip - 1];
+  *thminus = thick[im - 1];
+  double a = sigma_in * (*thminus) / amassa;
+  a = pow(1. - a, amassa);
+  a = 1. - a;
+  *tA = a * (*thplus);
+  double b = sigma_in * (*thplus) / amassa;
+  b = pow(1. - b, amassa);
+  b = 1. - b;
+  *tB = b * (*thminus);
+}
+
+/* H_of_eta (init.f90:933-967) without tilting, centre flag */
+static double orc_h_of_eta(double etac, double etaflat, double sigmaetasq_inv, double thplus, double thminus,
+                           double gamma_col, double beta_col) {
+  double eta0 = 0.5 * log(((thminus + thplus) * gamma_col + (thminus - thplus) * gamma_col * beta_col) /
+                          ((thminus + thplus) * gamma_col - (thminus - thplus) * gamma_col * beta_col));
+  double d = fabs(etac - eta0);
+  if (d > (etaflat * 0.5)) {
+    double q = d - (0.5 * etaflat);
+    return exp(-1.0 * (q * q) * 0.5 * sigmaetasq_inv);
+  }
+  return 1.0;
+}
+
+/* The energy density of calc_enedens (init.f90:902-929, no tilting) at the
+ * cell centres x1 + (i - 1/2) dx of an nx x ny x nz grid (Fortran order),
+ * with the weights of a b = 0 collision at the origin (init.f90:1805-1812)
+ * and eta from z1 + (k - 1/2) dz when nz > 1.  g: the EchoOpticalGlauber
+ * parameters; the thickness table of nmax points is built first.  Returns
+ * the check mass, or -1 (a radius that did not converge or a cell beyond
+ * the table). */
+double orc_optical_glauber(const EchoOpticalGlauber* g, int nx, int ny, int nz, double x1, double x2, double y1,
+                           double y2, double z1, double z2, double* e) {
+  const double dx = (x2 - x1) / nx, dy = (y2 - y1) / ny, dzz = (z2 - z1) / nz;
+  const double largestx = fmax(fabs(x1), fabs(x2)) + g->bimpact;
+  const double largesty = fmax(fabs(y1), fabs(y2));
+  const double rmax = sqrt(largestx * largestx + largesty * largesty);
+  const int nmax = (int)(rmax / g->dr) + 1;
+  double* thick = (double*)malloc(sizeof(double) * nmax);
+  double check = orc_thickness(g->radius, g->delta, g->roze, g->dr, g->dz1, g->acc, nmax, thick);
+  int bad = check < 0.;
+  double tt1, tt2, thp, thm;
+  orc_wound(thick, nmax, g->dr, g->mass_number, g->sigma_in, 0., 0., 0., &tt1, &tt2, &thp, &thm, &bad);
+  const double weightbin = g->sigma_in * thp * thm;
+  const double weightwound = tt1 + tt2;
+  const double ah = g->ah;
+  const double gamma_col = g->sqrt_s / (2. * g->nucleon_mass);
+  const double beta_col = sqrt(1. - (1. / (gamma_col * gamma_col)));
+  const double sigeta2_inv = 1. / (g->sigeta * g->sigeta);
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        const double xx = x1 + (i + 1 - 0.5) * dx, yy = y1 + (j + 1 - 0.5) * dy;
+        orc_wound(thick, nmax, g->dr, g->mass_number, g->sigma_in, xx, yy, g->bimpact, &tt1, &tt2, &thp, &thm, &bad);
+        const double bc = g->sigma_in * thp * thm;
+        double ed = g->ecenter * (ah * bc + (1. - ah) * (tt1 + tt2)) / ((ah * weightbin) + ((1 - ah) * weightwound));
+        if (nz > 1) {
+          const double eta = z1 + (k + 1 - 0.5) * dzz;
+          ed = orc_h_of_eta(eta, g->deta, sigeta2_inv, thp, thm, gamma_col, beta_col) * ed;
+        }
+        e[((size_t)k * ny + j) * nx + i] = ed;
+      }
+  free(thick);
+  return bad ? -1. : check;
+}

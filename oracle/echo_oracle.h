@@ -8,11 +8,16 @@
  * call it.
  *
  * Parity status: the reference is Fortran and no Fortran compiler exists in
- * this environment, so the restatement cannot be diffed against the
- * reference binary ("parity unpinned" against the Fortran build).  It is
- * pinned instead against the analytic solutions the reference's own test
- * problems use (Bjorken flow, Bjorken MHD flow, Gubser flow) and against
- * committed golden vectors it produced (tests/golden).
+ * this environment or on the GPU hosts (probed), so the restatement cannot
+ * be diffed against the reference binary ("parity unpinned" against the
+ * Fortran build of the step).  It is pinned instead against the analytic
+ * solutions the reference's own test problems use (Bjorken flow, Bjorken
+ * MHD flow, Gubser flow), against the two values of the step's
+ * neighbourhood that the reference printed in its own run log
+ * (doc/images/echo-qgp-output.txt: the optical Glauber thickness check and
+ * a tabulated-EoS energy, reproduced digit for digit and bit for bit,
+ * tests/test_reference_pins.py), and against committed golden vectors it
+ * produced (tests/golden).
  */
 #ifndef ECHO_ORACLE_H
 #define ECHO_ORACLE_H
@@ -74,6 +79,17 @@ int orc_flux(const EchoParams* p, const double* eos_table, int n_eos,
              double* vf);
 
 /* the learned con2prim seed network (gradient check, FP64) */
+/* tabulated EoS e(p) (get_energy, eos.f90:468-523); returns the code */
+int orc_eos_energy(const EchoParams* p, const double* eos_table, int n_eos, double pr, double* en);
+
+/* optical Glauber (init.f90:852-1242): the thickness table (returns the
+ * reference's printed "check nucleus mass") and the energy density of
+ * calc_enedens at the cell centres */
+double orc_thickness(double radius, double delta, double roze, double dr, double dz1, double acc, int nmax,
+                     double* thick);
+double orc_optical_glauber(const EchoOpticalGlauber* g, int nx, int ny, int nz, double x1, double x2, double y1,
+                           double y2, double z1, double z2, double* e);
+
 void orc_mlp_grad(const float* W, const float* Xs, const float* Ts, int n, double* loss, double* grad);
 void orc_mlp_forward(const float* W, const float* norm, const float* X, int n, double* out);
 

@@ -66,6 +66,11 @@ def lib():
         Fp = ctypes.POINTER(ctypes.c_float)
         L.orc_mlp_grad.argtypes = [Fp, Fp, Fp, ctypes.c_int, D, D]
         L.orc_mlp_forward.argtypes = [Fp, Fp, Fp, ctypes.c_int, D]
+        L.orc_eos_energy.argtypes = [P, D, ctypes.c_int, ctypes.c_double, D]
+        L.orc_thickness.restype = ctypes.c_double
+        L.orc_thickness.argtypes = [ctypes.c_double] * 6 + [ctypes.c_int, D]
+        L.orc_optical_glauber.restype = ctypes.c_double
+        L.orc_optical_glauber.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 6 + [D]
         _lib = L
     return _lib
 
@@ -254,3 +259,25 @@ def mlp_forward(weights, norm, X):
     out = np.zeros((len(X), 2))
     lib().orc_mlp_forward(_fp(W), _fp(N), _fp(X), len(X), _dp(out))
     return out
+
+
+def eos_energy(params, eos_table, pr: float) -> tuple[int, float]:
+    """get_energy (eos.f90:468-523) of the tabulated EoS at pressure pr."""
+    tab, n = _tab(eos_table)
+    en = ctypes.c_double(0)
+    err = lib().orc_eos_energy(ctypes.byref(params), _dp(tab), n, pr, ctypes.byref(en))
+    return err, en.value
+
+
+def thickness(radius, delta, roze, dr, dz1, acc, nmax):
+    """thickness (init.f90:1164-1219): (check mass, T(r) table)."""
+    thick = np.empty(nmax)
+    chk = lib().orc_thickness(radius, delta, roze, dr, dz1, acc, nmax, _dp(thick))
+    return chk, thick
+
+
+def optical_glauber(g, nx, ny, nz, x1, x2, y1, y2, z1, z2):
+    """calc_enedens (init.f90:902-929) at the cell centres: (check mass, e)."""
+    e = np.empty(nx * ny * nz)
+    chk = lib().orc_optical_glauber(ctypes.byref(g), nx, ny, nz, x1, x2, y1, y2, z1, z2, _dp(e))
+    return chk, e

@@ -62,7 +62,8 @@ def test_dump_layout_and_restart(case, tmp_path):
         vc, uc = c.download()
         assert np.array_equal(vb, vc) and np.array_equal(ub, uc)
     else:
-        assert np.array_equal(vb, va) and np.array_equal(ub, ua)
+        assert np.array_equal(vb, va), np.max(np.abs(vb - va))
+        assert np.array_equal(ub, ua), (np.max(np.abs(ub - ua)), np.argmax(np.abs(ub - ua)) // cfg.ncell)
     assert b.stats().t == a.stats().t
     # a dump of another run's shape is refused
     other = Evolve(*setup(CASES["hd2d"]().replace(nx=14))[:2], exact=True)
