@@ -458,6 +458,12 @@ def run_batched(args, torch, barrier, world, rank, net=None):
     b.glauber(srcs, es.cfg.tstart, es.tmax)
     ic_s = time.perf_counter() - t0
     tune_ms = b.autotune(3)
+    tune_rows = b.autotune_report()
+    tune_choice = b.tuning()
+    best_stage = {}
+    for r in tune_rows:
+        if r["slot"] == "stage" and (r["mode"] not in best_stage or r["ms"] < best_stage[r["mode"]]["ms"]):
+            best_stage[r["mode"]] = r
     b.run(max(args.warmup, 3))  # builds the step graphs
     b.glauber(srcs, es.cfg.tstart, es.tmax)
     stream = torch.cuda.ExternalStream(b.stream_handle())
@@ -564,6 +570,14 @@ def run_batched(args, torch, barrier, world, rank, net=None):
         "speedup_vs_sequential_note": "plain batched over plain single-grid, both on one GPU",
         "kernels_ms_per_step_at_start": {k: round(x, 4) for k, x in prof.items()},
         "autotuned_ms_per_launch": {k: round(x, 4) for k, x in tune_ms.items()},
+        "autotune": {"candidates_timed": len(tune_rows),
+                     "search_space": "per slot: tile of 128/256/512 faces or cells x (one CTA per tile, or "
+                                     "1..occupancy CTAs per SM); per stage: one launch per phase (7 launches) or "
+                                     "one cooperative launch (1..occupancy CTAs per SM)",
+                     "choice": tune_choice,
+                     "best_stage_ms": {k: {"ms": round(v["ms"], 4), "ctas": v["ctas"]} for k, v in best_stage.items()},
+                     "launches_per_stage": 1 if tune_choice["mode"] == "cooperative" else
+                     (7 if es.cfg.viscosity and es.cfg.smooth_temp > 0 else 6)},
         "ic": {"nucleon_sampling_s_host": sampling_s, "smearing_and_eos_s_device": ic_s},
         "con2prim": "viscous nested Newton (system.f90:564-666), plain and from the learned seed "
                     "(the 2+1D viscous workload's network)",

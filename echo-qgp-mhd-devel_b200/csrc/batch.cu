@@ -67,8 +67,16 @@ static void batch_faces_all(EchoBatch* b) {
     }
 }
 
-// one explicit RK stage of every live event (evolve_main, evolve.f90:114-298)
+// one explicit RK stage of every live event (evolve_main, evolve.f90:114-298):
+// one launch per phase (mode 0) or one cooperative launch (mode 1)
 static void enqueue_batch_stage(EchoBatch* b, int irk) {
+  if (b->mode == 1) {
+    BDISPATCH(b, launch_batch_stage, b, irk, (unsigned*)nullptr);
+    batch_mark(b, PK_STAGE);
+    if (irk == 1) b->ucur = 1 - b->ucur;
+    b->vcur = 1 - b->vcur;
+    return;
+  }
   batch_begin(b, irk);
   batch_faces_all(b);
   batch_scalars(b, irk);
@@ -170,12 +178,13 @@ int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos, int
       d.face[k] = face[k];
       if (n3[k] > 1) {
         face[k] += nf[k];
-        tiles[k] += tiles_of(nf[k]);
+        tiles[k] += tiles_of(nf[k], BATCH_TILE);
         b->has_dir[k] = true;
       }
     }
-    tiles[PH_CELL] += tiles_of(d.g.ncell);
+    tiles[PH_CELL] += tiles_of(d.g.ncell, BATCH_TILE);
   }
+  for (int ph = 0; ph < PH_N; ph++) b->tile[ph] = BATCH_TILE;
   for (int ph = 0; ph < PH_N; ph++) {
     if (tiles[ph] >= (1ll << 31)) {
       delete b;
@@ -236,6 +245,11 @@ int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos, int
   b->freeze_type = 1;
   b->vcur = b->ucur = b->vn = 0;
   b->marks = nullptr;
+  b->mode = 0;
+  b->coop_grid = 0;
+  b->graphs_off = false;
+  CK(cudaMalloc(&b->d_bar, 4 * sizeof(unsigned)));
+  CK(cudaMemset(b->d_bar, 0, 4 * sizeof(unsigned)));
   *out = b;
   return ECHO_OK;
 }
@@ -254,6 +268,7 @@ int echo_batch_free(EchoBatch* b) {
     cudaFree(b->d_WD[k]);
   }
   cudaFree(b->d_fail);
+  cudaFree(b->d_bar);
   cudaFree(b->d_mlp_frag);
   cudaFree(b->d_mlp_par);
   cudaFree(b->d_ev);
@@ -413,13 +428,29 @@ int echo_batch_run(EchoBatch* b, int nsteps) {
   if (b->p.algo_solver == ECHO_C2P_MLP && !b->d_mlp_frag) return ECHO_ERR_ARG;  // no network loaded
   for (int s = 0; s < nsteps; s++) {
     int key = b->ucur | (b->vcur << 1) | (b->vn << 2);
+    if (b->graphs_off) {  // launches straight onto the stream
+      enqueue_batch_step(b);
+      continue;
+    }
     if (!b->graph_ok[key]) {
-      cudaGraph_t gr;
+      cudaGraph_t gr = nullptr;
+      const int ucur = b->ucur, vcur = b->vcur, vn = b->vn;
       CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
       enqueue_batch_step(b);
-      CK(cudaStreamEndCapture(b->stream, &gr));
-      CK(cudaGraphInstantiate(&b->graph[key], gr, 0));
-      cudaGraphDestroy(gr);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[key], gr, 0);
+      if (gr) cudaGraphDestroy(gr);
+      if (e != cudaSuccess) {
+        // a launch this stream cannot capture (the cooperative stage
+        // kernel on a driver without that support): run without graphs
+        (void)cudaGetLastError();
+        b->graphs_off = true;
+        b->ucur = ucur;
+        b->vcur = vcur;
+        b->vn = vn;
+        enqueue_batch_step(b);
+        continue;
+      }
       b->graph_ok[key] = true;
     } else {
       advance_batch_roles(b);
@@ -427,6 +458,19 @@ int echo_batch_run(EchoBatch* b, int nsteps) {
     CK(cudaGraphLaunch(b->graph[key], b->stream));
   }
   CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+// the timeout flag of the cooperative stage's grid barrier
+static int check_barrier(EchoBatch* b) {
+  if (b->mode != 1) return ECHO_OK;
+  unsigned flag = 0;
+  CK(cudaMemcpyAsync(&flag, b->d_bar + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (flag) {
+    fprintf(stderr, "echo_batch: a grid barrier of the cooperative stage timed out\n");
+    return ECHO_ERR_TIMEOUT;
+  }
   return ECHO_OK;
 }
 
@@ -481,7 +525,7 @@ int echo_batch_sync(EchoBatch* b) {
   if (!b) return ECHO_ERR_ARG;
   CK(cudaStreamSynchronize(b->stream));
   CK(cudaGetLastError());
-  return ECHO_OK;
+  return check_barrier(b);
 }
 
 int echo_batch_stream(EchoBatch* b, void** stream) {
@@ -608,6 +652,15 @@ static int save_batch(EchoBatch* b, BatchSave& s, bool back) {
   return ECHO_OK;
 }
 
+// tiles of each list with every event live, for the current tile lengths
+static void recompute_max_tiles(EchoBatch* b) {
+  for (int ph = 0; ph < PH_N; ph++) {
+    long long n = 0;
+    for (int e = 0; e < b->nev; e++) n += event_tiles(b->h_ev[e].g, ph, b->tile[ph]);
+    b->max_tiles[ph] = (int)n;
+  }
+}
+
 // device time of `reps` launches of slot sl with its current shape
 static int time_slot(EchoBatch* b, int sl, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
   CK(cudaEventRecord(e0, b->stream));
@@ -629,6 +682,35 @@ static int time_slot(EchoBatch* b, int sl, int reps, cudaEvent_t e0, cudaEvent_t
   return ECHO_OK;
 }
 
+// device time of `reps` first stages in the current mode; the roles are
+// put back after each, so every repetition computes the same stage (it
+// writes only the buffers the stage produces)
+static int time_stage(EchoBatch* b, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+  const int u0 = b->ucur, v0 = b->vcur;
+  CK(cudaEventRecord(e0, b->stream));
+  for (int r = 0; r < reps; r++) {
+    enqueue_batch_stage(b, 1);
+    b->ucur = u0;
+    b->vcur = v0;
+  }
+  CK(cudaEventRecord(e1, b->stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaGetLastError());
+  int r = check_barrier(b);
+  if (r) return r;
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  *ms = t / reps;
+  return ECHO_OK;
+}
+
+static void tune_log(EchoBatch* b, double what, double shape, double ctas, double ms) {
+  b->tune.push_back(what);
+  b->tune.push_back(shape);
+  b->tune.push_back(ctas);
+  b->tune.push_back(ms);
+}
+
 int echo_batch_autotune(EchoBatch* b, int reps, double* ms_out) {
   (void)cudaGetLastError();
   if (!b || reps < 1) return ECHO_ERR_ARG;
@@ -642,39 +724,139 @@ int echo_batch_autotune(EchoBatch* b, int reps, double* ms_out) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
+  b->tune.clear();
   const bool smooth = b->kind == KIND_VISC && b->p.enable_smooth_viscosity;
   const int ph_of[SL_N] = {PH_FX, PH_FY, PH_FZ, PH_CELL, PH_CELL};
-  // the inputs of the first-stage update: tile lists, face fluxes and dt
-  batch_begin(b, 1);
-  batch_faces_all(b);
-  batch_scalars(b, 1);
+  const int tiles[3] = {128, 256, 512};
+  const int mode0 = b->mode;
+  b->mode = 0;
+  // one phase at a time: tile length x CTAs (one per tile, or k per SM)
+  double best_ms[SL_N];
+  int best_tile[SL_N], best_cta[SL_N];
   for (int sl = 0; sl < SL_N; sl++) {
-    if (ms_out) ms_out[sl] = 0.;
-    if (sl <= SL_FZ && !b->has_dir[sl]) continue;
-    if (sl == SL_SMOOTH && !smooth) continue;
-    std::vector<int> cand = {0};
-    for (int k = 1; k <= occ[sl]; k++)
-      if (k * b->nsm < b->max_tiles[ph_of[sl]]) cand.push_back(k * b->nsm);
-    double best = 1e300;
-    int best_c = 0;
-    for (int c : cand) {
-      b->sched[sl] = c;
+    best_ms[sl] = 1e300;
+    best_tile[sl] = b->tile[ph_of[sl]];
+    best_cta[sl] = b->sched[sl];
+  }
+  for (int ti = 0; ti < 3; ti++) {
+    for (int ph = 0; ph < PH_N; ph++) b->tile[ph] = tiles[ti];
+    recompute_max_tiles(b);
+    // the inputs of the first-stage update: tile lists, face fluxes and dt
+    batch_begin(b, 1);
+    batch_faces_all(b);
+    batch_scalars(b, 1);
+    for (int sl = 0; sl < SL_N; sl++) {
+      if (sl <= SL_FZ && !b->has_dir[sl]) continue;
+      if (sl == SL_SMOOTH && !smooth) continue;
+      std::vector<int> cand = {0};
+      for (int k = 1; k <= occ[sl]; k++)
+        if (k * b->nsm < b->max_tiles[ph_of[sl]]) cand.push_back(k * b->nsm);
+      for (int c : cand) {
+        b->sched[sl] = c;
+        double t;
+        r = time_slot(b, sl, 1, e0, e1, &t);  // warm-up
+        if (!r) r = time_slot(b, sl, reps, e0, e1, &t);
+        if (r) return r;
+        tune_log(b, sl, tiles[ti], c, t);
+        if (t < best_ms[sl]) {
+          best_ms[sl] = t;
+          best_tile[sl] = tiles[ti];
+          best_cta[sl] = c;
+        }
+      }
+      b->sched[sl] = best_cta[sl];
+    }
+  }
+  for (int sl = 0; sl < SL_N; sl++) {
+    if (ms_out) ms_out[sl] = best_ms[sl] < 1e299 ? best_ms[sl] : 0.;
+    b->sched[sl] = best_cta[sl];
+  }
+  for (int d = 0; d < 3; d++) b->tile[d] = best_tile[d];
+  // the cell list serves the update and the smoothing: the update's choice
+  b->tile[PH_CELL] = best_tile[SL_UPDATE];
+  recompute_max_tiles(b);
+  // the whole first stage: one launch per phase, then one cooperative
+  // launch with 1..occupancy CTAs per SM
+  double t_phased = 1e300, t_coop = 1e300;
+  r = time_stage(b, 1, e0, e1, &t_phased);
+  if (!r) r = time_stage(b, reps, e0, e1, &t_phased);
+  if (r) return r;
+  tune_log(b, SL_N, 0, 0, t_phased);
+  unsigned best_grid = 0;
+  if (b->p.recal == ECHO_REC_WENO5) {
+    b->mode = 1;
+    unsigned gmax = 0;
+    b->coop_grid = 0;
+    BDISPATCH(b, launch_batch_stage, b, 1, &gmax);  // warm-up, and the largest resident grid
+    CK(cudaStreamSynchronize(b->stream));
+    CK(cudaGetLastError());
+    r = check_barrier(b);
+    if (r) return r;
+    for (unsigned g = (unsigned)b->nsm; g <= gmax && gmax > 0; g += (unsigned)b->nsm) {
+      b->coop_grid = g;
       double t;
-      r = time_slot(b, sl, 1, e0, e1, &t);  // warm-up
-      if (!r) r = time_slot(b, sl, reps, e0, e1, &t);
+      r = time_stage(b, reps, e0, e1, &t);
       if (r) return r;
-      if (t < best) {
-        best = t;
-        best_c = c;
+      tune_log(b, SL_N, 1, g, t);
+      if (t < t_coop) {
+        t_coop = t;
+        best_grid = g;
       }
     }
-    b->sched[sl] = best_c;
-    if (ms_out) ms_out[sl] = best;
   }
+  if (t_coop < t_phased) {
+    b->mode = 1;
+    b->coop_grid = best_grid;
+  } else {
+    b->mode = 0;
+    b->coop_grid = 0;
+  }
+  (void)mode0;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   drop_graphs(b);
   return save_batch(b, sv, true);
+}
+
+int echo_batch_autotune_report(const EchoBatch* b, double* rows, int cap, int* n) {
+  if (!b || !n || cap < 0) return ECHO_ERR_ARG;
+  int m = (int)(b->tune.size() / 4);
+  *n = m;
+  if (rows)
+    for (int i = 0; i < m && i < cap; i++)
+      for (int q = 0; q < 4; q++) rows[4 * i + q] = b->tune[4 * (size_t)i + q];
+  return ECHO_OK;
+}
+
+int echo_batch_set_tiles(EchoBatch* b, const int* tiles) {
+  if (!b || !tiles) return ECHO_ERR_ARG;
+  for (int ph = 0; ph < PH_N; ph++)
+    if (tiles[ph] < BATCH_NT || tiles[ph] > 8 * BATCH_NT || tiles[ph] % BATCH_NT) return ECHO_ERR_ARG;
+  CK(cudaStreamSynchronize(b->stream));
+  for (int ph = 0; ph < PH_N; ph++) b->tile[ph] = tiles[ph];
+  recompute_max_tiles(b);
+  drop_graphs(b);
+  return ECHO_OK;
+}
+
+int echo_batch_set_mode(EchoBatch* b, int mode, int grid) {
+  if (!b || (mode != 0 && mode != 1) || grid < 0) return ECHO_ERR_ARG;
+  if (mode == 1 && b->p.recal != ECHO_REC_WENO5) return ECHO_ERR_UNSUPPORTED;
+  CK(cudaStreamSynchronize(b->stream));
+  b->mode = mode;
+  b->coop_grid = (unsigned)grid;
+  b->graphs_off = false;
+  drop_graphs(b);
+  return ECHO_OK;
+}
+
+int echo_batch_get_tuning(const EchoBatch* b, int* out) {
+  if (!b || !out) return ECHO_ERR_ARG;
+  for (int ph = 0; ph < PH_N; ph++) out[ph] = b->tile[ph];
+  out[PH_N] = b->mode;
+  out[PH_N + 1] = (int)b->coop_grid;
+  out[PH_N + 2] = b->graphs_off ? 0 : 1;
+  return ECHO_OK;
 }
 
 }  // extern "C"

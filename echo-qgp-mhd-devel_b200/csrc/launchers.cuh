@@ -488,6 +488,126 @@ void launch_batch_repair_smooth(EchoBatch* b) {
   }
 }
 
+// the instantiation of batch_stage_kernel a batch uses
+template <int KIND>
+static void* batch_stage_variant(const EchoBatch* b) {
+  constexpr bool CAN_SEED = Traits<KIND>::MHD || Traits<KIND>::VISC;
+  constexpr bool VISC = Traits<KIND>::VISC;
+  if (batch_seeded<KIND>(b) && VISC && b->p.imex) return (void*)batch_stage_kernel<KIND, CAN_SEED, VISC>;
+  if (batch_seeded<KIND>(b)) return (void*)batch_stage_kernel<KIND, CAN_SEED, false>;
+  if (VISC && b->p.imex) return (void*)batch_stage_kernel<KIND, false, VISC>;
+  return (void*)batch_stage_kernel<KIND, false, false>;
+}
+
+// Stage irk of every live event as one cooperative launch (mode 1): the
+// arguments of the per-phase launches, with the roles of the repair and the
+// smoothing those after the update (the update of stage 1 writes the other
+// u buffer).
+template <int KIND>
+int launch_batch_stage(EchoBatch* b, int irk, unsigned* grid_max) {
+  static const double crk[3][3][2] = {{{0., 1.}, {0., 0.}, {0., 0.}},
+                                      {{0., 1.}, {1. / 2., 1. / 2.}, {0., 0.}},
+                                      {{0., 1.}, {3. / 4., 1. / 4.}, {1. / 3., 2. / 3.}}};
+  void* fn = batch_stage_variant<KIND>(b);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BATCH_NT, 0) != cudaSuccess || occ < 1)
+    return ECHO_ERR_UNSUPPORTED;
+  const unsigned gmax = (unsigned)occ * (unsigned)b->nsm;
+  if (grid_max) *grid_max = gmax;
+  const unsigned grid = b->coop_grid > 0 && b->coop_grid <= gmax ? b->coop_grid : gmax;
+  BatchStageArgs S;
+  memset(&S, 0, sizeof(S));
+  S.face.P = b->P;
+  S.face.g = Grid{};
+  S.face.v = b->d_v[b->vcur];
+  S.face.sc = nullptr;
+  S.face.coordinates = b->p.coordinates;
+  for (int d = 0; d < 3; d++) {
+    S.bc[d] = b->bc[d];
+    S.bc_uniform[d] = b->bc_uniform[d];
+    S.bc_signed[d] = b->bc_signed[d];
+  }
+  for (int d = 0; d < 3; d++) {
+    S.F[d] = b->d_F[d];
+    S.WD[d] = b->d_WD[d];
+  }
+  UpdateArgs& A = S.upd;
+  A.P = b->P;
+  A.g = Grid{};
+  A.Fx = b->d_F[0];
+  A.Fy = b->d_F[1];
+  A.Fz = b->d_F[2];
+  A.WDx = b->d_WD[0];
+  A.WDy = b->d_WD[1];
+  A.WDz = b->d_WD[2];
+  A.vin = b->d_v[b->vcur];
+  A.vout = b->d_v[1 - b->vcur];
+  A.uin = b->d_u[b->ucur];
+  A.uout = irk == 1 ? b->d_u[1 - b->ucur] : b->d_u[b->ucur];
+  A.u0 = irk == 1 ? b->d_u[b->ucur] : b->d_u[1 - b->ucur];
+  A.vnew = b->d_vh[b->vn];
+  A.vold = b->d_vh[1 - b->vn];
+  A.vsnap = (Traits<KIND>::VISC && irk == 1) ? b->d_vh[b->vn] : nullptr;
+  A.du_out = nullptr;
+  A.fail = b->d_fail;
+  A.sc = nullptr;
+  const int nrk = b->p.nrk;
+  A.c1 = crk[nrk - 1][irk - 1][0];
+  A.c2 = crk[nrk - 1][irk - 1][1];
+  A.irk = irk;
+  A.nrk = nrk;
+  A.divclean = b->p.divclean;
+  A.coordinates = b->p.coordinates;
+  A.algo = b->p.algo_solver;
+  A.mode = MODE_RK;
+  A.tol = b->p.c2p_tol;
+  A.mlp.frag = b->d_mlp_frag;
+  A.mlp.par = b->d_mlp_par;
+  ScalarArgs& C = S.sca;
+  C.sc = nullptr;
+  C.g = Grid{};
+  C.cfl = b->p.cfl;
+  C.maxdt = b->p.maxdt;
+  C.glm_alpha = b->p.glm_alpha;
+  C.irk = irk;
+  C.nrk = b->p.nrk;
+  C.divclean = b->p.divclean;
+  C.mode = 0;
+  const int ucur_after = irk == 1 ? 1 - b->ucur : b->ucur;
+  RepairArgs& R = S.rep;
+  R.P = b->P;
+  R.g = Grid{};
+  R.vold = b->d_v[b->vcur];
+  R.vnew = b->d_v[1 - b->vcur];
+  R.u = b->d_u[ucur_after];
+  R.fail = b->d_fail;
+  R.sc = nullptr;
+  R.coordinates = b->p.coordinates;
+  R.algo = b->p.algo_solver;
+  R.maxspeed = b->p.maxspeed;
+  R.tol = b->p.c2p_tol;
+  R.h_alpha = 0.;
+  SmoothArgs& M = S.smo;
+  M.P = b->P;
+  M.g = Grid{};
+  M.v = b->d_v[1 - b->vcur];
+  M.u = b->d_u[ucur_after];
+  M.sc = nullptr;
+  M.coordinates = b->p.coordinates;
+  M.smooth_pressure = b->p.smooth_pressure;
+  S.B = batch_dev(b);
+  S.nv = b->nv;
+  S.irk = irk;
+  S.roles = b->ucur | (b->vcur << 1);
+  S.smooth = (KIND == KIND_VISC && b->p.enable_smooth_viscosity) ? 1 : 0;
+  S.bar = b->d_bar;
+  void* args[] = {&S};
+  cudaMemsetAsync(b->d_bar, 0, 3 * sizeof(unsigned), b->stream);
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(BATCH_NT), args, 0, b->stream) == cudaSuccess
+             ? ECHO_OK
+             : ECHO_ERR_CUDA;
+}
+
 template <int KIND>
 void launch_batch_p2c(EchoBatch* b) {
   batch_p2c_kernel<KIND><<<(unsigned)(b->max_tiles[PH_CELL] > 0 ? b->max_tiles[PH_CELL] : 1), 128, 0, b->stream>>>(
@@ -533,4 +653,5 @@ void batch_occupancy(const EchoBatch* b, int* per_sm) {
   template void echo::launch_batch_update<K>(EchoBatch*, int);                \
   template void echo::launch_batch_repair_smooth<K>(EchoBatch*);              \
   template void echo::launch_batch_p2c<K>(EchoBatch*);                        \
+  template int echo::launch_batch_stage<K>(EchoBatch*, int, unsigned*);        \
   template void echo::batch_occupancy<K>(const EchoBatch*, int*);

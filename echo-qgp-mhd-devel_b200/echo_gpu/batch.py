@@ -174,6 +174,37 @@ class Batch:
         self._check(self.lib.echo_batch_autotune(self.h, reps, _dp(ms)), "autotune")
         return dict(zip(SLOTS, ms.tolist()))
 
+    def autotune_report(self) -> list[dict]:
+        """Every candidate the last autotune timed."""
+        n = ctypes.c_int(0)
+        self._check(self.lib.echo_batch_autotune_report(self.h, None, 0, ctypes.byref(n)), "autotune_report")
+        rows = np.zeros(4 * max(n.value, 1))
+        self._check(self.lib.echo_batch_autotune_report(self.h, _dp(rows), n.value, ctypes.byref(n)),
+                    "autotune_report")
+        out = []
+        for i in range(n.value):
+            what, shape, ctas, ms = rows[4 * i:4 * i + 4]
+            if int(what) < len(SLOTS):
+                out.append({"slot": SLOTS[int(what)], "tile": int(shape), "ctas": int(ctas), "ms": float(ms)})
+            else:
+                out.append({"slot": "stage", "mode": "cooperative" if int(shape) else "phased",
+                            "ctas": int(ctas), "ms": float(ms)})
+        return out
+
+    def set_tiles(self, faces: int = 128, cells: int = 128):
+        t = np.array([faces, faces, faces, cells], dtype=np.int32)
+        self._check(self.lib.echo_batch_set_tiles(self.h, t.ctypes.data_as(I)), "set_tiles")
+
+    def set_mode(self, mode: int, grid: int = 0):
+        """0: one launch per phase; 1: one cooperative launch per stage."""
+        self._check(self.lib.echo_batch_set_mode(self.h, mode, grid), "set_mode")
+
+    def tuning(self) -> dict:
+        out = np.zeros(7, dtype=np.int32)
+        self._check(self.lib.echo_batch_get_tuning(self.h, out.ctypes.data_as(I)), "get_tuning")
+        return {"tiles": out[:4].tolist(), "mode": "cooperative" if out[4] else "phased",
+                "coop_grid": int(out[5]), "graphs": bool(out[6])}
+
     def profile_step(self):
         ms = np.zeros(len(KERNEL_CLASSES))
         n = np.zeros(len(KERNEL_CLASSES), dtype=np.int32)

@@ -140,6 +140,10 @@ FUNCTIONS = {
     "echo_batch_set_schedule": (ctypes.c_int, [P, I, I]),
     "echo_batch_get_schedule": (ctypes.c_int, [P, I]),
     "echo_batch_autotune": (ctypes.c_int, [P, ctypes.c_int, D]),
+    "echo_batch_autotune_report": (ctypes.c_int, [P, D, ctypes.c_int, I]),
+    "echo_batch_set_tiles": (ctypes.c_int, [P, I]),
+    "echo_batch_set_mode": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int]),
+    "echo_batch_get_tuning": (ctypes.c_int, [P, I]),
     "echo_batch_profile_step": (ctypes.c_int, [P, D, I]),
 }
 

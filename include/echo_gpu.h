@@ -554,11 +554,34 @@ int echo_batch_set_stop(EchoBatch* b, int freeze_type, double temp_end);
  * order in which the tile lists visit the events. */
 int echo_batch_set_schedule(EchoBatch* b, const int* ctas, const int* order);
 int echo_batch_get_schedule(const EchoBatch* b, int* ctas);
-/* Times the candidate launch shapes of every slot on the current state
- * (the face sweeps and the first-stage update are re-run `reps` times per
- * candidate; the state and every event's scalars are restored) and keeps
- * the fastest; ms[slot] = its time per launch.  Synchronises. */
+/* The autotuner: on the current state (the state and every event's scalars
+ * are restored afterwards) it times, per slot, every tile length (128, 256,
+ * 512 faces or cells per tile) with every launch shape (one CTA per tile,
+ * or 1..occupancy CTAs per SM persistent), keeps the fastest (the cell
+ * list takes the update's tile), and then times whole first stages run
+ * both ways -- one launch per phase, and one cooperative launch per stage
+ * with 1..occupancy CTAs per SM -- keeping the faster (echo_batch_set_mode).
+ * ms[slot] = the chosen per-launch time of each slot.  Synchronises. */
 int echo_batch_autotune(EchoBatch* b, int reps, double* ms);
+/* Every candidate the last autotune timed, 4 doubles per row: what (slot
+ * 0..4, or 5 = a whole stage), shape (the tile length; for a stage 0 =
+ * phased, 1 = cooperative), CTAs (0 = one per tile), ms.  *n = rows (the
+ * first `cap` are copied). */
+int echo_batch_autotune_report(const EchoBatch* b, double* rows, int cap, int* n);
+/* Tile lengths of the x, y, z face lists and the cell list (multiples of
+ * 128, at most 1024); drops the step graphs. */
+int echo_batch_set_tiles(EchoBatch* b, const int* tiles);
+/* How a stage runs: mode 0 = one launch per phase (stage begin, face
+ * sweeps, per-event scalars, update, repair, smoothing); mode 1 = one
+ * cooperative launch per stage running those phases with grid-wide
+ * barriers between them (all CTAs resident; every barrier wait is bounded
+ * and a timeout ends the launch, reported by echo_batch_sync as
+ * ECHO_ERR_TIMEOUT), grid CTAs (0 = the most that are resident; WENO5
+ * reconstruction only).  Drops the step graphs. */
+int echo_batch_set_mode(EchoBatch* b, int mode, int grid);
+/* out[7]: tile lengths (x, y, z faces, cells), mode, cooperative grid
+ * (0 = all resident), 1 when steps run as CUDA graphs. */
+int echo_batch_get_tuning(const EchoBatch* b, int* out);
 /* one step with per-phase CUDA-event timing, like echo_gpu_profile_step */
 int echo_batch_profile_step(EchoBatch* b, double* ms, int* launches);
 

@@ -97,6 +97,65 @@ def test_batch_launch_shapes_do_not_change_results(small):
     assert np.array_equal(v0, v1) and np.array_equal(u0, u1), b.get_schedule()
 
 
+def test_tiles_and_one_launch_per_stage_do_not_change_results(small):
+    """Tile lengths of 256 and 512 faces or cells, and the whole stage as one
+    cooperative launch (all phases, grid-wide barriers between them) with the
+    largest resident grid and with one CTA per SM, give the bits of the
+    default one-launch-per-phase run."""
+    es, v, _ = small
+    ref = _batch(es, v, exact=True)
+    ref.run(5)
+    v0, u0 = ref.download()
+    for tiles, mode, grid in [((256, 512), 0, 0), ((512, 256), 0, 0), ((128, 128), 1, 0), ((256, 256), 1, 148),
+                              ((512, 128), 1, 0)]:
+        b = _batch(es, v, exact=True)
+        b.set_tiles(*tiles)
+        b.set_mode(mode, grid)
+        b.run(5)
+        b.sync()
+        v1, u1 = b.download()
+        assert np.array_equal(v0, v1) and np.array_equal(u0, u1), (tiles, mode, grid, b.tuning())
+        assert b.tuning()["mode"] == ("cooperative" if mode else "phased")
+
+
+def test_cooperative_batch_matches_oracle_to_the_end(small):
+    """Every event run to tmax with one launch per stage meets the oracle
+    running it alone, step count and state."""
+    es, v, ref = small
+    b = _batch(es, v, exact=True)
+    b.set_mode(1)
+    b.run_to_end(chunk=4)
+    b.sync()
+    st = b.status()
+    vg, ug = b.download()
+    for e, (vs, us) in enumerate(zip(b.split(vg), b.split(ug))):
+        vo, uo, n, err = ref[e]
+        assert st[e]["state"] == DONE and st[e]["steps"] == n, (e, st[e], n)
+        assert rel_linf(vs, vo, b.nv) <= 1e-13 and rel_linf(us, uo, b.nv) <= 1e-13
+
+
+def test_autotune_search_space_and_choice(small):
+    """The autotuner times every tile length with every launch shape per
+    slot and both ways of running a stage, reports them, and its choice
+    changes no bit."""
+    es, v, _ = small
+    ref = _batch(es, v, exact=False)
+    ref.run(5)
+    v0, u0 = ref.download()
+    b = _batch(es, v, exact=False)
+    b.run(1)
+    b.autotune(reps=2)
+    rows = b.autotune_report()
+    upd = [r for r in rows if r["slot"] == "update"]
+    assert {r["tile"] for r in upd} == {128, 256, 512}
+    stages = [r for r in rows if r["slot"] == "stage"]
+    assert {r["mode"] for r in stages} == {"phased", "cooperative"}
+    print(b.tuning(), min(stages, key=lambda r: r["ms"]))
+    b.run(4)
+    v1, u1 = b.download()
+    assert np.array_equal(v0, v1) and np.array_equal(u0, u1), b.tuning()
+
+
 def test_crashed_event_is_abandoned_alone(small):
     """A 3x3 block of negative conserved energy in event 1: the inversion
     and its neighbour-average repair fail (reference code 1,
@@ -129,9 +188,11 @@ def test_crashed_event_is_abandoned_alone(small):
         assert rel_linf(vs, ref[e][0], b.nv) <= 1e-13
 
 
-def test_batch_of_hydro_and_mhd_events():
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_of_hydro_and_mhd_events(mode):
     """The batch runs every equation set: ideal hydro (2+1D) and ideal RMHD
-    with GLM cleaning (3+1D events)."""
+    with GLM cleaning (3+1D events: three face lists), one launch per phase
+    or per stage."""
     for base, ns in [(P.config0(), (9, 12, 7)), (P.config1(), (7, 9, 8))]:
         es = EV.small_events(ns=ns, bs=(3.0, 7.0, 5.0), base=base, tmax=0.41 if base.mhd else 0.8,
                              maxdt=base.maxdt if base.mhd else 1.0)
@@ -144,6 +205,7 @@ def test_batch_of_hydro_and_mhd_events():
             vs.append(I.primitives(cfg, tab, b=float(es.b[e])))
         es.grid = lambda e, g=grids: g[e]
         b = _batch(es, vs, exact=True)
+        b.set_mode(mode)
         b.run_to_end(chunk=4)
         st = b.status()
         vg, _ = b.download()
