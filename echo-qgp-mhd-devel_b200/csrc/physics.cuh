@@ -81,9 +81,13 @@ struct DevPhys {
   double sigma_el, sigma_chiral;  // resistive runs: conductivities (code units)
 };
 
-// metric (system_metric_*, system.f90:132-160), derived from t on device
+// metric (system_metric_*, system.f90:132-160), derived from t on device.
+// g_11 = g_22 = 1 in both coordinate systems of the reference (Minkowski
+// and Bjorken), so they are compile-time ones: x * 1.0 is exactly x, and
+// the multiplications the reference writes with them drop out.
 struct Metric {
-  double g1, g2, g3, gp, gm, g0, t, t3, ig3;
+  static constexpr double g1 = 1.0, g2 = 1.0;
+  double g3, gp, gm, g0, t, t3, ig3;
 };
 
 __device__ __forceinline__ Metric make_metric(int coordinates, double t, double t3) {
@@ -92,13 +96,11 @@ __device__ __forceinline__ Metric make_metric(int coordinates, double t, double 
   m.t = t;
   m.t3 = t3;
   if (coordinates == ECHO_BJORKEN) {
-    m.g1 = 1.;
-    m.g2 = 1.;
     m.g3 = t * t;
     m.gp = t;
     m.gm = 1. / m.gp;
   } else {
-    m.g1 = m.g2 = m.g3 = 1.;
+    m.g3 = 1.;
     m.gp = 1.;
     m.gm = 1.;
   }
@@ -391,24 +393,29 @@ __device__ __forceinline__ double mp5(double f, double f1, double f2, double f3,
 // dl, dr >= 3e-24 and stay far below 1e150 for the values a run holds.
 __device__ __forceinline__ void weno5_nd(double f1, double f2, double f3, double f4, double f5, double& num,
                                          double& den) {
-  const double eps = 1.e-6, r12 = 1. / 12.;
+  // The smoothness indicators beta_k / 12 + eps = 13/12 t1^2 + 1/4 t2^2 + eps
+  // as two fused multiply-adds each, the sub-stencil polynomials with the
+  // factor 1/8 and the linear weights 10 and 5 of p2 and p3 folded into their
+  // (exactly representable) coefficients, and the denominator sum_k d_k Q_j Q_l
+  // with d = (1, 10, 5): the same weights with fewer FP64 instructions.
+  const double eps = 1.e-6, c13 = 13. / 12.;
   double t1, t2, q1, q2, q3;
   t1 = f3 - 2 * f2 + f1;
-  t2 = 3. * f3 - 4. * f2 + f1;
-  q1 = (13. * (t1 * t1) + 3. * (t2 * t2)) * r12 + eps;
+  t2 = fma(3., f3, fma(-4., f2, f1));
+  q1 = fma(c13 * t1, t1, fma(0.25 * t2, t2, eps));
   t1 = f4 - 2 * f3 + f2;
   t2 = f4 - f2;
-  q2 = (13. * (t1 * t1) + 3. * (t2 * t2)) * r12 + eps;
+  q2 = fma(c13 * t1, t1, fma(0.25 * t2, t2, eps));
   t1 = f5 - 2 * f4 + f3;
-  t2 = f5 - 4. * f4 + 3. * f3;
-  q3 = (13. * (t1 * t1) + 3. * (t2 * t2)) * r12 + eps;
+  t2 = fma(3., f3, fma(-4., f4, f5));
+  q3 = fma(c13 * t1, t1, fma(0.25 * t2, t2, eps));
   double Q1 = q1 * q1, Q2 = q2 * q2, Q3 = q3 * q3;
-  double w1 = Q2 * Q3, w2 = 10. * (Q1 * Q3), w3 = 5. * (Q1 * Q2);
-  double p1 = (3. * f1 - 10. * f2 + 15. * f3) * 0.125;
-  double p2 = (-f2 + 6. * f3 + 3. * f4) * 0.125;
-  double p3 = (3. * f3 + 6. * f4 - f5) * 0.125;
-  num = w1 * p1 + w2 * p2 + w3 * p3;
-  den = w1 + w2 + w3;
+  double w1 = Q2 * Q3, w2 = Q1 * Q3, w3 = Q1 * Q2;
+  double p1 = fma(1.875, f3, fma(-1.25, f2, 0.375 * f1));       // (3 f1 - 10 f2 + 15 f3) / 8
+  double p2 = fma(3.75, f4, fma(7.5, f3, -1.25 * f2));          // 10 (-f2 + 6 f3 + 3 f4) / 8
+  double p3 = fma(-0.625, f5, fma(3.75, f4, 1.875 * f3));       // 5 (3 f3 + 6 f4 - f5) / 8
+  num = fma(w3, p3, fma(w2, p2, w1 * p1));
+  den = fma(5., w3, fma(10., w2, w1));
 }
 __device__ __forceinline__ void weno5_face(const double s[6], double& gl, double& gr) {
   double nl, dl, nr, dr;

@@ -141,8 +141,6 @@ extern "C" int echo_gpu_test_c2p(const EchoParams* p, const double* eos_table, i
   P.glm_alpha = p->glm_alpha;
   Metric M;
   M.g0 = -1.;
-  M.g1 = 1.;
-  M.g2 = 1.;
   M.g3 = g3;
   M.gp = gp;
   M.gm = 1. / gp;
@@ -251,8 +249,6 @@ extern "C" int echo_gpu_test_c2p_seeded(const EchoParams* p, const double* eos_t
   }
   Metric M;
   M.g0 = -1.;
-  M.g1 = 1.;
-  M.g2 = 1.;
   M.g3 = g3;
   M.gp = gp;
   M.gm = 1. / gp;
