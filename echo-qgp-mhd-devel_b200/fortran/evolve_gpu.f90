@@ -27,6 +27,16 @@ module evolve_gpu
     real(c_double) :: sigma_el, sigma_chiral   ! sigma_el_cond, sigma_chiral_cond (resistive runs)
   end type echo_params
 
+  ! init()'s GLAUBER_GEOMETRIC parameters (echo_gpu_optical_glauber)
+  type, bind(C) :: echo_optical_glauber
+    real(c_double) :: mass_number, radius, delta, roze   ! projmass, radius, delta, roze of nuclear_data.dat
+    real(c_double) :: sigma_in                           ! fm^2 (SIGMA_IN/10)
+    real(c_double) :: ah, bimpact, ecenter, rhocenter
+    real(c_double) :: dr, dz1, acc                       ! thickness table steps and accuracy
+    real(c_double) :: deta, sigeta                       ! 3+1D plateau and Gaussian width of H(eta)
+    real(c_double) :: sqrt_s, nucleon_mass               ! gamma_col = sqrt_s / (2 m)
+  end type echo_optical_glauber
+
   type(c_ptr), save :: echo_ctx = c_null_ptr
 
   interface
@@ -180,6 +190,24 @@ module evolve_gpu
       type(c_ptr), value :: buf
       integer(c_size_t), value :: nbytes
       integer(c_int), intent(out) :: iout
+    end function
+
+    ! init()'s optical Glauber branch on the device: the state is uploaded at t
+    integer(c_int) function echo_gpu_optical_glauber(ctx, g, t, check_mass, max_e) &
+        bind(C, name="echo_gpu_optical_glauber")
+      import :: c_int, c_ptr, c_double, echo_optical_glauber
+      type(c_ptr), value :: ctx
+      type(echo_optical_glauber), intent(in) :: g
+      real(c_double), value :: t
+      real(c_double), intent(out) :: check_mass, max_e
+    end function
+
+    ! the fused stage kernel on (1) or off (0); info(7) receives the choice
+    integer(c_int) function echo_gpu_set_stage(ctx, fused, tx, ty, zseg, info) bind(C, name="echo_gpu_set_stage")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: fused, tx, ty, zseg
+      integer(c_int), intent(out) :: info(7)
     end function
 
     ! learned con2prim seed (ALG_SOLV = 101): weights(ECHO_MLP_NWEIGHTS) and
