@@ -56,6 +56,9 @@ struct EchoCtx {
   // [1 - on] = vold / uold
   int keep_old, kold, on;
   double *d_oldv[2], *d_oldu[2];
+  // product build: how the face sweeps run: 0 one thread per face, 8 or 16
+  // the cell-centred kernel in segments of that many cells
+  int face_mode;
   // the fused stage kernel (stage.cuh): usable, on, tile, segment, launch
   int st_ok, st_on, st_tx, st_ty, st_zseg, st_nt;
   unsigned st_grid;

@@ -152,6 +152,11 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
   return ECHO_OK;
 }
 
+// how the product build's face sweeps run (echo_gpu_set_faces)
+#ifndef ECHO_FACE_MODE
+#define ECHO_FACE_MODE 0
+#endif
+
 #define DISPATCH(c, fn, ...)                                      \
   do {                                                            \
     switch ((c)->kind) {                                          \
@@ -407,7 +412,12 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->out_bytes = 0;
   c->d_out_err = nullptr;
   c->kold = p->mhd ? 8 : 5;  // krh..kvold_end: kbz with MHD, kpr without (common.f90:378-386)
-  // the fused stage kernel, when the run allows it (else the sweep kernels)
+#ifdef ECHO_EXACT
+  c->face_mode = 0;  // the parity build keeps the reference's face-by-face arithmetic
+#else
+  c->face_mode = ECHO_FACE_MODE;
+#endif
+  // the fused stage kernel: tile chosen here, off until echo_gpu_set_stage
   DISPATCH(c, setup_stage, c, 0, 0, 0);
   c->st_on = 0;
   (void)cudaGetLastError();
@@ -884,6 +894,22 @@ int echo_gpu_profile_step(EchoCtx* c, double* ms, int* launches) {
   }
   for (auto& m : marks) cudaEventDestroy(m.second);
   cudaEventDestroy(start);
+  return ECHO_OK;
+}
+
+int echo_gpu_set_faces(EchoCtx* c, int mode) {
+  if (!c || (mode != 0 && mode != 8 && mode != 16)) return ECHO_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+#ifdef ECHO_EXACT
+  c->face_mode = 0;
+#else
+  c->face_mode = mode;
+#endif
+  for (int i = 0; i < 16; i++)
+    if (c->graph_ok[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph_ok[i] = false;
+    }
   return ECHO_OK;
 }
 

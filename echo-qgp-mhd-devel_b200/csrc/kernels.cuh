@@ -426,6 +426,180 @@ __global__ void ECHO_FACE_BOUNDS(KIND) faces_kernel(FaceArgs A) {
   block_max_atomic(amax_local, &A.sc->amax_bits[DIR], red);
 }
 
+#ifndef ECHO_EXACT
+// ---------------------------------------------------------------------------
+// Face sweep by cell-centred reconstruction (product build, WENO5).  One lane
+// per cell: a lane reconstructs both face states of its cell at once
+// (weno5_cell: the cell's three smoothness indicators serve the face above
+// and the face below), then takes the upper-face state of the cell below it
+// from the neighbouring lane (__shfl_up_sync) and computes the flux of the
+// face between the two.  The arithmetic after reconstruction is face_tail's,
+// as in faces_kernel.
+//
+// A warp covers segments of L consecutive cells along the sweep; the first
+// cell of a segment only feeds the face above it, so a segment yields L - 1
+// faces and consecutive segments overlap by one cell.  The 32 / L segments of
+// a warp lie side by side across the sweep so that every load touches whole
+// sectors: for the x-sweep L lanes run along x (W = 32 / L pencils per warp);
+// for the y- and eta-sweeps W = 32 / L consecutive x columns, each L cells
+// along the sweep (lane = x-offset + W * position).
+// ---------------------------------------------------------------------------
+template <int KIND, int DIR, int L>
+__global__ void ECHO_FACE_BOUNDS(KIND) faces_seg_kernel(FaceArgs A) {
+  typedef Traits<KIND> T;
+  constexpr int NV = T::NV;
+  constexpr int W = 32 / L;
+  constexpr int DELTA = DIR == 0 ? 1 : W;  // lane of the cell below
+  __shared__ double red[4];
+  const Grid& g = A.g;
+  const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
+  const int nseg = (n + 1 + L - 2) / (L - 1);  // segments covering faces 0..n
+  const int lane = threadIdx.x & 31;
+  const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int s = DIR == 0 ? lane % L : lane / W;  // position in the segment
+  int seg, a, b;                                 // segment; transverse indices (0-based)
+  bool valid;
+  size_t base;
+  long long stride;
+  if (DIR == 0) {
+    const long long ntr = (long long)g.ny * g.nz;
+    seg = (int)(wid % nseg);
+    const long long p = (wid / nseg) * W + lane / L;
+    valid = p < ntr;
+    a = (int)(p % g.ny);
+    b = (int)(p / g.ny);
+    base = ((size_t)b * g.ny + a) * g.nx;
+    stride = 1;
+  } else {
+    const int nxg = (g.nx + W - 1) / W;
+    const int nbt = DIR == 1 ? g.nz : g.ny;
+    const long long xg = wid % nxg;
+    const long long r = wid / nxg;
+    seg = (int)(r % nseg);
+    b = (int)(r / nseg);
+    a = (int)(xg * W + lane % W);
+    valid = a < g.nx && b < nbt;
+    base = DIR == 1 ? (size_t)b * g.ny * g.nx + a : (size_t)b * g.nx + a;
+    stride = DIR == 1 ? (long long)g.nx : (long long)g.nx * g.ny;
+  }
+  const int c = seg * (L - 1) - 1 + s;  // this lane's cell (0-based, -1..n are used)
+  valid = valid && c <= n;
+  const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
+  double plus[NV], minus[NV], ctr[4], wplus[4], wminus[4];
+#pragma unroll
+  for (int k = 0; k < NV; k++) plus[k] = minus[k] = 0.;
+#pragma unroll
+  for (int q = 0; q < 4; q++) ctr[q] = wplus[q] = wminus[q] = 0.;
+  if (valid) {
+    // the stencil v(c-2..c+2) of cell c: 1-based pencil positions c-1..c+3
+    long long off[5];
+    double sg[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      int qq;
+      map_ghost(c - 1 + q, n, A.bc.c[0][0], A.bc.c[0][1], qq, sg[q]);
+      off[q] = (long long)base + (long long)(qq - 1) * stride;
+    }
+    double sv[3][5];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      const double* vk = A.v + (size_t)k * g.ncell;
+      double s5[5];
+      if (A.bc_uniform) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) s5[q] = __ldg(vk + off[q]);
+        if (A.bc_signed) {
+#pragma unroll
+          for (int q = 0; q < 5; q++) s5[q] = sg[q] * s5[q];
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 5; q++) s5[q] = ghost_val(vk, base, stride, n, c - 1 + q, A.bc.c[k][0], A.bc.c[k][1]);
+      }
+      weno5_cell(s5[0], s5[1], s5[2], s5[3], s5[4], plus[k], minus[k]);
+      if (k >= KVX && k <= KPR) ctr[k - KVX] = s5[2];
+      if (T::VISC && k >= KVX && k <= KVZ) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) sv[k - KVX][q] = s5[q];
+      }
+    }
+    if (T::VISC) {
+      double s4[4][5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        double vx = sv[0][q], vy = sv[1][q], vz = sv[2][q];
+        double gg = 1. / sqrt(1. - vx * vx - vy * vy - M.g3 * (vz * vz));
+        s4[0][q] = gg;
+        s4[1][q] = gg * vx;
+        s4[2][q] = gg * vy;
+        s4[3][q] = gg * vz;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) weno5_cell(s4[q][0], s4[q][1], s4[q][2], s4[q][3], s4[q][4], wplus[q], wminus[q]);
+    }
+  }
+  // the cell below: its upper-face states and its centre (the fix-ups' w0)
+  double wl[NV], w0[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    wl[k] = __shfl_up_sync(0xffffffffu, plus[k], DELTA);
+    w0[k] = 0.;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) w0[KVX + q] = __shfl_up_sync(0xffffffffu, ctr[q], DELTA);
+  if (T::VISC) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) wplus[q] = __shfl_up_sync(0xffffffffu, wplus[q], DELTA);
+  }
+  double amax_local = 0.0;
+  if (valid && s >= 1) {
+    // face c, between cells c-1 and c
+    const size_t nfaces = faces_of<DIR>(g);
+    size_t fid;
+    if (DIR == 0)
+      fid = ((size_t)b * g.ny + a) * (g.nx + 1) + c;
+    else if (DIR == 1)
+      fid = ((size_t)b * (g.ny + 1) + c) * g.nx + a;
+    else
+      fid = ((size_t)c * g.ny + b) * g.nx + a;
+    if (T::VISC) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        A.WD[(size_t)q * nfaces + fid] = wplus[q];
+        A.WD[(size_t)(4 + q) * nfaces + fid] = wminus[q];
+      }
+    }
+    double F[NV];
+    int err = face_tail<KIND, DIR>(A.P, M, A.sc->glm_ch_old, wl, minus, w0, F, amax_local);
+    if (err) {
+      amax_local = 0.0;
+      size_t cell = base + (size_t)((c >= 1 ? c : 1) - 1) * stride;
+      atomicMin(&A.sc->err_key, ((unsigned long long)cell << 20) | (unsigned long long)err);
+#pragma unroll
+      for (int k = 0; k < NV; k++) A.F[(size_t)k * nfaces + fid] = 0.0;
+    } else {
+#pragma unroll
+      for (int k = 0; k < NV; k++) A.F[(size_t)k * nfaces + fid] = F[k];
+      // GLM speed of the reference: the last face of the last pencil (work.f90:217,310,401)
+      const int na = DIR == 0 ? g.ny : g.nx;
+      const int nb = DIR == 2 ? g.ny : g.nz;
+      if (c == n && a == na - 1 && b == nb - 1) A.sc->aflux[DIR] = amax_local;
+    }
+  }
+  block_max_atomic(amax_local, &A.sc->amax_bits[DIR], red);
+}
+
+// warps of faces_seg_kernel<DIR, L> for grid g
+template <int DIR, int L>
+__host__ __device__ inline long long seg_warps(const Grid& g) {
+  constexpr int W = 32 / L;
+  const int n = DIR == 0 ? g.nx : DIR == 1 ? g.ny : g.nz;
+  const long long nseg = (n + 1 + L - 2) / (L - 1);
+  if (DIR == 0) return nseg * (((long long)g.ny * g.nz + W - 1) / W);
+  return (long long)((g.nx + W - 1) / W) * nseg * (DIR == 1 ? g.nz : g.ny);
+}
+#endif
+
 // ---------------------------------------------------------------------------
 // scalar logic of evolve_main (evolve.f90:156-201) and evolve_dt (:723-764)
 // ---------------------------------------------------------------------------

@@ -24,6 +24,22 @@ void launch_faces(EchoCtx* c, int dir) {
   A.sc = c->d_sc;
   A.coordinates = c->p.coordinates;
   unsigned blocks = (unsigned)((c->nfaces[dir] + 127) / 128);
+#ifndef ECHO_EXACT
+  // product build: the cell-centred sweep in segments of face_mode cells
+  if (c->p.recal == ECHO_REC_WENO5 && c->face_mode > 0) {
+    const Grid& g = c->g;
+    if (c->face_mode == 8) {
+      if (dir == 0) faces_seg_kernel<KIND, 0, 8><<<(unsigned)((seg_warps<0, 8>(g) + 3) / 4), 128, 0, c->stream>>>(A);
+      if (dir == 1) faces_seg_kernel<KIND, 1, 8><<<(unsigned)((seg_warps<1, 8>(g) + 3) / 4), 128, 0, c->stream>>>(A);
+      if (dir == 2) faces_seg_kernel<KIND, 2, 8><<<(unsigned)((seg_warps<2, 8>(g) + 3) / 4), 128, 0, c->stream>>>(A);
+    } else {
+      if (dir == 0) faces_seg_kernel<KIND, 0, 16><<<(unsigned)((seg_warps<0, 16>(g) + 3) / 4), 128, 0, c->stream>>>(A);
+      if (dir == 1) faces_seg_kernel<KIND, 1, 16><<<(unsigned)((seg_warps<1, 16>(g) + 3) / 4), 128, 0, c->stream>>>(A);
+      if (dir == 2) faces_seg_kernel<KIND, 2, 16><<<(unsigned)((seg_warps<2, 16>(g) + 3) / 4), 128, 0, c->stream>>>(A);
+    }
+    return;
+  }
+#endif
   if (c->p.recal == ECHO_REC_WENO5) {
     if (dir == 0) faces_kernel<KIND, 0, ECHO_REC_WENO5><<<blocks, 128, 0, c->stream>>>(A);
     if (dir == 1) faces_kernel<KIND, 1, ECHO_REC_WENO5><<<blocks, 128, 0, c->stream>>>(A);

@@ -417,6 +417,43 @@ __device__ __forceinline__ void weno5_nd(double f1, double f2, double f3, double
   num = fma(w3, p3, fma(w2, p2, w1 * p1));
   den = fma(5., w3, fma(10., w2, w1));
 }
+// Cell-centred WENO5 (product build): both face states of one cell from its
+// five-point stencil f1..f5 = v(c-2..c+2).  plus = the state at c+1/2 (the
+// left state of the face above, holib.f90:198-212 on f1..f5), minus = the
+// state at c-1/2 (the right state of the face below, the same formula on
+// f5..f1).  The two orientations share their three smoothness indicators
+// (the reversed stencil's first is the forward stencil's third) and the
+// three products of the weights, and one division serves both.
+__device__ __forceinline__ void weno5_cell(double f1, double f2, double f3, double f4, double f5, double& plus,
+                                           double& minus) {
+  const double eps = 1.e-6, c13 = 13. / 12.;
+  double t1, t2;
+  t1 = f3 - 2 * f2 + f1;
+  t2 = fma(3., f3, fma(-4., f2, f1));
+  const double qa = fma(c13 * t1, t1, fma(0.25 * t2, t2, eps));
+  t1 = f4 - 2 * f3 + f2;
+  t2 = f4 - f2;
+  const double qb = fma(c13 * t1, t1, fma(0.25 * t2, t2, eps));
+  t1 = f5 - 2 * f4 + f3;
+  t2 = fma(3., f3, fma(-4., f4, f5));
+  const double qc = fma(c13 * t1, t1, fma(0.25 * t2, t2, eps));
+  const double Qa = qa * qa, Qb = qb * qb, Qc = qc * qc;
+  const double wbc = Qb * Qc, wac = Qa * Qc, wab = Qa * Qb;
+  // forward: weights (wbc, 10 wac, 5 wab); reversed: (wab, 10 wac, 5 wbc)
+  const double p1 = fma(1.875, f3, fma(-1.25, f2, 0.375 * f1));
+  const double p2 = fma(3.75, f4, fma(7.5, f3, -1.25 * f2));
+  const double p3 = fma(-0.625, f5, fma(3.75, f4, 1.875 * f3));
+  const double r1 = fma(1.875, f3, fma(-1.25, f4, 0.375 * f5));
+  const double r2 = fma(3.75, f2, fma(7.5, f3, -1.25 * f4));
+  const double r3 = fma(-0.625, f1, fma(3.75, f2, 1.875 * f3));
+  const double np = fma(wab, p3, fma(wac, p2, wbc * p1));
+  const double dp = fma(5., wab, fma(10., wac, wbc));
+  const double nm = fma(wbc, r3, fma(wac, r2, wab * r1));
+  const double dm = fma(5., wbc, fma(10., wac, wab));
+  const double inv = 1. / (dp * dm);
+  plus = np * dm * inv;
+  minus = nm * dp * inv;
+}
 __device__ __forceinline__ void weno5_face(const double s[6], double& gl, double& gr) {
   double nl, dl, nr, dr;
   weno5_nd(s[0], s[1], s[2], s[3], s[4], nl, dl);

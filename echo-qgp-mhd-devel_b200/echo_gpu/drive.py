@@ -59,6 +59,9 @@ def main():
     ap.add_argument("--stage", default="auto", choices=["auto", "fused", "sweeps"],
                     help="fused stage kernel or the sweep kernels (auto: the library's default)")
     ap.add_argument("--tile", default="", help="fused stage tile tx,ty,zseg (0 = chosen for the grid)")
+    ap.add_argument("--faces", type=int, default=-1, choices=[-1, 0, 8, 16],
+                    help="product build face sweeps: 0 one thread per face, 8/16 cell-centred segments "
+                         "(-1: the library's default)")
     a = ap.parse_args()
     if a.config == "batch":
         run_batch(a)
@@ -87,6 +90,8 @@ def main():
         tx, ty, zs = (int(x) for x in a.tile.split(",")) if a.tile else (0, 0, 0)
         info = ev.set_stage(a.stage != "sweeps", tx, ty, zs)
         print(f"stage: {info}")
+    if a.faces >= 0:
+        ev.set_faces(a.faces)
     ev.upload(I.primitives(cfg, tab), None, cfg.tstart)
     t0 = time.perf_counter()
     ev.run(a.steps)

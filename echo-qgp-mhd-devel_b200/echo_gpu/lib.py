@@ -103,6 +103,7 @@ FUNCTIONS = {
     "echo_gpu_get_state": (ctypes.c_int, [P, P, P]),
     "echo_gpu_profile_step": (ctypes.c_int, [P, D, I]),
     "echo_gpu_set_stage": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, I]),
+    "echo_gpu_set_faces": (ctypes.c_int, [P, ctypes.c_int]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
@@ -288,6 +289,12 @@ class Evolve:
         n = np.zeros(len(self.KERNEL_CLASSES), dtype=np.int32)
         self._check(self.lib.echo_gpu_profile_step(self.h, _dp(ms), _ip(n)), "profile_step")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def set_faces(self, mode: int):
+        """Product build: how the WENO5 face sweeps run -- 0 one thread per
+        face (the default), 8 or 16 cell-centred segments of that many
+        cells."""
+        self._check(self.lib.echo_gpu_set_faces(self.h, mode), "set_faces")
 
     def set_stage(self, fused: bool = True, tx: int = 0, ty: int = 0, zseg: int = 0) -> dict:
         """Fused stage kernel on or off (and its tile); returns the choice."""

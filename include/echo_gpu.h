@@ -333,12 +333,28 @@ int echo_gpu_hyp_get(EchoCtx* ctx, double* out);
  * run. */
 int echo_gpu_profile_step(EchoCtx* ctx, double* ms, int* launches);
 
+/* No counterpart in the reference (an execution option).  How the product
+ * build (libechogpu.so) computes the WENO5 face sweeps:
+ *   mode 0   one thread per face, both face states in one thread (the
+ *            default; the reference's arrangement, which the parity build
+ *            always runs);
+ *   mode 8, 16  one thread per cell, in segments of that many cells along
+ *            the sweep: a thread reconstructs both face states of its cell
+ *            from one set of WENO5 smoothness indicators and takes the
+ *            state of the cell below from its neighbouring lane, so a
+ *            segment yields mode - 1 faces.
+ * All meet the oracle at the product build's tolerance.  Other
+ * reconstructions always run mode 0.  ECHO_ERR_ARG for other modes.
+ * Synchronises the stream and drops the step graphs. */
+int echo_gpu_set_faces(EchoCtx* ctx, int mode);
+
 /* No counterpart in the reference (an execution option).  How a stage runs:
- * fused = 1 (the default wherever the run allows it) runs the three sweeps,
+ * fused = 1 (where the run allows it) runs the three sweeps,
  * the flux divergence, the sources, the update and con2prim of a stage in
  * one kernel over x-y tiles of tx x ty cells marching through eta segments
  * of zseg planes, with no face flux in global memory; fused = 0 runs the
- * sweep kernels and the update kernel.  The first stage of an explicit RK
+ * sweep kernels and the update kernel (the default: the sweeps are faster
+ * on the benchmarked grids).  The first stage of an explicit RK
  * step without divergence cleaning always runs the sweeps (its dt needs
  * every face's signal speed before any update).  tx, ty, zseg = 0 choose
  * the tile and segment for this grid.  Both give the same results within
