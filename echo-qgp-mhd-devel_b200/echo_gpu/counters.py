@@ -2,9 +2,10 @@
 of one launch of each kernel class, as ncu measured them, tied to the
 sources they were measured on.
 
-    python -m echo_gpu.counters <report.ncu-rep> <out.json> --workload NAME
+    python -m echo_gpu.counters <report.ncu-rep | raw.csv> <out.json> --workload NAME
 
-reads the raw page of an ncu report (metrics dfma/dadd/dmul thread
+reads the raw page of an ncu report, or that page exported beforehand with
+``ncu -i report --page raw --csv`` (metrics dfma/dadd/dmul thread
 instructions, dram bytes, duration) and writes one record per kernel class
 (faces_x/y/z, update_c2p, stage_fused) with the build hash of the CUDA
 sources; ``load`` returns the records and whether they belong to the sources
@@ -50,8 +51,12 @@ def kernel_class(name: str) -> str | None:
 
 
 def parse(report: str) -> dict:
-    out = subprocess.run(["ncu", "-i", report, "--page", "raw", "--csv"], check=True, capture_output=True,
-                         text=True).stdout
+    if report.endswith(".csv"):
+        with open(report) as fh:
+            out = fh.read()
+    else:
+        out = subprocess.run(["ncu", "-i", report, "--page", "raw", "--csv"], check=True, capture_output=True,
+                             text=True).stdout
     rows = list(csv.reader(io.StringIO(out)))
     hdr = rows[0]
     units = dict(zip(hdr, rows[1]))
