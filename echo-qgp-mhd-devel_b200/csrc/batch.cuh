@@ -247,6 +247,7 @@ __global__ void __launch_bounds__(256) batch_repair_kernel(RepairArgs base, Batc
   if (B.state[e] != EV_LIVE || B.sc[e].nfail == 0) return;
   __shared__ RepairArgs sA;
   __shared__ int s_any, s_stop;
+  __shared__ unsigned s_list[ECHO_REPAIR_LIST];
   if (threadIdx.x == 0) {
     const EvDesc& d = B.ev[e];
     const size_t cv = (size_t)nv * d.cell;
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(256) batch_repair_kernel(RepairArgs base, Batc
     sA.sc = B.sc + e;
   }
   __syncthreads();
-  repair_grid<KIND>(sA, s_any, s_stop);
+  repair_grid<KIND, ECHO_REPAIR_LIST>(sA, s_any, s_stop, s_list);
 }
 
 // evolve_smooth_viscosity over the cell tiles of all live events
@@ -631,7 +632,7 @@ __global__ void __launch_bounds__(BATCH_NT, ECHO_BATCH_STAGE_MINB(KIND, SEED)) b
       sA.r.sc = B.sc + e;
     }
     __syncthreads();
-    repair_grid<KIND>(sA.r, s_any, s_stop);
+    repair_grid<KIND, 0>(sA.r, s_any, s_stop, nullptr);
     __syncthreads();
   }
   if (!S.smooth) return;

@@ -1218,15 +1218,158 @@ __device__ __forceinline__ double flat_u(const double* u, size_t tot, long long 
   return u[off];
 }
 
-// Called by every thread of one block; s_any and s_stop are block-shared.
+// The repair of one failed cell (evolve.f90:795-842): con2prim of the
+// failed state, the six-neighbour average of u in the reference's flat
+// addressing (flat_u), con2prim, the velocity and pressure fixes, prim2cons
+// and con2prim again.  The reference averages in place, so where a flat
+// neighbour is the same cell (2-D grids, whose eta offset nx*ny is one
+// variable's length) it reads the already averaged variable: un[] holds
+// those.  Returns whether the repaired state is valid; uu and vv receive the
+// conserved and primitive values to store.
 template <int KIND>
-__device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int& s_stop) {
+__device__ __noinline__ bool repair_cell(const RepairArgs& A, const Metric& M, double h, size_t cell, double* uu,
+                                         double* vv) {
+  typedef Traits<KIND> T;
+  const int NV = T::NV;
+  const Grid& g = A.g;
+  int it;
+  for (int k = 0; k < NV; k++) vv[k] = A.vold[(size_t)k * g.ncell + cell];
+  for (int k = 0; k < NV; k++) uu[k] = A.u[(size_t)k * g.ncell + cell];
+  (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
+  const size_t totu = g.ncell * NV;
+  const long long nx = g.nx, nxy = (long long)g.nx * g.ny;
+  double un[NV];
+  for (int k = 0; k < NV; k++) {
+    const long long o = (long long)k * g.ncell + (long long)cell;
+    const long long q[6] = {o - 1, o + 1, o - nx, o + nx, o - nxy, o + nxy};
+    double a[6];
+    for (int j = 0; j < 6; j++) {
+      a[j] = flat_u(A.u, totu, q[j]);
+      if (q[j] >= 0 && (size_t)q[j] < totu && (size_t)q[j] % g.ncell == cell) {
+        const int kq = (int)((size_t)q[j] / g.ncell);
+        if (kq < k) a[j] = un[kq];
+      }
+    }
+    un[k] = (a[0] + a[1] + a[2] + a[3] + a[4] + a[5]) / 6.;
+    uu[k] = un[k];
+  }
+  (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
+  double v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
+  if (v2 > 1) {
+    double fac = A.maxspeed / sqrt(v2);
+    vv[KVX] = fac * vv[KVX];
+    vv[KVY] = fac * vv[KVY];
+    vv[KVZ] = fac * vv[KVZ];
+  }
+  if (vv[KPR] < 0) {
+    long long o = (long long)KPR * g.ncell + (long long)cell;
+    double pxl = flat_v<KIND>(A, o - 1, cell), pxr = flat_v<KIND>(A, o + 1, cell);
+    double pyl = flat_v<KIND>(A, o - nx, cell), pyr = flat_v<KIND>(A, o + nx, cell);
+    double pzl = flat_v<KIND>(A, o - nxy, cell), pzr = flat_v<KIND>(A, o + nxy, cell);
+    vv[KPR] = (pxl + pxr + pyl + pyr + pzl + pzr) / 6.;
+  }
+  (void)prim2cons<KIND>(A.P, M, vv, uu);
+  (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
+  v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
+  return (vv[KPR] > 0) && (v2 < 1);
+}
+
+// Whether failed cell c reads another failed cell: its flat neighbours
+// c +- 1, c +- nx, c +- nx*ny of any variable (modulo the cell count).
+__device__ __forceinline__ bool repair_touches(const unsigned char* fail, const Grid& g, size_t c) {
+  const long long n = (long long)g.ncell;
+  const long long d[3] = {1, (long long)g.nx, (long long)g.nx * g.ny};
+  for (int j = 0; j < 3; j++) {
+    const long long dd = d[j] % n;
+    const long long lo = ((long long)c - dd + n) % n, hi = ((long long)c + dd) % n;
+    if ((lo != (long long)c && fail[lo]) || (hi != (long long)c && fail[hi])) return true;
+  }
+  return false;
+}
+
+// The repair of every failed cell of a grid.  The reference repairs them
+// one after another in cell order, each reading its neighbours' current u
+// and v, and stops at the first cell it cannot repair (the run crashes).
+// Called by every thread of one block; s_any and s_stop are block-shared.
+// s_list (CAP entries, block-shared; CAP may be 0) holds the failed cells in
+// order: when they fit and none reads another, their repairs do not depend
+// on each other, so the block repairs them in parallel, a round of
+// blockDim.x cells at a time in cell order, and stores what the sequential
+// loop would: every cell before the first failure in full, the failing cell's
+// u, nothing after it.  Otherwise thread 0 repairs them in order.
+template <int KIND, int CAP>
+__device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int& s_stop, unsigned* s_list) {
   typedef Traits<KIND> T;
   const int NV = T::NV;
   const Grid& g = A.g;
   const Metric M = make_metric(A.coordinates, A.sc->t, A.sc->t3);
   const double h = A.h_alpha * A.sc->dt;
-  if (threadIdx.x == 0) s_stop = 0;
+  __shared__ int s_n, s_conflict;
+  __shared__ int s_wc[32];
+  __shared__ unsigned s_crash;
+  if (threadIdx.x == 0) {
+    s_stop = 0;
+    s_n = 0;
+    s_conflict = CAP == 0 || g.ncell >= 0xffffffffull;
+  }
+  __syncthreads();
+  if (CAP > 0 && !s_conflict) {
+    // the failed cells in order, and whether any reads another
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    for (size_t chunk = 0; chunk < g.ncell; chunk += blockDim.x) {
+      const size_t c = chunk + threadIdx.x;
+      const bool f = c < g.ncell && A.fail[c];
+      if (f && repair_touches(A.fail, g, c)) s_conflict = 1;
+      const unsigned bal = __ballot_sync(0xffffffffu, f);
+      if (lane == 0) s_wc[w] = __popc(bal);
+      __syncthreads();
+      if (f) {
+        int pos = s_n + __popc(bal & ((1u << lane) - 1u));
+        for (int i = 0; i < w; i++) pos += s_wc[i];
+        if (pos < CAP) s_list[pos] = (unsigned)c;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int tot = 0;
+        for (int i = 0; i < nw; i++) tot += s_wc[i];
+        s_n += tot;
+      }
+      __syncthreads();
+    }
+  }
+  if (CAP > 0 && !s_conflict && s_n <= CAP) {
+    const int n = s_n;
+    for (int r = 0; r < n; r += blockDim.x) {
+      const int i = r + (int)threadIdx.x;
+      const bool mine = i < n;
+      const size_t cell = mine ? s_list[i] : 0;
+      double uu[NV], vv[NV];
+      bool ok = true;
+      if (mine) ok = repair_cell<KIND>(A, M, h, cell, uu, vv);
+      if (threadIdx.x == 0) s_crash = 0xffffffffu;
+      __syncthreads();
+      if (mine && !ok) atomicMin(&s_crash, (unsigned)cell);
+      __syncthreads();
+      const unsigned crash = s_crash;
+      if (mine && cell <= crash) {
+        atomicAdd(&A.sc->repairs, 1ull);
+        if (T::VISC && A.P.obtained_zz) A.vnew[(size_t)KPIZZ * g.ncell + cell] = vv[KPIZZ];
+        for (int k = 0; k < NV; k++) A.u[(size_t)k * g.ncell + cell] = uu[k];
+        if (cell < crash) {
+          for (int k = 0; k < NV; k++) A.vnew[(size_t)k * g.ncell + cell] = vv[k];
+        } else {
+          // the run crashes here (evolve.f90:836-858)
+          atomicMin(&A.sc->err_key, ((unsigned long long)cell << 20) | 1ull);
+        }
+      }
+      __syncthreads();  // every thread has read s_crash before the next round resets it
+      if (crash != 0xffffffffu) {
+        if (threadIdx.x == 0) s_stop = 1;
+        break;
+      }
+    }
+    return;
+  }
   for (size_t chunk = 0; chunk < g.ncell; chunk += blockDim.x) {
     size_t c = chunk + threadIdx.x;
     int f = (c < g.ncell) ? A.fail[c] : 0;
@@ -1243,38 +1386,7 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
         if (!A.fail[cell]) continue;
         A.sc->repairs++;
         double uu[NV], vv[NV];
-        int it;
-        for (int k = 0; k < NV; k++) vv[k] = A.vold[(size_t)k * g.ncell + cell];
-        for (int k = 0; k < NV; k++) uu[k] = A.u[(size_t)k * g.ncell + cell];
-        (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
-        size_t totu = g.ncell * NV;
-        long long nx = g.nx, nxy = (long long)g.nx * g.ny;
-        for (int k = 0; k < NV; k++) {
-          long long o = (long long)k * g.ncell + (long long)cell;
-          double s = flat_u(A.u, totu, o - 1) + flat_u(A.u, totu, o + 1) + flat_u(A.u, totu, o - nx) +
-                     flat_u(A.u, totu, o + nx) + flat_u(A.u, totu, o - nxy) + flat_u(A.u, totu, o + nxy);
-          A.u[o] = s / 6.;
-          uu[k] = A.u[o];
-        }
-        (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
-        double v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
-        if (v2 > 1) {
-          double fac = A.maxspeed / sqrt(v2);
-          vv[KVX] = fac * vv[KVX];
-          vv[KVY] = fac * vv[KVY];
-          vv[KVZ] = fac * vv[KVZ];
-        }
-        if (vv[KPR] < 0) {
-          long long o = (long long)KPR * g.ncell + (long long)cell;
-          double pxl = flat_v<KIND>(A, o - 1, cell), pxr = flat_v<KIND>(A, o + 1, cell);
-          double pyl = flat_v<KIND>(A, o - nx, cell), pyr = flat_v<KIND>(A, o + nx, cell);
-          double pzl = flat_v<KIND>(A, o - nxy, cell), pzr = flat_v<KIND>(A, o + nxy, cell);
-          vv[KPR] = (pxl + pxr + pyl + pyr + pzl + pzr) / 6.;
-        }
-        (void)prim2cons<KIND>(A.P, M, vv, uu);
-        (void)cons2prim<KIND, true>(A.P, M, A.algo, A.tol, uu, vv, &it, nullptr, nullptr, h);
-        v2 = vv[KVX] * vv[KVX] + vv[KVY] * vv[KVY] + vv[KVZ] * vv[KVZ] * M.g3;
-        bool ok = (vv[KPR] > 0) && (v2 < 1);
+        const bool ok = repair_cell<KIND>(A, M, h, cell, uu, vv);
         if (T::VISC && A.P.obtained_zz) A.vnew[(size_t)KPIZZ * g.ncell + cell] = vv[KPIZZ];
         for (int k = 0; k < NV; k++) A.u[(size_t)k * g.ncell + cell] = uu[k];
         if (!ok) {
@@ -1291,11 +1403,15 @@ __device__ __forceinline__ void repair_grid(const RepairArgs& A, int& s_any, int
   }
 }
 
+// failed cells a repair block can list (4 KiB of shared memory)
+#define ECHO_REPAIR_LIST 1024
+
 template <int KIND>
 __global__ void __launch_bounds__(256) repair_kernel(RepairArgs A) {
   if (A.sc->nfail == 0) return;
   __shared__ int s_any, s_stop;
-  repair_grid<KIND>(A, s_any, s_stop);
+  __shared__ unsigned s_list[ECHO_REPAIR_LIST];
+  repair_grid<KIND, ECHO_REPAIR_LIST>(A, s_any, s_stop, s_list);
 }
 
 // evolve_smooth_viscosity (evolve.f90:1159-1207)
