@@ -166,6 +166,7 @@ int echo_batch_init(const EchoParams* p, const double* eos_table, int n_eos, int
     d.g.ddx = q.nx > 1 ? 1. / dx : 0.;
     d.g.ddy = q.ny > 1 ? 1. / dy : 0.;
     d.g.ddz = q.nz > 1 ? 1. / dz : 0.;
+    set_grid_div(d.g);
     d.x1 = q.x1;
     d.y1 = q.y1;
     d.dx = dx;

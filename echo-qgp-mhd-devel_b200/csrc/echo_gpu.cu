@@ -360,6 +360,7 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->g.ddx = p->nx > 1 ? 1. / dx : 0.;
   c->g.ddy = p->ny > 1 ? 1. / dy : 0.;
   c->g.ddz = p->nz > 1 ? 1. / dz : 0.;
+  set_grid_div(c->g);
   echo_setup_bc(p, c->nv, c->bc, c->bc_uniform, c->bc_signed);
   c->nfaces[0] = (size_t)(p->nx + 1) * p->ny * p->nz;
   c->nfaces[1] = (size_t)p->nx * (p->ny + 1) * p->nz;

@@ -33,11 +33,44 @@ struct DevScalars {
   unsigned long long brackets;    // con2prim solves that fell back to the bracketed BRENTM
 };
 
+// Unsigned 32-bit division by a run-time invariant d >= 1 as a multiply-high,
+// a subtraction, an addition and two shifts (T. Granlund and P. L.
+// Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994, Fig. 4.1): with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1,
+// t = umulhi(m, n) and q = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0) is
+// floor(n / d) for every n < 2^32.
+struct FastDiv {
+  unsigned m;
+  unsigned char s1, s2;
+};
+__host__ __device__ inline FastDiv make_fastdiv(unsigned d) {
+  int l = 0;
+  while ((1ull << l) < (unsigned long long)d) l++;
+  FastDiv f;
+  f.m = (unsigned)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+  f.s1 = (unsigned char)(l > 0 ? 1 : 0);
+  f.s2 = (unsigned char)(l > 0 ? l - 1 : 0);
+  return f;
+}
+__device__ __forceinline__ unsigned fast_div(unsigned n, const FastDiv& f) {
+  const unsigned t = __umulhi(f.m, n);
+  return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+
 struct Grid {
   int nx, ny, nz;
   size_t ncell;
   double ddx, ddy, ddz;
+  // division by nx, ny, nx + 1 and ny + 1 of face and cell indices below
+  // 2^32 (set_grid_div)
+  FastDiv dnx, dny, dnx1, dny1;
 };
+__host__ __device__ inline void set_grid_div(Grid& g) {
+  g.dnx = make_fastdiv((unsigned)g.nx);
+  g.dny = make_fastdiv((unsigned)g.ny);
+  g.dnx1 = make_fastdiv((unsigned)g.nx + 1u);
+  g.dny1 = make_fastdiv((unsigned)g.ny + 1u);
+}
 
 // boundary codes for one sweep direction: bc[k][side]
 struct BcDir {
@@ -292,25 +325,47 @@ __device__ __forceinline__ double face_flux(const FaceArgs& A, size_t fid) {
     int i, a, b;  // face index along DIR, transverse coordinates (1-based)
     size_t base;
     long long stride;
-    if (DIR == 0) {
+    if (nfaces < (1ull << 32)) {  // multiply-high divisions (FastDiv)
+      const unsigned f = (unsigned)fid;
+      if (DIR == 0) {
+        const unsigned r = fast_div(f, g.dnx1), q = fast_div(r, g.dny);
+        i = (int)(f - r * (unsigned)(g.nx + 1));
+        a = (int)(r - q * (unsigned)g.ny) + 1;
+        b = (int)q + 1;
+      } else if (DIR == 1) {
+        const unsigned r = fast_div(f, g.dnx), q = fast_div(r, g.dny1);
+        a = (int)(f - r * (unsigned)g.nx) + 1;
+        i = (int)(r - q * (unsigned)(g.ny + 1));
+        b = (int)q + 1;
+      } else {
+        const unsigned r = fast_div(f, g.dnx), q = fast_div(r, g.dny);
+        a = (int)(f - r * (unsigned)g.nx) + 1;
+        b = (int)(r - q * (unsigned)g.ny) + 1;
+        i = (int)q;
+      }
+    } else if (DIR == 0) {
       i = (int)(fid % (g.nx + 1));
       size_t r = fid / (g.nx + 1);
       a = (int)(r % g.ny) + 1;
       b = (int)(r / g.ny) + 1;
-      base = ((size_t)(b - 1) * g.ny + (a - 1)) * g.nx;
-      stride = 1;
     } else if (DIR == 1) {
       a = (int)(fid % g.nx) + 1;
       size_t r = fid / g.nx;
       i = (int)(r % (g.ny + 1));
       b = (int)(r / (g.ny + 1)) + 1;
-      base = (size_t)(b - 1) * g.ny * g.nx + (a - 1);
-      stride = g.nx;
     } else {
       a = (int)(fid % g.nx) + 1;
       size_t r = fid / g.nx;
       b = (int)(r % g.ny) + 1;
       i = (int)(r / g.ny);
+    }
+    if (DIR == 0) {
+      base = ((size_t)(b - 1) * g.ny + (a - 1)) * g.nx;
+      stride = 1;
+    } else if (DIR == 1) {
+      base = (size_t)(b - 1) * g.ny * g.nx + (a - 1);
+      stride = g.nx;
+    } else {
       base = (size_t)(b - 1) * g.nx + (a - 1);
       stride = (long long)g.nx * g.ny;
     }
@@ -944,10 +999,17 @@ __device__ __forceinline__ void update_cell(const UpdateArgs& A, size_t c, bool 
   int ix = 0, iy = 0, iz = 0;
   double du[NV], dv[NDER];
   if (active) {
-    ix = (int)(c % g.nx);
-    size_t r = c / g.nx;
-    iy = (int)(r % g.ny);
-    iz = (int)(r / g.ny);
+    if (g.ncell < (1ull << 32)) {  // multiply-high divisions (FastDiv)
+      const unsigned cc = (unsigned)c, r = fast_div(cc, g.dnx), q = fast_div(r, g.dny);
+      ix = (int)(cc - r * (unsigned)g.nx);
+      iy = (int)(r - q * (unsigned)g.ny);
+      iz = (int)q;
+    } else {
+      ix = (int)(c % g.nx);
+      size_t r = c / g.nx;
+      iy = (int)(r % g.ny);
+      iz = (int)(r / g.ny);
+    }
     const size_t nfx = (size_t)(g.nx + 1) * g.ny * g.nz;
     const size_t nfy = (size_t)g.nx * (g.ny + 1) * g.nz;
     const size_t nfz = (size_t)g.nx * g.ny * (g.nz + 1);

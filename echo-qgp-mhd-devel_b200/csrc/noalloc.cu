@@ -113,6 +113,7 @@ extern "C" int echo_gpu_rhs_noalloc(const EchoParams* p, const double* d_eos_col
   c.g.ddx = p->nx > 1 ? 1. / dx : 0.;
   c.g.ddy = p->ny > 1 ? 1. / dy : 0.;
   c.g.ddz = p->nz > 1 ? 1. / dz : 0.;
+  set_grid_div(c.g);
   for (int d = 0; d < 3; d++) {
     int uni = 1, sgn = 0;
     for (int k = 0; k < ECHO_MAX_NV; k++)

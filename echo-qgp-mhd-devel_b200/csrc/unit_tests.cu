@@ -65,6 +65,34 @@ static void launch_c2p_test(DevPhys P, Metric M, int algo, double tol, int ncell
   c2p_test_kernel<KIND><<<(ncells + 127) / 128, 128>>>(P, M, algo, tol, ncells, u, v, err, iters);
 }
 
+static __global__ void fastdiv_test_kernel(const unsigned* d, int nd, const unsigned* n, int nn, unsigned* q) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nd * nn) return;
+  const int i = (int)(t / nn), j = (int)(t % nn);
+  q[t] = echo::fast_div(n[j], echo::make_fastdiv(d[i]));
+}
+
+extern "C" int echo_gpu_test_fastdiv(const unsigned* d, int nd, const unsigned* n, int nn, unsigned* q) {
+  (void)cudaGetLastError();
+  if (nd <= 0 || nn <= 0 || !d || !n || !q) return ECHO_ERR_ARG;
+  for (int i = 0; i < nd; i++)
+    if (d[i] == 0) return ECHO_ERR_ARG;
+  const size_t nq = (size_t)nd * nn;
+  unsigned *dd, *dn, *dq;
+  CK(cudaMalloc(&dd, nd * sizeof(unsigned)));
+  CK(cudaMalloc(&dn, nn * sizeof(unsigned)));
+  CK(cudaMalloc(&dq, nq * sizeof(unsigned)));
+  CK(cudaMemcpy(dd, d, nd * sizeof(unsigned), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dn, n, nn * sizeof(unsigned), cudaMemcpyHostToDevice));
+  fastdiv_test_kernel<<<(unsigned)((nq + 127) / 128), 128>>>(dd, nd, dn, nn, dq);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(q, dq, nq * sizeof(unsigned), cudaMemcpyDeviceToHost));
+  cudaFree(dd);
+  cudaFree(dn);
+  cudaFree(dq);
+  return ECHO_OK;
+}
+
 extern "C" int echo_gpu_test_recon(int recal, int m, int n, const double* f, double* gl, double* gr) {
   (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
   if (m <= 0 || n <= 0 || !f || !gl || !gr) return ECHO_ERR_ARG;

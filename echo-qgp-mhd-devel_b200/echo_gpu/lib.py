@@ -105,6 +105,8 @@ FUNCTIONS = {
     "echo_gpu_set_stage": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, I]),
     "echo_gpu_set_faces": (ctypes.c_int, [P, ctypes.c_int]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
+    "echo_gpu_test_fastdiv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                             ctypes.c_void_p]),
     "echo_gpu_test_c2p": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, D, D, I, I]),
     "echo_gpu_hyp_init": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
@@ -406,6 +408,18 @@ def unit_recon(recal: int, f: np.ndarray, n: int, exact: bool = True):
     if rc:
         raise RuntimeError(f"test_recon status {rc}")
     return gl, gr
+
+
+def unit_fastdiv(d, n, exact: bool = False):
+    """n[j] // d[i] on the device by the kernels' multiply-high division."""
+    L = load(exact)
+    d = np.ascontiguousarray(d, dtype=np.uint32)
+    n = np.ascontiguousarray(n, dtype=np.uint32)
+    q = np.empty((len(d), len(n)), dtype=np.uint32)
+    rc = L.echo_gpu_test_fastdiv(d.ctypes.data, len(d), n.ctypes.data, len(n), q.ctypes.data)
+    if rc:
+        raise RuntimeError(f"test_fastdiv status {rc}")
+    return q
 
 
 def unit_c2p(params, eos_table, g3, gp, u, vguess, exact: bool = True):

@@ -378,6 +378,12 @@ int echo_gpu_rhs(EchoCtx* ctx, double* du, double* amax3);
  * Allocates 8 bytes and synchronises the device. */
 int echo_gpu_fp64_peak(double* gflops, double* ms);
 
+/* No counterpart in the reference (a check of the kernels' index
+ * arithmetic): q[i*nn + j] = n[j] / d[i] (unsigned, d[i] >= 1) computed on
+ * the device with the multiply-high division the face and cell kernels use
+ * to split flat indices into grid coordinates. */
+int echo_gpu_test_fastdiv(const unsigned* d, int nd, const unsigned* n, int nn, unsigned* q);
+
 /* Reconstruction of m pencils of length n (+ghosts) with REC_ALGO.
  * f is m rows of (n + 8) values, f[row*(n+8) + (i+4)] = f(i), i=-4..n+3;
  * gl/gr are m rows of n+1 faces (holib.f90:47-348). */
