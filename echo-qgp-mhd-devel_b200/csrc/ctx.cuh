@@ -59,6 +59,11 @@ struct EchoCtx {
   // product build: how the face sweeps run: 0 one thread per face, 8 or 16
   // the cell-centred kernel in segments of that many cells
   int face_mode;
+  // concurrent sweeps: the y and eta sweeps of a stage run on two side
+  // streams forked from and joined back into `stream` (par_sweeps = 1)
+  int par_sweeps;
+  cudaStream_t side[2];
+  cudaEvent_t ev_fork, ev_join[2];
   // the fused stage kernel (stage.cuh): usable, on, tile, segment, launch
   int st_ok, st_on, st_tx, st_ty, st_zseg, st_nt;
   unsigned st_grid;

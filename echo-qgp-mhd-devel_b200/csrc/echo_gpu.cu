@@ -152,6 +152,11 @@ int echo_setup_phys(const EchoParams* p, const double* eos_table, int n_eos, Dev
   return ECHO_OK;
 }
 
+// whether the sweeps of a stage run concurrently (launch_sweeps)
+#ifndef ECHO_PAR_SWEEPS
+#define ECHO_PAR_SWEEPS 1
+#endif
+
 // how the product build's face sweeps run (echo_gpu_set_faces)
 #ifndef ECHO_FACE_MODE
 #define ECHO_FACE_MODE 0
@@ -182,16 +187,43 @@ static void launch_scalars(EchoCtx* c, int irk, int mode = 0) {
   stage_scalars_kernel<<<1, 1, 0, c->stream>>>(S);
 }
 
-// the three flux sweeps of a stage; the CFL maxima start from zero
-static void enqueue_sweeps(EchoCtx* c) {
-  cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream);
+// The flux sweeps of a stage.  They are independent of each other: each
+// reads v and writes its own face fluxes and its own signal-speed slots
+// (amax_bits[d], aflux[d]).  With par_sweeps the first runs on `stream` and
+// the others on the side streams, forked from and joined back into it, so
+// that the partial last wave of one overlaps the others (under stream
+// capture the fork and join become branches of the step graph).  Per-kernel
+// profiling keeps them in order, so that each can be timed.
+static void launch_sweeps(EchoCtx* c) {
+  int dirs[3], nd = 0;
   for (int d = 0; d < 3; d++) {
     int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
-    if (n > 1) {
-      DISPATCH(c, launch_faces, c, d);
-      mark(c, PK_FACES_X + d);
-    }
+    if (n > 1) dirs[nd++] = d;
   }
+  if (!c->par_sweeps || c->marks || nd < 2) {
+    for (int j = 0; j < nd; j++) {
+      DISPATCH(c, launch_faces, c, dirs[j]);
+      mark(c, PK_FACES_X + dirs[j]);
+    }
+    return;
+  }
+  cudaEventRecord(c->ev_fork, c->stream);
+  const cudaStream_t main = c->stream;
+  for (int j = 1; j < nd; j++) {
+    cudaStreamWaitEvent(c->side[j - 1], c->ev_fork, 0);
+    c->stream = c->side[j - 1];
+    DISPATCH(c, launch_faces, c, dirs[j]);
+    cudaEventRecord(c->ev_join[j - 1], c->stream);
+  }
+  c->stream = main;
+  DISPATCH(c, launch_faces, c, dirs[0]);
+  for (int j = 1; j < nd; j++) cudaStreamWaitEvent(c->stream, c->ev_join[j - 1], 0);
+}
+
+// the flux sweeps of a stage; the CFL maxima start from zero
+static void enqueue_sweeps(EchoCtx* c) {
+  cudaMemsetAsync(c->d_sc->amax_bits, 0, sizeof(unsigned long long) * 3, c->stream);
+  launch_sweeps(c);
 }
 
 // IMEX-SSP3(4,3,3) stage (evolve.f90:204-267), all asynchronous
@@ -259,13 +291,7 @@ static void enqueue_stage(EchoCtx* c, int irk) {
     launch_scalars(c, irk, 4);
     mark(c, PK_SCALARS);
   } else {
-    for (int d = 0; d < 3; d++) {
-      int n = d == 0 ? c->g.nx : d == 1 ? c->g.ny : c->g.nz;
-      if (n > 1) {
-        DISPATCH(c, launch_faces, c, d);
-        mark(c, PK_FACES_X + d);
-      }
-    }
+    launch_sweeps(c);
     launch_scalars(c, irk);
     cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
     cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
@@ -367,6 +393,12 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   c->nfaces[2] = (size_t)p->nx * p->ny * (p->nz + 1);
   size_t nvc = (size_t)c->nv * c->g.ncell;
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->side[0], cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->side[1], cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_join[0], cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_join[1], cudaEventDisableTiming));
+  c->par_sweeps = ECHO_PAR_SWEEPS;
   for (int i = 0; i < 2; i++) {
     CK(cudaMalloc(&c->d_v[i], sizeof(double) * nvc));
     CK(cudaMalloc(&c->d_u[i], sizeof(double) * nvc));
@@ -459,6 +491,11 @@ int echo_gpu_free(EchoCtx* c) {
   echo_hyp_free(c->hyp);
   echo_out_free(c);
   cudaStreamDestroy(c->stream);
+  cudaStreamDestroy(c->side[0]);
+  cudaStreamDestroy(c->side[1]);
+  cudaEventDestroy(c->ev_fork);
+  cudaEventDestroy(c->ev_join[0]);
+  cudaEventDestroy(c->ev_join[1]);
   free(c);
   return ECHO_OK;
 }
@@ -895,6 +932,18 @@ int echo_gpu_profile_step(EchoCtx* c, double* ms, int* launches) {
   }
   for (auto& m : marks) cudaEventDestroy(m.second);
   cudaEventDestroy(start);
+  return ECHO_OK;
+}
+
+int echo_gpu_set_sweeps(EchoCtx* c, int concurrent) {
+  if (!c || (concurrent != 0 && concurrent != 1)) return ECHO_ERR_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  c->par_sweeps = concurrent;
+  for (int i = 0; i < 16; i++)
+    if (c->graph_ok[i]) {
+      cudaGraphExecDestroy(c->graph[i]);
+      c->graph_ok[i] = false;
+    }
   return ECHO_OK;
 }
 

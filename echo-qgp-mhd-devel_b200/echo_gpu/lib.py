@@ -104,6 +104,7 @@ FUNCTIONS = {
     "echo_gpu_profile_step": (ctypes.c_int, [P, D, I]),
     "echo_gpu_set_stage": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, I]),
     "echo_gpu_set_faces": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_gpu_set_sweeps": (ctypes.c_int, [P, ctypes.c_int]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_fastdiv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                              ctypes.c_void_p]),
@@ -297,6 +298,11 @@ class Evolve:
         face (the default), 8 or 16 cell-centred segments of that many
         cells."""
         self._check(self.lib.echo_gpu_set_faces(self.h, mode), "set_faces")
+
+    def set_sweeps(self, concurrent: bool = True):
+        """The x, y and eta sweeps of a stage side by side on three streams
+        (the default) or one after another."""
+        self._check(self.lib.echo_gpu_set_sweeps(self.h, 1 if concurrent else 0), "set_sweeps")
 
     def set_stage(self, fused: bool = True, tx: int = 0, ty: int = 0, zseg: int = 0) -> dict:
         """Fused stage kernel on or off (and its tile); returns the choice."""

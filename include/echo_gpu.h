@@ -348,6 +348,13 @@ int echo_gpu_profile_step(EchoCtx* ctx, double* ms, int* launches);
  * Synchronises the stream and drops the step graphs. */
 int echo_gpu_set_faces(EchoCtx* ctx, int mode);
 
+/* No counterpart in the reference (an execution option).  concurrent = 1
+ * (the default) runs the x, y and eta flux sweeps of a stage side by side
+ * on three streams, joined before the update; 0 runs them one after
+ * another.  The sweeps are independent, so both give the same bits.
+ * Synchronises the stream and drops the step graphs. */
+int echo_gpu_set_sweeps(EchoCtx* ctx, int concurrent);
+
 /* No counterpart in the reference (an execution option).  How a stage runs:
  * fused = 1 (where the run allows it) runs the three sweeps,
  * the flux divergence, the sources, the update and con2prim of a stage in

@@ -13,7 +13,7 @@ import pytest
 import pyoracle as O
 from echo_gpu import params as P
 from echo_gpu.lib import Evolve, unit_c2p, unit_recon
-from helpers import CASES, gubser_case, rel_linf, setup
+from helpers import CASES, gubser_case, rel_linf, resistive_state, setup
 
 pytestmark = pytest.mark.gpu
 
@@ -271,3 +271,35 @@ def test_rhs_parity():
     du_g, am_g = g.rhs()
     assert rel_linf(du_g, du_o, cfg.nv) <= 1e-13
     assert np.allclose(am_g, am_o, rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("case,nrk", [("rmhd3d", P.RK3), ("visc2d", P.RK2), ("res3d", P.SSP)])
+def test_concurrent_sweeps_give_the_same_bits(case, nrk):
+    """The three sweeps of a stage run side by side on three streams by
+    default: they are independent (each writes its own face fluxes and its
+    own signal-speed slots), so the run equals the one with the sweeps in
+    order, bit for bit, in both builds; stepped eagerly and through the step
+    graph."""
+    cfg = CASES[case]().replace(nrk=nrk)
+    if case == "res3d":
+        cfg = cfg.replace(sigma_el=500.0)
+    pc, tab, v = setup(cfg)
+    if case == "res3d":
+        v = resistive_state(cfg, tab)
+    for exact in (True, False):
+        out = []
+        for concurrent in (False, True):
+            g = Evolve(pc, tab, exact=exact)
+            g.set_sweeps(concurrent)
+            g.upload(v, None, cfg.tstart)
+            g.step()
+            g.run(3)
+            g.sync()
+            st = g.stats()
+            assert st.errcode == 0
+            out.append((g.download(), st.t))
+            g.close()
+        (v0, u0), t0 = out[0]
+        (v1, u1), t1 = out[1]
+        assert t0 == t1
+        assert np.array_equal(v0, v1) and np.array_equal(u0, u1)
