@@ -15,7 +15,8 @@ value:   cell-updates/s with the state resident in HBM (the library's CUDA
          beside it in `variants`.
 e2e:     the same metric through the C-ABI with host buffers: every step
          copies v and u from page-locked host memory to the device, runs one
-         step and copies v back.
+         step and copies v and u back (echo_gpu_advance_host, whose copy of
+         u overlaps the first flux sweeps).
 --impl reference: the reference algorithm on the host cores (the CPU
          restatement in oracle/, all threads), on a bounded sample of the
          same workload.
@@ -687,9 +688,8 @@ def run_b200(args):
     f1 = torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(e2e_steps):
-        ev.put_state(hv.data_ptr(), hu.data_ptr())
-        ev.run(1)
-        ev.get_state(hv.data_ptr(), hu.data_ptr())  # the host owns the whole state between steps
+        # the host owns the whole state between steps: copied in, one step, copied out
+        ev.advance_host(hv.data_ptr(), hu.data_ptr(), hv.data_ptr(), hu.data_ptr(), 1)
     f1.record(stream)
     ev.sync()
     barrier()

@@ -64,6 +64,12 @@ struct EchoCtx {
   int par_sweeps;
   cudaStream_t side[2];
   cudaEvent_t ev_fork, ev_join[2];
+  // echo_gpu_advance_host: the host copy of u runs on copy_stream and ev_u
+  // marks its end; while wait_u is set, the next step's first u access
+  // waits for it (join_u)
+  cudaStream_t copy_stream;
+  cudaEvent_t ev_u, ev_u_fork;
+  int wait_u;
   // the fused stage kernel (stage.cuh): usable, on, tile, segment, launch
   int st_ok, st_on, st_tx, st_ty, st_zseg, st_nt;
   unsigned st_grid;

@@ -273,6 +273,12 @@ static void enqueue_stage_ssp(EchoCtx* c, int irk) {
 }
 
 // one explicit RK stage, all asynchronous
+// the stream waits for the host copy of u of echo_gpu_advance_host
+static void join_u(EchoCtx* c) {
+  cudaStreamWaitEvent(c->stream, c->ev_u, 0);
+  c->wait_u = 0;
+}
+
 static void enqueue_stage(EchoCtx* c, int irk) {
   if (c->p.nrk == ECHO_SSP) {
     enqueue_stage_ssp(c, irk);
@@ -292,6 +298,7 @@ static void enqueue_stage(EchoCtx* c, int irk) {
     mark(c, PK_SCALARS);
   } else {
     launch_sweeps(c);
+    if (c->wait_u) join_u(c);  // the update reads u
     launch_scalars(c, irk);
     cudaMemsetAsync(&c->d_sc->nfail, 0, sizeof(int), c->stream);
     cudaMemsetAsync(&c->d_sc->c2p_iters, 0, sizeof(unsigned long long), c->stream);
@@ -328,9 +335,14 @@ static void end_step(EchoCtx* c) {
 }
 
 static void enqueue_step(EchoCtx* c) {
+  // a host copy of u still in flight (echo_gpu_advance_host): the explicit
+  // RK stages wait for it after their first sweeps, which read v only; the
+  // other paths touch u at once
+  if (c->wait_u && (c->keep_old || c->p.nrk == ECHO_SSP || (c->st_ok && c->st_on))) join_u(c);
   snapshot_vnewstep(c);
   for (int irk = 1; irk <= c->p.nrk; irk++) enqueue_stage(c, irk);
   end_step(c);
+  if (c->wait_u) join_u(c);
 }
 
 // the role changes of enqueue_step without launching anything
@@ -398,6 +410,9 @@ int echo_gpu_init(const EchoParams* p, const double* eos_table, int n_eos, EchoC
   CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&c->ev_join[0], cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&c->ev_join[1], cudaEventDisableTiming));
+  CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&c->ev_u, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_u_fork, cudaEventDisableTiming));
   c->par_sweeps = ECHO_PAR_SWEEPS;
   for (int i = 0; i < 2; i++) {
     CK(cudaMalloc(&c->d_v[i], sizeof(double) * nvc));
@@ -496,6 +511,9 @@ int echo_gpu_free(EchoCtx* c) {
   cudaEventDestroy(c->ev_fork);
   cudaEventDestroy(c->ev_join[0]);
   cudaEventDestroy(c->ev_join[1]);
+  cudaStreamDestroy(c->copy_stream);
+  cudaEventDestroy(c->ev_u);
+  cudaEventDestroy(c->ev_u_fork);
   free(c);
   return ECHO_OK;
 }
@@ -667,6 +685,33 @@ int echo_gpu_run(EchoCtx* c, int nsteps) {
     }
     CK(cudaGraphLaunch(c->graph[key], c->stream));
   }
+  CK(cudaGetLastError());
+  return ECHO_OK;
+}
+
+int echo_gpu_advance_host(EchoCtx* c, const double* v_in, const double* u_in, double* v_out, double* u_out,
+                          int nsteps) {
+  if (c && c->p.algo_solver == ECHO_C2P_MLP && !c->d_mlp_frag) return ECHO_ERR_ARG;  // no network loaded
+  (void)cudaGetLastError();  // a failed launch of an earlier call must not be reported here
+  if (!c || !v_in || !u_in || nsteps < 0) return ECHO_ERR_ARG;
+  const size_t bytes = sizeof(double) * c->nv * c->g.ncell;
+  // v first, at the link's full rate: the first sweeps need it
+  CK(cudaMemcpyAsync(c->d_v[c->vcur], v_in, bytes, cudaMemcpyHostToDevice, c->stream));
+  // u beside the first sweeps, after everything queued so far (which may
+  // still read or write u)
+  CK(cudaEventRecord(c->ev_u_fork, c->stream));
+  CK(cudaStreamWaitEvent(c->copy_stream, c->ev_u_fork, 0));
+  CK(cudaMemcpyAsync(c->d_u[c->ucur], u_in, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+  CK(cudaEventRecord(c->ev_u, c->copy_stream));
+  c->wait_u = 1;
+  if (nsteps > 0) {
+    enqueue_step(c);  // launched directly: its first stage waits for u after the sweeps
+    int r = echo_gpu_run(c, nsteps - 1);
+    if (r) return r;
+  }
+  if (c->wait_u) join_u(c);
+  if (v_out) CK(cudaMemcpyAsync(v_out, c->d_v[c->vcur], bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (u_out) CK(cudaMemcpyAsync(u_out, c->d_u[c->ucur], bytes, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaGetLastError());
   return ECHO_OK;
 }

@@ -105,6 +105,8 @@ FUNCTIONS = {
     "echo_gpu_set_stage": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, I]),
     "echo_gpu_set_faces": (ctypes.c_int, [P, ctypes.c_int]),
     "echo_gpu_set_sweeps": (ctypes.c_int, [P, ctypes.c_int]),
+    "echo_gpu_advance_host": (ctypes.c_int, [P, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int]),
     "echo_gpu_test_recon": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D]),
     "echo_gpu_test_fastdiv": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                              ctypes.c_void_p]),
@@ -262,6 +264,13 @@ class Evolve:
         if code.value:
             raise CrashError(code.value)
         return dt.value
+
+    def advance_host(self, v_in_ptr: int, u_in_ptr: int, v_out_ptr: int | None, u_out_ptr: int | None,
+                     nsteps: int = 1):
+        """put_state, run(nsteps) and get_state in one call (host pointers,
+        asynchronous); the copy of u overlaps the first flux sweeps."""
+        self._check(self.lib.echo_gpu_advance_host(self.h, v_in_ptr, u_in_ptr, v_out_ptr, u_out_ptr, nsteps),
+                    "advance_host")
 
     def run(self, nsteps: int):
         self._check(self.lib.echo_gpu_run(self.h, nsteps), "run")

@@ -185,6 +185,17 @@ int echo_gpu_step(EchoCtx* ctx, double* dt, int* errcode);
  * per step after the first).  Check errors with echo_gpu_stats. */
 int echo_gpu_run(EchoCtx* ctx, int nsteps);
 
+/* No counterpart in the reference (the call of a host that owns the state
+ * between steps): echo_gpu_put_state(v_in, u_in), echo_gpu_run(nsteps),
+ * echo_gpu_get_state(v_out, u_out) in one call, with the same results.  The
+ * copy of u runs on a second stream beside the first stage's flux sweeps,
+ * which read v only; the first update waits for it.  v_out and u_out may be
+ * v_in and u_in, or NULL (not copied).  Asynchronous like
+ * echo_gpu_get_state: synchronise before reading the outputs.  Host buffers
+ * should be page-locked. */
+int echo_gpu_advance_host(EchoCtx* ctx, const double* v_in, const double* u_in, double* v_out,
+                          double* u_out, int nsteps);
+
 int echo_gpu_stats(EchoCtx* ctx, EchoStats* st);
 int echo_gpu_sync(EchoCtx* ctx);
 
