@@ -599,6 +599,19 @@ __device__ __forceinline__ void derived_pi_zz(const Metric& M, const double* p, 
   double g1 = M.g1, g2 = M.g2, g3 = M.g3;
   double vx = p[KVX], vy = p[KVY], vz = p[KVZ];
   double pixy = p[KPIXY], pixx = p[KPIXX], piyy = p[KPIYY], piyz = p[KPIYZ], pixz = p[KPIXZ];
+  if (vz == 0.) {
+    // v^eta = 0 (every cell of a boost-invariant run): the terms below with
+    // a factor vz are exact zeros and 1 - vz^2 g3 is exactly 1, so these are
+    // the same sums in the same order, with the same bits
+    o.tt = vx * g1 * pixy * vy * g2 + vx * vx * g1 * g1 * pixx + vy * g1 * g1 * pixy * vx + vy * vy * g1 * piyy * g2;
+    o.tx = pixx * vx * g1 + pixy * vy * g2;
+    o.ty = pixy * vx * g1 + piyy * vy * g2;
+    o.tz = pixz * vx * g1 + piyz * vy * g2;
+    o.zz = 1. / g3 *
+           (vx * g1 * pixy * vy * g2 - pixx * g1 - piyy * g2 + vx * vx * g1 * g1 * pixx + vy * g1 * g1 * pixy * vx +
+            vy * vy * g1 * piyy * g2);
+    return;
+  }
   o.tt = 1. / (1. - vz * vz * g3) *
          (vx * g1 * pixy * vy * g2 + vx * vx * g1 * g1 * pixx + vy * g1 * piyz * vz * g3 +
           2. * vx * g1 * pixz * vz * g3 + vy * g1 * g1 * pixy * vx + vy * vy * g1 * piyy * g2 +
