@@ -1098,7 +1098,13 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
       if (fabs(nvy) < eps) nvy = 0.;
       double nvz = sz / (en1 + pr);
       if (fabs(nvz) < eps) nvz = 0.;
-      const double dv = fmax3(fabs(nvx - vx), fabs(nvy - vy), fabs(nvz - vz) * M.gp);
+      // the converged passes' test: a component below eps is zeroed (above), so
+      // one that sits at that threshold can alternate between 0 and just above
+      // eps forever; one whose old and new values are both below 2 eps counts
+      // as settled
+      const double dvs = fmax3(fabs(nvx) < 2. * eps && fabs(vx) < 2. * eps ? 0. : fabs(nvx - vx),
+                               fabs(nvy) < 2. * eps && fabs(vy) < 2. * eps ? 0. : fabs(nvy - vy),
+                               fabs(nvz) < 2. * eps && fabs(vz) < 2. * eps ? 0. : fabs(nvz - vz) * M.gp);
       vx = nvx;
       vy = nvy;
       vz = nvz;
@@ -1107,7 +1113,7 @@ __device__ int cons2prim(const DevPhys& P, const Metric& M, int algo, double tol
       vprim[KVZ] = vz;
       if (conv) {
         p0 = pr;
-        if (dv <= 1.e-14 && !seeded_pass) break;
+        if (dvs <= 1.e-14 && !seeded_pass) break;
       } else if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) {
         break;
       }

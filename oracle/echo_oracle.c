@@ -1623,7 +1623,12 @@ static int cons2prim(const Phys* ph, double* u, double* v, int* iters) {
       if (fabs(nvy) < eps) nvy = 0.;
       double nvz = sz / (en1 + pr);
       if (fabs(nvz) < eps) nvz = 0.;
-      double dv = fmax(fmax(fabs(nvx - vx), fabs(nvy - vy)), fabs(nvz - vz) * ph->gp);
+      /* the converged passes' test, as the library states it: a component whose
+       * old and new values are both below 2 eps (where the zeroing above can
+       * make the passes alternate) counts as settled */
+      double dvs = fmax(fmax(fabs(nvx) < 2. * eps && fabs(vx) < 2. * eps ? 0. : fabs(nvx - vx),
+                             fabs(nvy) < 2. * eps && fabs(vy) < 2. * eps ? 0. : fabs(nvy - vy)),
+                        fabs(nvz) < 2. * eps && fabs(vz) < 2. * eps ? 0. : fabs(nvz - vz) * ph->gp);
       vx = nvx;
       vy = nvy;
       vz = nvz;
@@ -1632,7 +1637,7 @@ static int cons2prim(const Phys* ph, double* u, double* v, int* iters) {
       vprim[KVZ] = vz;
       if (conv) {
         p0 = pr;
-        if (dv <= 1.e-14) break;
+        if (dvs <= 1.e-14) break;
       } else if (fabs(g1 * (vx * vx) + g2 * (vy * vy) + g3 * (vz * vz) - v2) < eps) {
         break;
       }
