@@ -311,7 +311,7 @@ class Evolve:
     def set_sweeps(self, concurrent: bool = True):
         """The x, y and eta sweeps of a stage side by side on three streams
         (the default) or one after another."""
-        self._check(self.lib.echo_gpu_set_sweeps(self.h, 1 if concurrent else 0), "set_sweeps")
+        self._check(self.lib.echo_gpu_set_sweeps(self.h, int(concurrent)), "set_sweeps")
 
     def set_stage(self, fused: bool = True, tx: int = 0, ty: int = 0, zseg: int = 0) -> dict:
         """Fused stage kernel on or off (and its tile); returns the choice."""

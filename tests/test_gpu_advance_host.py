@@ -61,3 +61,22 @@ def test_advance_host_equals_put_run_get(name, exact):
     (v0, u0, t0, d0), (v1, u1, t1, d1) = states
     assert t0 == t1 and d0 == d1
     assert np.array_equal(v0, v1) and np.array_equal(u0, u1)
+
+
+def test_advance_host_and_set_sweeps_check_their_arguments():
+    cfg = CASES["hd2d"]()
+    pc, tab, v = setup(cfg)
+    g = Evolve(pc, tab, exact=False)
+    g.upload(v, None, cfg.tstart)
+    hv, hu = g.download()
+    with pytest.raises(RuntimeError):
+        g.advance_host(hv.ctypes.data, hu.ctypes.data, None, None, -1)
+    with pytest.raises(RuntimeError):
+        g.advance_host(0, hu.ctypes.data, None, None, 1)
+    with pytest.raises(RuntimeError):
+        g.set_sweeps(2)
+    # outputs may be omitted: the state advances on the device all the same
+    g.advance_host(hv.ctypes.data, hu.ctypes.data, None, None, 2)
+    g.sync()
+    assert g.stats().errcode == 0
+    g.close()
